@@ -1,0 +1,147 @@
+/*
+ * yasf_b200 — C ABI of the B200-native coupling backend for the T-matrix multiple-sphere solve.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status (YASF_OK == 0), never
+ * synchronises the host unless stated, and never takes ownership of caller memory. Vectors are
+ * device pointers to interleaved complex numbers (re, im), particle-major: element (s, n) sits
+ * at s*nmax + n, n = (tau-1)*lmax*(lmax+2) + (l-1)*(l+1) + l + m, exactly the unknown ordering of
+ * yasfpy/functions/cpu_numba.py:371-407. `stream` is a cudaStream_t passed as void*
+ * (NULL = legacy default stream). Positions are device float64 (N, 3) row-major, lengths in the
+ * same unit as the wavelength; k_medium is the real medium wavenumber (yasfpy/parameters.py:96-100).
+ *
+ * Precision codes: YASF_C128 computes the translation generation and contraction in complex128;
+ * YASF_C64 computes them in complex64 while vectors stay complex128 (inputs are rounded on the
+ * way in, outputs widened on the way out).
+ */
+#ifndef YASF_B200_H
+#define YASF_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define YASF_ABI_VERSION 1
+
+enum yasf_status {
+  YASF_OK = 0,
+  YASF_ERR_INVALID_ARGUMENT = 1, /* null pointer, non-positive size, bad enum value */
+  YASF_ERR_UNSUPPORTED = 2,      /* lmax outside [1, 8], non-finite k, ... */
+  YASF_ERR_ALIGNMENT = 3,        /* pointer not 16-byte aligned */
+  YASF_ERR_CUDA = 4,             /* a CUDA runtime call failed (see yasf_last_cuda_error) */
+  YASF_ERR_OUT_OF_MEMORY = 5,    /* a device allocation made by the library failed */
+  YASF_ERR_WORKSPACE = 6,        /* workspace smaller than the size query returned */
+  YASF_ERR_NOT_FINITE = 7,       /* NaN/Inf in the right-hand side or the iteration */
+  YASF_ERR_NOT_PREPARED = 8      /* preconditioner used before prepare */
+};
+
+enum yasf_precision { YASF_C128 = 0, YASF_C64 = 1 };
+
+typedef struct yasf_plan yasf_plan;         /* per-lmax translation structure on one device */
+typedef struct yasf_precond yasf_precond;   /* block-Jacobi preconditioner on one device */
+
+/* ---- library ---------------------------------------------------------------------------- */
+int yasf_abi_version(void);
+const char* yasf_status_string(int status);
+/* Last CUDA error string seen by the library on this thread ("" if none). */
+const char* yasf_last_cuda_error(void);
+
+/* ---- plan: the a5/b5 translation table in the layout the kernels stream -----------------
+ * Replaces the per-Simulation table handling of yasfpy/coupling/cpu_dense.py:45-64 and
+ * yasfpy/coupling/cuda_dense.py:52-158. `translation_ab5` is the HOST complex128 array
+ * (nmax, nmax, 2*lmax+1) of yasfpy/numerics.py:187-281 (Numerics.translation_ab5), indexed
+ * [n_source, n_receiver, p] as the matvec reads it (cpu_numba.py:86). The plan is built for the
+ * current CUDA device and allocates its own device memory. */
+int yasf_plan_create(int lmax, const double* translation_ab5, yasf_plan** plan);
+int yasf_plan_destroy(yasf_plan* plan);
+/* nmax, stream entries per source particle (all bundles), source-side terms per particle. */
+int yasf_plan_info(const yasf_plan* plan, int* nmax, long long* stream_entries,
+                   long long* source_terms);
+
+/* Bytes of caller-provided device workspace needed by the coupling entry points for
+ * n_particles spheres and nrhs right-hand sides at `precision`. */
+int yasf_coupling_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, int precision,
+                                 size_t* bytes);
+
+/* ---- coupling matvec -----------------------------------------------------------------------
+ * y = W x with every W_ij generated on the fly (spherical Hankel h_p(k r_ij) by upward
+ * recurrence, normalised Legendre P_p^{|m-m'|}(cos theta_ij) by the CELES recurrence, the
+ * azimuthal phase e^{i(m'-m) phi_ij}, and the a5/b5 coefficients), summed over s_j != s_i.
+ * Replaces particle_interaction_scalar (yasfpy/functions/cpu_numba.py:22-95) behind
+ * DenseCouplingOps.matvec (yasfpy/coupling/ops.py:29-49) and CouplingBackend.multiply
+ * (yasfpy/coupling/backends.py:47-66).
+ * x, y: (n_particles*nmax) complex128 on the device; nrhs columns are stored column after
+ * column with leading dimension ld (>= n_particles*nmax). */
+int yasf_coupling_matvec(const yasf_plan* plan, int n_particles, const double* positions,
+                         double k_medium, const double* x, double* y, int nrhs, long long ld,
+                         int precision, void* workspace, size_t workspace_bytes, void* stream);
+
+/* y = x - T (.) (W x): the master operator of yasfpy/matrix_apply.py:66-120 fused into the
+ * reduction epilogue. tmat is (n_particles*nmax) complex128: T[s,n] = mie[sidx[s], n, w]. */
+int yasf_master_matvec(const yasf_plan* plan, int n_particles, const double* positions,
+                       double k_medium, const double* tmat, const double* x, double* y, int nrhs,
+                       long long ld, int precision, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/* ---- cross sections (yasfpy/optics.py:55-156) ------------------------------------------------
+ * out[0..1] (device) <- sum_{s,n} conj(b) (W_reg b), the bilinear form of
+ * compute_scattering_cross_section (yasfpy/functions/cpu_numba.py:410-457): regular spherical
+ * Bessel j_p, self pairs included. C_sca = pi/|k|^2 * |out|. */
+int yasf_scattering_bilinear(const yasf_plan* plan, int n_particles, const double* positions,
+                             double k_medium, const double* b, double* out, void* workspace,
+                             size_t workspace_bytes, void* stream);
+/* out[0..1] (device) <- sum conj(a) * b over n elements (C_ext = -pi/|k|^2 * Re(out)). */
+int yasf_dotc(long long n, const double* a, const double* b, double* out, void* workspace,
+              size_t workspace_bytes, void* stream);
+
+/* ---- block-Jacobi preconditioner (yasfpy/preconditioner.py:58-219) ---------------------------
+ * Blocks are given as a particle list per block (CSR: block_ptr[n_blocks+1], particles[]); the
+ * library assembles M_B = (I - T W)[B,B] on the device with the same generator as the matvec
+ * (particle-major rows and columns, receiver Mie factor), the caller replaces every block by its
+ * inverse in place (any dense complex128 inversion on the device, e.g. a cuSOLVER getrf/getrs),
+ * and finalize makes the complex64 copy used by YASF_C64 applications.
+ * apply: y = M^{-1} x, block by block (x and y must not alias). */
+int yasf_precond_create(const yasf_plan* plan, int n_particles, int n_blocks,
+                        const int* block_ptr /*host*/, const int* particles /*host*/,
+                        yasf_precond** pc);
+int yasf_precond_destroy(yasf_precond* pc);
+/* Replaces prepare()'s block assembly (yasfpy/preconditioner.py:92-175, 365-442). Asynchronous. */
+int yasf_precond_assemble(yasf_precond* pc, const double* positions, double k_medium,
+                          const double* tmat, void* stream);
+/* Device pointer and order of block `block`: row-major (dim, dim) complex128, dim = n_B*nmax,
+ * rows/columns in the block's particle order, particle-major inside. */
+int yasf_precond_block(const yasf_precond* pc, int block, double** matrix, int* dim);
+/* Call after every block holds its inverse. */
+int yasf_precond_finalize(yasf_precond* pc, void* stream);
+/* Replaces BlockDiagonalPreconditioner.apply (yasfpy/preconditioner.py:177-219). */
+int yasf_precond_apply(const yasf_precond* pc, const double* x, double* y, int nrhs, long long ld,
+                       int precision, void* stream);
+/* Device bytes held by the factors. */
+int yasf_precond_bytes(const yasf_precond* pc, size_t* bytes);
+
+/* ---- device GMRES (yasfpy/solver.py:65-181 -> scipy.sparse.linalg.gmres) --------------------
+ * Restarted, left-preconditioned GMRES with SciPy's stopping rules: the inner loop stops when the
+ * preconditioned residual estimate reaches ptol (adapted per restart as SciPy does), every restart
+ * cycle ends with the true residual ||b - A x|| checked against rtol*||b||; maxiter counts
+ * restart cycles. A = I - T W. x holds x0 on entry and the solution on exit. Arnoldi uses
+ * classical Gram-Schmidt with one re-orthogonalisation pass; Givens rotations and the Hessenberg
+ * solve run on the device in float64.
+ * inner_precision: YASF_C128 for the plain solve; YASF_C64 runs the Krylov iterations on the
+ * complex64 matvec and wraps them in float64 iterative refinement (true residual, update and
+ * stopping test in float64), see the solve stats.
+ * stats (host, may be NULL): [0] inner iterations, [1] matvecs at inner precision,
+ * [2] float64 matvecs, [3] final ||b - A x|| / ||b||, [4] info (0 converged, else maxiter),
+ * [5] refinement steps. */
+int yasf_gmres_workspace_size(const yasf_plan* plan, int n_particles, int restart,
+                              int inner_precision, size_t* bytes);
+int yasf_gmres_solve(const yasf_plan* plan, int n_particles, const double* positions,
+                     double k_medium, const double* tmat, const yasf_precond* pc, const double* b,
+                     double* x, double rtol, int restart, int maxiter, int inner_precision,
+                     void* workspace, size_t workspace_bytes, double* stats, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* YASF_B200_H */

@@ -1,0 +1,221 @@
+"""Generate the golden fixtures in tests/golden/ by running the upstream reference itself.
+
+Run in a container where the reference ``yasfpy`` source tree is available (read-only) at
+``$YASF_REFERENCE`` (default ``/root/reference``):
+
+    python tests/golden/make_golden.py
+
+The reference imports with the stand-ins from ``oracle/stubs`` (pywigxjpf via sympy's exact 3j,
+refidxdb and pyperf as inert stand-ins). Two kinds of fixtures are written:
+
+- ``celes_*.npz``: the MATLAB/CELES golden vectors that the reference's own tests hold
+  (reference tests/data/*.mat, read by tests/test_comparison.py and tests/test_full_simulation.py),
+  converted to particle-major numpy arrays.
+- ``ref_*.npz``: outputs of the reference code path on seeded synthetic inputs (coupling matvec,
+  master operator, Mie / incident / right-hand side, GMRES solve, cross sections, and the
+  preconditioner block matrices assembled column by column from the reference's own
+  master_matrix_multiply).
+
+Nothing on the GPU box reads the reference: the fixtures are committed.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+REF = Path(os.environ.get("YASF_REFERENCE", "/root/reference"))
+sys.path.insert(0, str(REPO))
+sys.path.insert(0, str(REPO / "oracle" / "stubs"))
+sys.path.insert(0, str(REF))
+os.environ.setdefault("HOME", "/tmp/yasf_golden_home")
+
+from scipy.io import loadmat  # noqa: E402
+
+from yasf_b200.workloads import aggregate_c1, rsa_ball, rsa_cube  # noqa: E402
+
+
+def ref_modules():
+    from yasfpy.initial_field import InitialField
+    from yasfpy.numerics import Numerics
+    from yasfpy.optics import Optics
+    from yasfpy.parameters import Parameters
+    from yasfpy.particles import Particles
+    from yasfpy.simulation import Simulation
+    from yasfpy.solver import Solver
+
+    return InitialField, Numerics, Optics, Parameters, Particles, Simulation, Solver
+
+
+def ref_simulation(positions, radii, m, wavelength, lmax, tol=1e-8, restart=100, max_iter=1000,
+                   polar=0.0, azimuthal=0.0, pol="TE", wavelengths=None):
+    InitialField, Numerics, Optics, Parameters, Particles, Simulation, Solver = ref_modules()
+    n = positions.shape[0]
+    particles = Particles(position=positions, r=radii, refractive_index=np.full(n, m, dtype=complex))
+    field = InitialField(beam_width=0, focal_point=np.zeros(3), polar_angle=polar,
+                         azimuthal_angle=azimuthal, polarization=pol)
+    wl = np.atleast_1d(wavelength if wavelengths is None else wavelengths).astype(float)
+    params = Parameters(wavelength=wl, medium_refractive_index=np.ones(wl.size, dtype=complex),
+                        particles=particles, initial_field=field)
+    solver = Solver(solver_type="gmres", tolerance=tol, max_iter=max_iter, restart=restart)
+    numerics = Numerics(lmax=lmax, sampling_points_number=np.array([10]), gpu=False, solver=solver,
+                        coupling_backend="dense")
+    numerics.compute_translation_table()
+    sim = Simulation(params, numerics)
+    return sim, Optics
+
+
+def save(name: str, **arrays):
+    path = HERE / name
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path.name} ({path.stat().st_size / 1024:.0f} KiB)")
+
+
+def celes_fixtures():
+    data = REF / "tests" / "data"
+    d = loadmat(data / "coupling_matrix_multiply_data.mat")
+    lmax = int(d["lmax"][0, 0])
+    nmax = 2 * lmax * (lmax + 2)
+    npart = d["particles_position"].shape[0]
+    to_pm = lambda v: v.flatten().reshape((nmax, npart)).T.flatten()  # noqa: E731
+    save("celes_coupling.npz", lmax=lmax, wavelength=float(d["wavelength"][0, 0]),
+         medium_index=float(d["mediumRefractiveIndex"][0, 0]),
+         positions=d["particles_position"].astype(float),
+         radii=d["particles_radius"].flatten().astype(float),
+         refractive_index=d["particles_refractiveIndex"].flatten(),
+         x=to_pm(d["input_x"]), wx=to_pm(d["coupling_matrix_output_Wx"]).astype(np.complex128))
+    t = loadmat(data / "translation_table_ab_data.mat")
+    save("celes_translation_lmax3.npz", table=t["translation_table_tta"]["ab5"][0, 0].astype(np.complex128))
+    f = loadmat(data / "full_simulation_data.mat")
+    save("celes_full_simulation.npz", lmax=int(f["lmax"][0, 0]), wavelength=float(f["wavelength"][0, 0]),
+         medium_index=float(f["mediumRefractiveIndex"][0, 0]),
+         positions=f["particles_position"].astype(float),
+         radii=f["particles_radius"].flatten().astype(float),
+         refractive_index=f["particles_refractiveIndex"].flatten(),
+         initial=f["initial_field_coefficients"].astype(np.complex128),
+         mie=f["mie_coefficients"].astype(np.complex128),
+         scattered=f["scattered_field_coefficients"].astype(np.complex128))
+
+
+def translation_fixtures(lmax_values=(1, 2, 3, 4, 5, 6)):
+    _, Numerics, *_ = ref_modules()
+    out = {}
+    for L in lmax_values:
+        t0 = time.time()
+        num = Numerics(lmax=L, sampling_points_number=np.array([10]))
+        num.compute_translation_table(force_compute=True)
+        out[f"lmax{L}"] = num.translation_ab5
+        print(f"  translation table lmax={L}: {time.time() - t0:.1f}s")
+    save("ref_translation.npz", **out)
+
+
+def matvec_fixture(name, positions, radii, m, wavelength, lmax, seed):
+    sim, _ = ref_simulation(positions, radii, m, wavelength, lmax)
+    rng = np.random.default_rng(seed)
+    n = positions.shape[0] * sim.numerics.nmax
+    x = rng.normal(size=n) + 1j * rng.normal(size=n)
+    wx = sim.coupling_matrix_multiply(x, idx=0)
+    sim.compute_mie_coefficients()
+    mx = sim.master_matrix_multiply(x, 0)
+    sidx = sim.parameters.particles.single_unique_array_idx
+    tmat = sim.mie_coefficients[sidx, :, 0].ravel()
+    save(name, lmax=lmax, wavelength=wavelength, refractive_index=m, positions=positions, radii=radii,
+         x=x, wx=wx, mx=mx, tmat=tmat)
+
+
+def multichannel_fixture():
+    pos = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.25, 0.5, 0.0]])
+    radii = np.array([0.1, 0.1, 0.1])
+    sim, _ = ref_simulation(pos, radii, 1.5 + 0.0j, None, 2, wavelengths=np.array([1.0, 1.3]))
+    rng = np.random.default_rng(0)
+    n = 3 * sim.numerics.nmax
+    x = rng.normal(size=n) + 1j * rng.normal(size=n)
+    save("ref_multichannel.npz", lmax=2, wavelengths=np.array([1.0, 1.3]), positions=pos, radii=radii,
+         x=x, wx_all=sim.coupling_matrix_multiply(x), wx_1=sim.coupling_matrix_multiply(x, idx=1))
+
+
+def solve_fixture(name, agg, tol, restart=100):
+    sim, Optics = ref_simulation(agg.positions, agg.radii, agg.refractive_index, agg.wavelength, agg.lmax,
+                                 tol=tol, restart=restart)
+    t0 = time.time()
+    sim.compute_mie_coefficients()
+    sim.compute_initial_field_coefficients()
+    sim.compute_right_hand_side()
+    sim.compute_scattered_field_coefficients()
+    t_solve = time.time() - t0
+    opt = Optics(sim)
+    opt.compute_cross_sections()
+    sidx = sim.parameters.particles.single_unique_array_idx
+    save(name, lmax=agg.lmax, wavelength=agg.wavelength, refractive_index=agg.refractive_index,
+         positions=agg.positions, radii=agg.radii, tol=tol,
+         mie=sim.mie_coefficients[:, :, 0], sidx=sidx,
+         initial=sim.initial_field_coefficients[:, :, 0], rhs=sim.right_hand_side[:, :, 0],
+         scattered=sim.scattered_field_coefficients[:, :, 0],
+         err_code=sim.scattered_field_err_codes[0], c_ext=float(opt.c_ext[0]),
+         c_sca=float(opt.c_sca[0]), solve_seconds=t_solve)
+    print(f"  {name}: C_ext={opt.c_ext[0]:.10g} C_sca={opt.c_sca[0]:.10g} ({t_solve:.1f}s)")
+
+
+def precond_fixture():
+    """Reference-derived block matrices for a geometry whose cells hold several spheres."""
+    from yasfpy.preconditioner import make_particle_partition
+
+    rng = np.random.default_rng(7)
+    radii = rng.uniform(0.05, 0.1, size=10)
+    pos = rsa_cube(radii, 0.10, rng, max_attempts=200_000)
+    lmax = 2
+    sim, _ = ref_simulation(pos, radii, 1.55 + 0.02j, 0.6, lmax)
+    sim.compute_mie_coefficients()
+    extent = pos.max(axis=0) - pos.min(axis=0)
+    edges = (extent + 2.0) / 2.0
+    blocks = make_particle_partition(pos, edges)
+    nmax = sim.numerics.nmax
+    mats = {}
+    for b, blk in enumerate(blocks):
+        idx = (blk[:, None] * nmax + np.arange(nmax)[None, :]).ravel()
+        M = np.zeros((idx.size, idx.size), dtype=complex)
+        for c, gi in enumerate(idx):
+            e = np.zeros(pos.shape[0] * nmax, dtype=complex)
+            e[gi] = 1.0
+            M[:, c] = sim.master_matrix_multiply(e, 0)[idx]
+        mats[f"block{b}"] = M
+        mats[f"particles{b}"] = blk
+    sidx = sim.parameters.particles.single_unique_array_idx
+    save("ref_precond_blocks.npz", lmax=lmax, wavelength=0.6, refractive_index=1.55 + 0.02j,
+         positions=pos, radii=radii, edges=edges, n_blocks=len(blocks),
+         tmat=sim.mie_coefficients[sidx, :, 0].ravel(), **mats)
+
+
+def main():
+    t0 = time.time()
+    only = set(sys.argv[1:])
+    if not only or "tables" in only:
+        celes_fixtures()
+        translation_fixtures()
+    c1 = aggregate_c1(seed=0)
+    if not only or "c1" in only:
+        matvec_fixture("ref_matvec_c1.npz", c1.positions, c1.radii, c1.refractive_index,
+                       c1.wavelength, c1.lmax, seed=11)
+    rng = np.random.default_rng(3)
+    r6 = np.clip(rng.lognormal(np.log(0.1), 0.2, size=12), 0.04, 0.25)
+    p6 = rsa_ball(r6, 0.08, rng, max_attempts=200_000)
+    matvec_fixture("ref_matvec_l6.npz", p6, r6, 1.6 + 0.005j, 0.6, 6, seed=12)
+    rng = np.random.default_rng(5)
+    r3 = rng.uniform(0.05, 0.15, size=9)
+    p3 = rsa_cube(r3, 0.12, rng, max_attempts=200_000)
+    matvec_fixture("ref_matvec_l3.npz", p3, r3, 1.45 + 0.03j, 0.5, 3, seed=13)
+    multichannel_fixture()
+    solve_fixture("ref_solve_c1_tol1e-8.npz", c1, 1e-8)
+    solve_fixture("ref_solve_c1_tol1e-13.npz", c1, 1e-13)
+    precond_fixture()
+    print(f"done in {time.time() - t0:.0f}s")
+
+
+if __name__ == "__main__":
+    main()

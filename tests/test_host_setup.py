@@ -1,0 +1,89 @@
+"""Host-side setup of the product against the reference (CPU only).
+
+translation table (yasfpy/numerics.py:187-281), Mie coefficients (yasfpy/mie_coefficients.py),
+plane-wave coefficients (yasfpy/initial_field_coefficients.py:79-142), right-hand side
+(yasfpy/simulation.py:189-205), cell partition (yasfpy/preconditioner.py:222-265).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import rel_err
+
+from yasf_b200.incident import compute_initial_field_coefficients
+from yasf_b200.initial_field import InitialField
+from yasf_b200.mie import compute_mie_coefficients
+from yasf_b200.parameters import Parameters
+from yasf_b200.particles import Particles
+from yasf_b200.preconditioner import make_particle_partition
+from yasf_b200.wigner import translation_table_ab5, wigner_3j
+
+
+@pytest.mark.parametrize("lmax", [1, 2, 3, 4, 5, 6])
+def test_translation_table_matches_reference(golden, lmax):
+    ref = golden("ref_translation.npz")[f"lmax{lmax}"]
+    ours = translation_table_ab5(lmax)
+    assert ours.shape == ref.shape
+    # exact 3j (product) vs exact 3j (sympy stand-in inside the reference): float64 rounding only
+    assert np.max(np.abs(ours - ref)) <= 1e-14 * np.max(np.abs(ref))
+
+
+def test_translation_table_matches_celes_golden(golden):
+    celes = golden("celes_translation_lmax3.npz")["table"]
+    np.testing.assert_allclose(translation_table_ab5(3), celes, rtol=1e-5, atol=1e-7)
+
+
+def test_wigner_selection_rules():
+    assert wigner_3j(1, 1, 3, 0, 0, 0) == 0.0  # triangle
+    assert wigner_3j(1, 1, 1, 0, 0, 0) == 0.0  # odd sum with m = 0
+    assert wigner_3j(2, 2, 2, 1, 1, -1) == 0.0  # sum of m != 0
+    assert abs(wigner_3j(1, 1, 0, 0, 0, 0) - (-1 / np.sqrt(3))) < 3e-16
+
+
+def _setup(g):
+    n = g["positions"].shape[0]
+    particles = Particles(g["positions"], g["radii"], np.full(n, complex(g["refractive_index"])))
+    field = InitialField(beam_width=0, focal_point=np.zeros(3), polar_angle=0.0, azimuthal_angle=0.0,
+                         polarization="TE")
+    params = Parameters(np.array([float(g["wavelength"])]), np.array([1.0 + 0j]), particles, field)
+    return particles, field, params
+
+
+def test_mie_initial_rhs_match_reference(golden):
+    g = golden("ref_solve_c1_tol1e-8.npz")
+    lmax = int(g["lmax"])
+    particles, field, params = _setup(g)
+    mie, _ = compute_mie_coefficients(lmax, params.omega, params.k_medium,
+                                      particles.unique_radius_index_pairs)
+    assert rel_err(mie[:, :, 0], g["mie"]) < 1e-13
+    np.testing.assert_array_equal(particles.single_unique_array_idx, g["sidx"])
+    a = compute_initial_field_coefficients(lmax, particles.position, params.k_medium, field)
+    assert rel_err(a[:, :, 0], g["initial"]) < 1e-13
+    rhs = mie[particles.single_unique_array_idx, :, 0] * a[:, :, 0]
+    assert rel_err(rhs, g["rhs"]) < 1e-13
+
+
+def test_mie_initial_match_celes_golden(golden):
+    g = golden("celes_full_simulation.npz")
+    lmax = int(g["lmax"])
+    n = g["positions"].shape[0]
+    particles = Particles(g["positions"], g["radii"], g["refractive_index"])
+    field = InitialField(beam_width=0, focal_point=np.zeros(3), polarization="TE")
+    params = Parameters(np.array([float(g["wavelength"])]), np.array([float(g["medium_index"])]),
+                        particles, field)
+    mie, _ = compute_mie_coefficients(lmax, params.omega, params.k_medium,
+                                      particles.unique_radius_index_pairs)
+    tm = mie[particles.single_unique_array_idx, :, 0]
+    np.testing.assert_allclose(tm, g["mie"], rtol=1e-4, atol=1e-6)
+    a = compute_initial_field_coefficients(lmax, particles.position, params.k_medium, field)[:, :, 0]
+    np.testing.assert_allclose(a, g["initial"], rtol=1e-4, atol=1e-5)
+    assert n == 3
+
+
+def test_partition_semantics(golden):
+    g = golden("ref_precond_blocks.npz")
+    blocks = make_particle_partition(g["positions"], g["edges"])
+    assert len(blocks) == int(g["n_blocks"])
+    for b, blk in enumerate(blocks):
+        np.testing.assert_array_equal(blk, g[f"particles{b}"])

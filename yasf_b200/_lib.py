@@ -1,0 +1,119 @@
+"""ctypes binding of the C ABI declared in ``include/yasf_b200.h``.
+
+The shared library is built in-tree (``yasf_b200/_build/libyasf_b200.so``, see
+``yasf_b200/build.py``). There is no CPU fallback: if the library is missing or cannot be loaded,
+importing the device layer raises ``RuntimeError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import torch  # noqa: F401  (loads the CUDA runtime the library links against)
+
+LIB_PATH = Path(__file__).resolve().parent / "_build" / "libyasf_b200.so"
+
+YASF_OK = 0
+YASF_C128 = 0
+YASF_C64 = 1
+
+_STATUS_NAMES = {
+    1: "YASF_ERR_INVALID_ARGUMENT",
+    2: "YASF_ERR_UNSUPPORTED",
+    3: "YASF_ERR_ALIGNMENT",
+    4: "YASF_ERR_CUDA",
+    5: "YASF_ERR_OUT_OF_MEMORY",
+    6: "YASF_ERR_WORKSPACE",
+    7: "YASF_ERR_NOT_FINITE",
+    8: "YASF_ERR_NOT_PREPARED",
+}
+
+
+class YasfError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, func: str, status: int, detail: str = ""):
+        self.status = status
+        name = _STATUS_NAMES.get(status, f"status {status}")
+        msg = f"{func} failed: {name}"
+        if detail:
+            msg += f" ({detail})"
+        super().__init__(msg)
+
+
+_c = ctypes
+_vp = _c.c_void_p
+_i = _c.c_int
+_ll = _c.c_longlong
+_d = _c.c_double
+_sz = _c.c_size_t
+_dp = _c.POINTER(_c.c_double)
+
+# name -> (argtypes)
+SIGNATURES = {
+    "yasf_abi_version": [],
+    "yasf_status_string": [_i],
+    "yasf_last_cuda_error": [],
+    "yasf_plan_create": [_i, _vp, _c.POINTER(_vp)],
+    "yasf_plan_destroy": [_vp],
+    "yasf_plan_info": [_vp, _c.POINTER(_i), _c.POINTER(_ll), _c.POINTER(_ll)],
+    "yasf_coupling_workspace_size": [_vp, _i, _i, _i, _c.POINTER(_sz)],
+    "yasf_coupling_matvec": [_vp, _i, _vp, _d, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],
+    "yasf_master_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],
+    "yasf_scattering_bilinear": [_vp, _i, _vp, _d, _vp, _vp, _vp, _sz, _vp],
+    "yasf_dotc": [_ll, _vp, _vp, _vp, _vp, _sz, _vp],
+    "yasf_precond_create": [_vp, _i, _i, _vp, _vp, _c.POINTER(_vp)],
+    "yasf_precond_destroy": [_vp],
+    "yasf_precond_assemble": [_vp, _vp, _d, _vp, _vp],
+    "yasf_precond_block": [_vp, _i, _c.POINTER(_vp), _c.POINTER(_i)],
+    "yasf_precond_finalize": [_vp, _vp],
+    "yasf_precond_apply": [_vp, _vp, _vp, _i, _ll, _i, _vp],
+    "yasf_precond_bytes": [_vp, _c.POINTER(_sz)],
+    "yasf_gmres_workspace_size": [_vp, _i, _i, _i, _c.POINTER(_sz)],
+    "yasf_gmres_solve": [
+        _vp, _i, _vp, _d, _vp, _vp, _vp, _vp, _d, _i, _i, _i, _vp, _sz, _dp, _vp,
+    ],
+}
+_RESTYPES = {
+    "yasf_status_string": _c.c_char_p,
+    "yasf_last_cuda_error": _c.c_char_p,
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: Path | str | None = None) -> ctypes.CDLL:
+    """Load (once) and return the C library with argument types set."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise RuntimeError(
+                f"yasf_b200 CUDA library not found at {p}; build it with "
+                "`python -c 'import __graft_entry__ as g; g.build()'` or `python yasf_b200/build.py`"
+            )
+        lib = ctypes.CDLL(str(p))
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, _i)
+        _lib = lib
+        return lib
+
+
+def check(func: str, status: int) -> None:
+    if status != YASF_OK:
+        detail = ""
+        if status == 4:
+            detail = (load().yasf_last_cuda_error() or b"").decode()
+        raise YasfError(func, status, detail)
+
+
+def call(name: str, *args) -> None:
+    """Call a status-returning entry point and raise ``YasfError`` on failure."""
+    check(name, getattr(load(), name)(*args))

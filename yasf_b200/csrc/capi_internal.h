@@ -1,0 +1,74 @@
+// Internal host-side declarations shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "coupling.cuh"
+
+struct yasf_plan {
+  int lmax = 0;
+  int nmax = 0;
+  int device = -1;
+  int n_bundles = 0;
+  int bundle_begin[8] = {0};
+  int bundle_len[8] = {0};
+  int total_entries = 0;          // per source, all bundles (padded)
+  long long total_terms = 0;
+  // device arrays
+  int* d_entry_ptr = nullptr;
+  int* d_term_n2 = nullptr;
+  double2* d_term_coef = nullptr;
+  yasf::LegendreTables* d_leg = nullptr;
+  // nonzero (n1, n2, p) terms for explicit block assembly, CSR over (n1, n2)
+  int* d_pair_ptr = nullptr;      // [nmax*nmax + 1]
+  int* d_pair_p = nullptr;        // p of each term
+  double2* d_pair_coef = nullptr; // A[n2][n1][p]
+  long long pair_terms = 0;
+};
+
+namespace yasf {
+
+void set_cuda_error(cudaError_t e);
+void set_error_text(const std::string& s);
+
+#define YASF_CUDA_TRY(expr)                   \
+  do {                                        \
+    cudaError_t _e = (expr);                  \
+    if (_e != cudaSuccess) {                  \
+      ::yasf::set_cuda_error(_e);             \
+      return YASF_ERR_CUDA;                   \
+    }                                         \
+  } while (0)
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Coupling launch geometry and workspace layout for one matvec column.
+struct CouplingLayout {
+  int threads = 128;
+  int tiles = 1;
+  int chunks = 1;
+  int sources_per_chunk = 1;
+  size_t v_bytes = 0;        // stream buffer
+  size_t partial_bytes = 0;  // chunk partial sums
+  size_t dot_bytes = 0;      // block sums of the bilinear form
+  size_t total = 0;
+};
+
+CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int precision);
+
+// Launch the full coupling pipeline for one column (vbuild, contract, reduce).
+// mode: 0 -> y = W x, 1 -> y = x - T (.) W x, 2 -> block sums of conj(x) (.) W_reg x.
+int coupling_column(const yasf_plan* plan, int n_particles, const double* positions, double k,
+                    const double* tmat, const double* x, double* y, int precision, int mode,
+                    void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
+int dispatch_contract(int lmax, int precision, bool regular, const ContractArgs& a, int tiles,
+                      int chunks, int threads, cudaStream_t stream);
+
+int validate_coupling(const yasf_plan* plan, int n_particles, const double* positions,
+                      double k, int precision);
+
+}  // namespace yasf

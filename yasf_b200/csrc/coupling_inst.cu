@@ -1,0 +1,39 @@
+// Explicit instantiation of the coupling kernels for one lmax. The build compiles this file
+// once per lmax in [1, 8] with -DYASF_INST_L=<lmax> so the per-lmax kernels compile in parallel.
+#include "coupling.cuh"
+
+#ifndef YASF_INST_L
+#error "compile with -DYASF_INST_L=<lmax>"
+#endif
+
+namespace yasf {
+
+template <>
+cudaError_t launch_contract<YASF_INST_L>(int precision, bool regular, const ContractArgs& a,
+                                          int tiles, int chunks, int threads,
+                                          cudaStream_t stream) {
+  constexpr int L = YASF_INST_L;
+  const dim3 grid(tiles, chunks, num_bundles(L));
+  const size_t stage64 = 2 * (size_t)max_bundle_stream<L>() * sizeof(double2);
+  const size_t stage32 = 2 * (size_t)max_bundle_stream<L>() * sizeof(float2);
+  cudaError_t e;
+  if (regular) {
+    e = cudaFuncSetAttribute(contract_kernel<L, double, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage64);
+    if (e != cudaSuccess) return e;
+    contract_kernel<L, double, true><<<grid, threads, stage64, stream>>>(a);
+  } else if (precision == YASF_C64) {
+    e = cudaFuncSetAttribute(contract_kernel<L, float, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage32);
+    if (e != cudaSuccess) return e;
+    contract_kernel<L, float, false><<<grid, threads, stage32, stream>>>(a);
+  } else {
+    e = cudaFuncSetAttribute(contract_kernel<L, double, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage64);
+    if (e != cudaSuccess) return e;
+    contract_kernel<L, double, false><<<grid, threads, stage64, stream>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace yasf

@@ -1,0 +1,566 @@
+// Device GMRES (plain float64 and float64-refined complex64 inner solves).
+//
+// Semantics follow scipy.sparse.linalg.gmres as called by yasfpy/solver.py:108-121 (SciPy 1.18):
+// left preconditioning, restart cycles counted by maxiter, inner stop on the preconditioned
+// residual estimate against ptol (adapted per cycle as SciPy does), true residual ||b - A x||
+// checked against atol = rtol*||b|| at the end of every cycle, breakdown when h_{j+1,j} <=
+// eps*||w||. Orthogonalisation is classical Gram-Schmidt with one re-orthogonalisation pass
+// (two sweeps over the basis per step) instead of SciPy's modified Gram-Schmidt; Givens
+// rotations (LAPACK lartg form), the S vector and the triangular solve live on the device.
+#include <cmath>
+#include <vector>
+
+#include "capi_internal.h"
+
+namespace yasf {
+
+constexpr int kDotBlocks = 240;
+constexpr int kScal = 16;  // device scalars: see ScalarSlot
+
+enum ScalarSlot {
+  SL_H0 = 0,       // ||w|| before orthogonalisation
+  SL_H1 = 1,       // ||w|| after
+  SL_PRESID = 2,   // |S[col+1]|
+  SL_BREAK = 3,    // 1 if breakdown
+  SL_NORM = 4,     // generic norm result
+  SL_NONFINITE = 5
+};
+
+// partial[blk][k] = sum_{i in blk} conj(Q_k[i]) w[i]
+__global__ void __launch_bounds__(256) mdot_kernel(long long n, const double2* Q, long long ldq,
+                                                   int nvec, const double2* w, double2* partial) {
+  __shared__ double sr[8], si[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int k = 0; k < nvec; ++k) {
+    const double2* q = Q + (size_t)k * ldq;
+    double re = 0.0, im = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+      const double2 a = q[i], b = w[i];
+      re += a.x * b.x + a.y * b.y;
+      im += a.x * b.y - a.y * b.x;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      re += __shfl_down_sync(0xffffffffu, re, off);
+      im += __shfl_down_sync(0xffffffffu, im, off);
+    }
+    if (lane == 0) { sr[wid] = re; si[wid] = im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tr = 0.0, ti = 0.0;
+      for (int t = 0; t < (int)(blockDim.x >> 5); ++t) { tr += sr[t]; ti += si[t]; }
+      partial[(size_t)blockIdx.x * nvec + k] = make_double2(tr, ti);
+    }
+    __syncthreads();
+  }
+}
+
+// out[k] (+)= sum_blk partial[blk][k]; if as_norm, out is real sqrt(|.|) of vector 0 into scal.
+__global__ void mdot_final_kernel(int nvec, int nblk, const double2* partial, double2* out,
+                                  int accumulate, double* norm_out) {
+  __shared__ double sr[256], si[256];
+  const int k = blockIdx.x;
+  double re = 0.0, im = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    const double2 v = partial[(size_t)b * nvec + k];
+    re += v.x;
+    im += v.y;
+  }
+  sr[threadIdx.x] = re;
+  si[threadIdx.x] = im;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if (threadIdx.x < off) {
+      sr[threadIdx.x] += sr[threadIdx.x + off];
+      si[threadIdx.x] += si[threadIdx.x + off];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (norm_out) {
+      norm_out[0] = sqrt(fmax(sr[0], 0.0));
+    } else if (accumulate) {
+      out[k].x += sr[0];
+      out[k].y += si[0];
+    } else {
+      out[k] = make_double2(sr[0], si[0]);
+    }
+  }
+}
+
+// w -= sum_k h[k] Q_k   (sign = -1)   or   w += sum_k h[k] Q_k   (sign = +1)
+__global__ void __launch_bounds__(256) update_kernel(long long n, const double2* Q, long long ldq,
+                                                     int nvec, const double2* h, double sign,
+                                                     double2* w) {
+  __shared__ double2 sh[512];
+  for (int k = threadIdx.x; k < nvec && k < 512; k += blockDim.x) sh[k] = h[k];
+  __syncthreads();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < nvec; ++k) {
+      const double2 q = Q[(size_t)k * ldq + i];
+      const double2 c = sh[k];
+      re += c.x * q.x - c.y * q.y;
+      im += c.x * q.y + c.y * q.x;
+    }
+    double2 v = w[i];
+    v.x += sign * re;
+    v.y += sign * im;
+    w[i] = v;
+  }
+}
+
+// out = alpha_from_device (1 / *norm) * in ; if norm <= 0 copy.
+__global__ void scale_kernel(long long n, const double2* in, const double* norm, double2* out) {
+  const double nv = *norm;
+  const double f = nv > 0.0 ? 1.0 / nv : 1.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    out[i] = make_double2(v.x * f, v.y * f);
+  }
+}
+
+__global__ void sub_kernel(long long n, const double2* a, const double2* b, double2* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 x = a[i], y = b[i];
+    out[i] = make_double2(x.x - y.x, x.y - y.y);
+  }
+}
+
+__global__ void add_kernel(long long n, const double2* a, double2* x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double2 v = x[i];
+    const double2 d = a[i];
+    v.x += d.x;
+    v.y += d.y;
+    x[i] = v;
+  }
+}
+
+__global__ void copy_kernel(long long n, const double2* a, double2* b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+__device__ inline double cabs_d(double2 z) { return hypot(z.x, z.y); }
+
+// Start of a cycle: S = 0, S[0] = beta (= scal[SL_NORM]).
+__global__ void cycle_start_kernel(int m, double2* S, const double* scal) {
+  for (int i = threadIdx.x; i <= m; i += blockDim.x) S[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  if (threadIdx.x == 0) S[0] = make_double2(scal[SL_NORM], 0.0);
+}
+
+// After orthogonalisation of column col (h = H + col*(m+1)): set h[col+1] = h1, breakdown test,
+// apply previous rotations, compute the new one, update S, write presid.
+__global__ void givens_kernel(int col, int m, double2* H, double* gc, double2* gs, double2* S,
+                              double* scal, double eps) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double2* h = H + (size_t)col * (m + 1);
+  const double h0 = scal[SL_H0], h1 = scal[SL_H1];
+  bool brk = false;
+  if (h1 <= eps * h0) {
+    h[col + 1] = make_double2(0.0, 0.0);
+    brk = true;
+  } else {
+    h[col + 1] = make_double2(h1, 0.0);
+  }
+  for (int k = 0; k < col; ++k) {
+    const double c = gc[k];
+    const double2 s = gs[k];
+    const double2 n0 = h[k], n1 = h[k + 1];
+    // [c*n0 + s*n1, -conj(s)*n0 + c*n1]
+    const double2 a = make_double2(c * n0.x + s.x * n1.x - s.y * n1.y, c * n0.y + s.x * n1.y + s.y * n1.x);
+    const double2 b = make_double2(-(s.x * n0.x + s.y * n0.y) + c * n1.x, -(s.x * n0.y - s.y * n0.x) + c * n1.y);
+    h[k] = a;
+    h[k + 1] = b;
+  }
+  // lartg(f, g): c real, s complex, r with [c s; -conj(s) c][f; g] = [r; 0]
+  const double2 f = h[col], g = h[col + 1];
+  const double af = cabs_d(f), ag = cabs_d(g);
+  double c;
+  double2 s, r;
+  if (ag == 0.0) {
+    c = 1.0;
+    s = make_double2(0.0, 0.0);
+    r = f;
+  } else if (af == 0.0) {
+    c = 0.0;
+    s = make_double2(g.x / ag, -g.y / ag);
+    r = make_double2(ag, 0.0);
+  } else {
+    const double t = hypot(af, ag);
+    c = af / t;
+    const double2 fu = make_double2(f.x / af, f.y / af);
+    // s = fu * conj(g) / t
+    s = make_double2((fu.x * g.x + fu.y * g.y) / t, (fu.y * g.x - fu.x * g.y) / t);
+    r = make_double2(fu.x * t, fu.y * t);
+  }
+  gc[col] = c;
+  gs[col] = s;
+  h[col] = r;
+  h[col + 1] = make_double2(0.0, 0.0);
+  const double2 Sc = S[col];
+  // tmp = -conj(s) * S[col]
+  const double2 tmp = make_double2(-(s.x * Sc.x + s.y * Sc.y), -(s.x * Sc.y - s.y * Sc.x));
+  S[col] = make_double2(c * Sc.x, c * Sc.y);
+  S[col + 1] = tmp;
+  scal[SL_PRESID] = cabs_d(tmp);
+  scal[SL_BREAK] = brk ? 1.0 : 0.0;
+  if (!isfinite(h1) || !isfinite(h0) || !isfinite(scal[SL_PRESID])) scal[SL_NONFINITE] = 1.0;
+}
+
+// Solve the (col+1) upper triangular system H y = S (SciPy's pseudo-solve for zero pivots).
+__global__ void backsolve_kernel(int col, int m, const double2* H, double2* S, double2* y) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  auto Hk = [&](int row, int c) { return H[(size_t)c * (m + 1) + row]; };
+  if (Hk(col, col).x == 0.0 && Hk(col, col).y == 0.0) S[col] = make_double2(0.0, 0.0);
+  for (int i = 0; i <= col; ++i) y[i] = S[i];
+  for (int k = col; k > 0; --k) {
+    if (y[k].x != 0.0 || y[k].y != 0.0) {
+      const double2 d = Hk(k, k);
+      const double den = d.x * d.x + d.y * d.y;
+      const double2 q = make_double2((y[k].x * d.x + y[k].y * d.y) / den, (y[k].y * d.x - y[k].x * d.y) / den);
+      y[k] = q;
+      for (int i = 0; i < k; ++i) {
+        const double2 hk = Hk(i, k);
+        y[i].x -= q.x * hk.x - q.y * hk.y;
+        y[i].y -= q.x * hk.y + q.y * hk.x;
+      }
+    }
+  }
+  if (y[0].x != 0.0 || y[0].y != 0.0) {
+    const double2 d = Hk(0, 0);
+    const double den = d.x * d.x + d.y * d.y;
+    y[0] = make_double2((y[0].x * d.x + y[0].y * d.y) / den, (y[0].y * d.x - y[0].x * d.y) / den);
+  }
+}
+
+// --------------------------------------------------------------------------------------------
+struct GmresWs {
+  size_t coupling = 0;
+  size_t total = 0;
+  // offsets
+  size_t o_coupling = 0, o_Q = 0, o_w = 0, o_r = 0, o_t = 0, o_d = 0, o_H = 0, o_gc = 0, o_gs = 0,
+         o_S = 0, o_y = 0, o_part = 0, o_scal = 0;
+};
+
+static GmresWs gmres_layout(const yasf_plan* plan, int n_particles, int restart, int inner_prec) {
+  GmresWs L;
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t n = (size_t)n_particles * plan->nmax;
+  const size_t c128 = coupling_layout(plan, n_particles, YASF_C128).total;
+  const size_t c64 = inner_prec == YASF_C64 ? coupling_layout(plan, n_particles, YASF_C64).total : 0;
+  L.coupling = std::max(c128, c64);
+  size_t o = 0;
+  L.o_coupling = o; o += up(L.coupling);
+  L.o_Q = o; o += up((size_t)(restart + 1) * n * sizeof(double2));
+  L.o_w = o; o += up(n * sizeof(double2));
+  L.o_r = o; o += up(n * sizeof(double2));
+  L.o_t = o; o += up(n * sizeof(double2));
+  L.o_d = o; o += up(n * sizeof(double2));
+  L.o_H = o; o += up((size_t)(restart + 1) * restart * sizeof(double2));
+  L.o_gc = o; o += up((size_t)restart * sizeof(double));
+  L.o_gs = o; o += up((size_t)restart * sizeof(double2));
+  L.o_S = o; o += up((size_t)(restart + 1) * sizeof(double2));
+  L.o_y = o; o += up((size_t)(restart + 1) * sizeof(double2));
+  L.o_part = o; o += up((size_t)kDotBlocks * (restart + 1) * sizeof(double2));
+  L.o_scal = o; o += up(kScal * sizeof(double));
+  L.total = o;
+  return L;
+}
+
+struct Operator {
+  const yasf_plan* plan;
+  int N;
+  const double* pos;
+  double k;
+  const double* tmat;
+  const yasf_precond* pc;
+  void* cws;
+  size_t cws_bytes;
+  cudaStream_t s;
+};
+
+static int op_apply(const Operator& op, int precision, const double2* x, double2* y) {
+  return coupling_column(op.plan, op.N, op.pos, op.k, op.tmat, reinterpret_cast<const double*>(x),
+                         reinterpret_cast<double*>(y), precision, 1, op.cws, op.cws_bytes, op.s);
+}
+
+}  // namespace yasf
+
+extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, double* y, int nrhs,
+                                  long long ld, int precision, void* stream);
+
+namespace yasf {
+
+static int psolve(const Operator& op, int precision, const double2* x, double2* y, long long n) {
+  if (op.pc)
+    return yasf_precond_apply(op.pc, reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y),
+                              1, n, precision, op.s);
+  copy_kernel<<<1024, 256, 0, op.s>>>(n, x, y);
+  YASF_CUDA_TRY(cudaGetLastError());
+  return YASF_OK;
+}
+
+// Pinned scratch for the per-iteration device -> host scalar read.
+static double* pinned_scalars() {
+  static thread_local double* p = nullptr;
+  if (!p) {
+    if (cudaHostAlloc(reinterpret_cast<void**>(&p), kScal * sizeof(double), cudaHostAllocDefault) !=
+        cudaSuccess)
+      p = nullptr;
+  }
+  return p;
+}
+
+static int read_scalars(double* dscal, cudaStream_t s, double* host) {
+  double* pin = pinned_scalars();
+  if (!pin) return YASF_ERR_OUT_OF_MEMORY;
+  YASF_CUDA_TRY(cudaMemcpyAsync(pin, dscal, kScal * sizeof(double), cudaMemcpyDeviceToHost, s));
+  YASF_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int i = 0; i < kScal; ++i) host[i] = pin[i];
+  return YASF_OK;
+}
+
+struct Counters {
+  long long inner = 0, mv_inner = 0, mv64 = 0, refine = 0;
+};
+
+static int norm_into(long long n, const double2* v, double2* part, double* dst, cudaStream_t s) {
+  mdot_kernel<<<kDotBlocks, 256, 0, s>>>(n, v, n, 1, v, part);
+  YASF_CUDA_TRY(cudaGetLastError());
+  mdot_final_kernel<<<1, 256, 0, s>>>(1, kDotBlocks, part, nullptr, 0, dst);
+  YASF_CUDA_TRY(cudaGetLastError());
+  return YASF_OK;
+}
+
+// One GMRES run in SciPy's form on A = I - T W at `prec`, for rhs b and iterate x (both device).
+// Returns status; *info = 0 if ||b - A x|| <= atol at exit else maxiter; *rnorm_out final norm.
+static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, const double2* b,
+                      double2* x, double bnrm2, double atol, int restart, int maxiter,
+                      bool x_nonzero, Counters& cnt, int* info, double* rnorm_out) {
+  const long long n = (long long)op.N * op.plan->nmax;
+  double2* Q = reinterpret_cast<double2*>(ws + L.o_Q);
+  double2* w = reinterpret_cast<double2*>(ws + L.o_w);
+  double2* r = reinterpret_cast<double2*>(ws + L.o_r);
+  double2* t = reinterpret_cast<double2*>(ws + L.o_t);
+  double2* H = reinterpret_cast<double2*>(ws + L.o_H);
+  double* gc = reinterpret_cast<double*>(ws + L.o_gc);
+  double2* gs = reinterpret_cast<double2*>(ws + L.o_gs);
+  double2* S = reinterpret_cast<double2*>(ws + L.o_S);
+  double2* yv = reinterpret_cast<double2*>(ws + L.o_y);
+  double2* part = reinterpret_cast<double2*>(ws + L.o_part);
+  double* scal = reinterpret_cast<double*>(ws + L.o_scal);
+  cudaStream_t s = op.s;
+  const double eps = 2.220446049250313e-16;
+  double hs[kScal];
+  int st;
+  const int m = restart;
+
+  // Mb_nrm2 = ||psolve(b)||
+  if ((st = psolve(op, prec, b, t, n)) != YASF_OK) return st;
+  if ((st = norm_into(n, t, part, scal + SL_NORM, s)) != YASF_OK) return st;
+  if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
+  const double Mb_nrm2 = hs[SL_NORM];
+  double ptol_max_factor = 1.0;
+  double ptol = Mb_nrm2 * std::min(ptol_max_factor, atol / bnrm2);
+  double presid = 0.0, rnorm = 0.0;
+
+  // r = b - A x (or b)
+  if (x_nonzero) {
+    if ((st = op_apply(op, prec, x, t)) != YASF_OK) return st;
+    cnt.mv_inner += (prec == YASF_C128) ? 0 : 1;
+    cnt.mv64 += (prec == YASF_C128) ? 1 : 0;
+    sub_kernel<<<1024, 256, 0, s>>>(n, b, t, r);
+  } else {
+    copy_kernel<<<1024, 256, 0, s>>>(n, b, r);
+  }
+  YASF_CUDA_TRY(cudaGetLastError());
+  if ((st = norm_into(n, r, part, scal + SL_NORM, s)) != YASF_OK) return st;
+  if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
+  rnorm = hs[SL_NORM];
+  if (!std::isfinite(rnorm)) return YASF_ERR_NOT_FINITE;
+  if (rnorm < atol) {
+    *info = 0;
+    *rnorm_out = rnorm;
+    return YASF_OK;
+  }
+
+  for (int iter = 0; iter < maxiter; ++iter) {
+    // v0 = psolve(r) / ||.||
+    if ((st = psolve(op, prec, r, Q, n)) != YASF_OK) return st;
+    if ((st = norm_into(n, Q, part, scal + SL_NORM, s)) != YASF_OK) return st;
+    scale_kernel<<<1024, 256, 0, s>>>(n, Q, scal + SL_NORM, Q);
+    cycle_start_kernel<<<1, 256, 0, s>>>(m, S, scal);
+    YASF_CUDA_TRY(cudaGetLastError());
+    bool breakdown = false;
+    int col = 0;
+    for (col = 0; col < m; ++col) {
+      double2* vcol = Q + (size_t)col * n;
+      double2* hcol = H + (size_t)col * (m + 1);
+      if ((st = op_apply(op, prec, vcol, t)) != YASF_OK) return st;
+      if (prec == YASF_C128) cnt.mv64++; else cnt.mv_inner++;
+      if ((st = psolve(op, prec, t, w, n)) != YASF_OK) return st;
+      if ((st = norm_into(n, w, part, scal + SL_H0, s)) != YASF_OK) return st;
+      // CGS2: two projection sweeps
+      for (int pass = 0; pass < 2; ++pass) {
+        mdot_kernel<<<kDotBlocks, 256, 0, s>>>(n, Q, n, col + 1, w, part);
+        mdot_final_kernel<<<col + 1, 256, 0, s>>>(col + 1, kDotBlocks, part, pass == 0 ? hcol : yv,
+                                                   0, nullptr);
+        update_kernel<<<1024, 256, 0, s>>>(n, Q, n, col + 1, pass == 0 ? hcol : yv, -1.0, w);
+        if (pass == 1) {
+          // second-sweep coefficients are still in `part`: fold them into the column, h += h2
+          mdot_final_kernel<<<col + 1, 256, 0, s>>>(col + 1, kDotBlocks, part, hcol, 1, nullptr);
+        }
+        YASF_CUDA_TRY(cudaGetLastError());
+      }
+      if ((st = norm_into(n, w, part, scal + SL_H1, s)) != YASF_OK) return st;
+      scale_kernel<<<1024, 256, 0, s>>>(n, w, scal + SL_H1, Q + (size_t)(col + 1) * n);
+      givens_kernel<<<1, 1, 0, s>>>(col, m, H, gc, gs, S, scal, eps);
+      YASF_CUDA_TRY(cudaGetLastError());
+      if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
+      if (hs[SL_NONFINITE] != 0.0) return YASF_ERR_NOT_FINITE;
+      presid = hs[SL_PRESID];
+      breakdown = hs[SL_BREAK] != 0.0;
+      cnt.inner++;
+      if (presid <= ptol || breakdown) break;
+    }
+    if (col == m) col = m - 1;
+    backsolve_kernel<<<1, 1, 0, s>>>(col, m, H, S, yv);
+    update_kernel<<<1024, 256, 0, s>>>(n, Q, n, col + 1, yv, 1.0, x);
+    YASF_CUDA_TRY(cudaGetLastError());
+    if ((st = op_apply(op, prec, x, t)) != YASF_OK) return st;
+    if (prec == YASF_C128) cnt.mv64++; else cnt.mv_inner++;
+    sub_kernel<<<1024, 256, 0, s>>>(n, b, t, r);
+    YASF_CUDA_TRY(cudaGetLastError());
+    if ((st = norm_into(n, r, part, scal + SL_NORM, s)) != YASF_OK) return st;
+    if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
+    rnorm = hs[SL_NORM];
+    if (!std::isfinite(rnorm)) return YASF_ERR_NOT_FINITE;
+    if (rnorm <= atol) break;
+    if (breakdown) break;
+    if (presid <= ptol) ptol_max_factor = std::max(eps, 0.25 * ptol_max_factor);
+    else ptol_max_factor = std::min(1.0, 1.5 * ptol_max_factor);
+    ptol = presid * std::min(ptol_max_factor, atol / rnorm);
+  }
+  *info = (rnorm <= atol) ? 0 : maxiter;
+  *rnorm_out = rnorm;
+  return YASF_OK;
+}
+
+}  // namespace yasf
+
+using namespace yasf;
+
+extern "C" int yasf_gmres_workspace_size(const yasf_plan* plan, int n_particles, int restart,
+                                         int inner_precision, size_t* bytes) {
+  if (!plan || !bytes || n_particles <= 0 || restart <= 0 || restart > 512)
+    return YASF_ERR_INVALID_ARGUMENT;
+  if (inner_precision != YASF_C128 && inner_precision != YASF_C64) return YASF_ERR_INVALID_ARGUMENT;
+  *bytes = gmres_layout(plan, n_particles, restart, inner_precision).total;
+  return YASF_OK;
+}
+
+extern "C" int yasf_gmres_solve(const yasf_plan* plan, int n_particles, const double* positions,
+                                double k_medium, const double* tmat, const yasf_precond* pc,
+                                const double* b, double* x, double rtol, int restart, int maxiter,
+                                int inner_precision, void* workspace, size_t workspace_bytes,
+                                double* stats, void* stream) {
+  int st = validate_coupling(plan, n_particles, positions, k_medium, inner_precision);
+  if (st != YASF_OK) return st;
+  if (!tmat || !b || !x || restart <= 0 || restart > 512 || maxiter <= 0 || !(rtol >= 0.0))
+    return YASF_ERR_INVALID_ARGUMENT;
+  if (!aligned16(tmat) || !aligned16(b) || !aligned16(x) || !aligned16(workspace))
+    return YASF_ERR_ALIGNMENT;
+  const long long n = (long long)n_particles * plan->nmax;
+  const int m = (int)std::min<long long>(restart, n);
+  // the refined solve keeps its inner right-hand side in basis column m: needs m >= 2
+  if (inner_precision == YASF_C64 && m < 2) return YASF_ERR_INVALID_ARGUMENT;
+  const GmresWs L = gmres_layout(plan, n_particles, restart, inner_precision);
+  if (!workspace || workspace_bytes < L.total) return YASF_ERR_WORKSPACE;
+  char* ws = static_cast<char*>(workspace);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Operator op{plan, n_particles, positions, k_medium, tmat, pc, ws + L.o_coupling, L.coupling, s};
+  const double2* bb = reinterpret_cast<const double2*>(b);
+  double2* xx = reinterpret_cast<double2*>(x);
+  double2* part = reinterpret_cast<double2*>(ws + L.o_part);
+  double* scal = reinterpret_cast<double*>(ws + L.o_scal);
+  YASF_CUDA_TRY(cudaMemsetAsync(scal, 0, kScal * sizeof(double), s));
+  double hs[kScal];
+  // ||b|| and x0 != 0 test (SciPy: r = b - A x0 only if x0.any()).
+  if ((st = norm_into(n, bb, part, scal + SL_NORM, s)) != YASF_OK) return st;
+  if ((st = norm_into(n, xx, part, scal + SL_H0, s)) != YASF_OK) return st;
+  if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
+  const double bnrm2 = hs[SL_NORM];
+  const bool x_nonzero = hs[SL_H0] != 0.0;
+  if (!std::isfinite(bnrm2) || !std::isfinite(hs[SL_H0])) return YASF_ERR_NOT_FINITE;
+  Counters cnt;
+  int info = 0;
+  double rnorm = 0.0;
+  if (bnrm2 == 0.0) {
+    copy_kernel<<<1024, 256, 0, s>>>(n, bb, xx);
+    YASF_CUDA_TRY(cudaGetLastError());
+    YASF_CUDA_TRY(cudaStreamSynchronize(s));
+  } else if (inner_precision == YASF_C128) {
+    const double atol = rtol * bnrm2;
+    st = gmres_core(op, L, ws, YASF_C128, bb, xx, bnrm2, atol, m, maxiter, x_nonzero, cnt, &info,
+                    &rnorm);
+    if (st != YASF_OK) return st;
+  } else {
+    // Float64 iterative refinement around complex64 inner GMRES solves.
+    double2* r = reinterpret_cast<double2*>(ws + L.o_r);
+    double2* t = reinterpret_cast<double2*>(ws + L.o_t);
+    double2* d = reinterpret_cast<double2*>(ws + L.o_d);
+    const double atol = rtol * bnrm2;
+    const double inner_rtol = 1e-5;
+    const int max_refine = 20;
+    for (int it = 0;; ++it) {
+      if ((st = op_apply(op, YASF_C128, xx, t)) != YASF_OK) return st;
+      cnt.mv64++;
+      sub_kernel<<<1024, 256, 0, s>>>(n, bb, t, r);
+      YASF_CUDA_TRY(cudaGetLastError());
+      if ((st = norm_into(n, r, part, scal + SL_NORM, s)) != YASF_OK) return st;
+      if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
+      rnorm = hs[SL_NORM];
+      if (!std::isfinite(rnorm)) return YASF_ERR_NOT_FINITE;
+      if (rnorm <= atol) { info = 0; break; }
+      if (it >= max_refine) { info = maxiter; break; }
+      // inner solve A d = r at complex64, d0 = 0; r is preserved in a copy (d region reused)
+      YASF_CUDA_TRY(cudaMemsetAsync(d, 0, n * sizeof(double2), s));
+      // gmres_core overwrites r/t; keep the residual as the inner rhs in Q's last slot? use w.
+      double2* rhs = reinterpret_cast<double2*>(ws + L.o_w);
+      copy_kernel<<<1024, 256, 0, s>>>(n, r, rhs);
+      YASF_CUDA_TRY(cudaGetLastError());
+      // rhs lives in w, which the core uses as scratch; move it to the tail of d's neighbour: use
+      // the basis' last column as stable storage for the inner rhs.
+      double2* rhs_store = reinterpret_cast<double2*>(ws + L.o_Q) + (size_t)m * n;
+      copy_kernel<<<1024, 256, 0, s>>>(n, rhs, rhs_store);
+      YASF_CUDA_TRY(cudaGetLastError());
+      int inner_info = 0;
+      double inner_rn = 0.0;
+      const double inner_atol = std::max(inner_rtol * rnorm, 0.5 * atol);
+      // basis restricted to m-1 columns so the rhs column is never overwritten
+      st = gmres_core(op, L, ws, YASF_C64, rhs_store, d, rnorm, inner_atol,
+                      std::max(1, m - 1), maxiter, false, cnt, &inner_info, &inner_rn);
+      if (st != YASF_OK) return st;
+      add_kernel<<<1024, 256, 0, s>>>(n, d, xx);
+      YASF_CUDA_TRY(cudaGetLastError());
+      cnt.refine++;
+    }
+  }
+  if (stats) {
+    stats[0] = (double)cnt.inner;
+    stats[1] = (double)cnt.mv_inner;
+    stats[2] = (double)cnt.mv64;
+    stats[3] = bnrm2 > 0.0 ? rnorm / bnrm2 : 0.0;
+    stats[4] = (double)info;
+    stats[5] = (double)cnt.refine;
+  }
+  return YASF_OK;
+}
