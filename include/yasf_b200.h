@@ -46,6 +46,9 @@ int yasf_abi_version(void);
 const char* yasf_status_string(int status);
 /* Last CUDA error string seen by the library on this thread ("" if none). */
 const char* yasf_last_cuda_error(void);
+/* Kernels launched by the library in this process so far (all threads). Counterpart of the
+ * per-operator matvec_calls / uploads counters of yasfpy/coupling/cuda_dense.py:102-105. */
+unsigned long long yasf_kernel_launches(void);
 
 /* ---- plan: the a5/b5 translation table in the layout the kernels stream -----------------
  * Replaces the per-Simulation table handling of yasfpy/coupling/cpu_dense.py:45-64 and

@@ -56,6 +56,7 @@ SIGNATURES = {
     "yasf_abi_version": [],
     "yasf_status_string": [_i],
     "yasf_last_cuda_error": [],
+    "yasf_kernel_launches": [],
     "yasf_plan_create": [_i, _vp, _c.POINTER(_vp)],
     "yasf_plan_destroy": [_vp],
     "yasf_plan_info": [_vp, _c.POINTER(_i), _c.POINTER(_ll), _c.POINTER(_ll)],
@@ -79,6 +80,7 @@ SIGNATURES = {
 _RESTYPES = {
     "yasf_status_string": _c.c_char_p,
     "yasf_last_cuda_error": _c.c_char_p,
+    "yasf_kernel_launches": _c.c_ulonglong,
 }
 
 _lib = None

@@ -1,6 +1,7 @@
 // C-ABI: library status, translation plan, coupling matvec, cross-section reductions.
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <new>
 
@@ -9,6 +10,9 @@
 namespace yasf {
 
 static thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_cuda_error(cudaError_t e) { g_last_error = cudaGetErrorString(e); }
 void set_error_text(const std::string& s) { g_last_error = s; }
@@ -117,8 +121,8 @@ int coupling_column(const yasf_plan* plan, int n_particles, const double* positi
   va.v = vbuf;
   {
     const dim3 grid((plan->total_entries + 255) / 256, std::min(n_particles, 65535));
-    if (precision == YASF_C64) vbuild_kernel<float><<<grid, 256, 0, stream>>>(va);
-    else vbuild_kernel<double><<<grid, 256, 0, stream>>>(va);
+    if (precision == YASF_C64) YASF_COUNTED(vbuild_kernel<float><<<grid, 256, 0, stream>>>(va));
+    else YASF_COUNTED(vbuild_kernel<double><<<grid, 256, 0, stream>>>(va));
     YASF_CUDA_TRY(cudaGetLastError());
   }
   // 2) pair side + contraction
@@ -142,19 +146,19 @@ int coupling_column(const yasf_plan* plan, int n_particles, const double* positi
   // 3) chunk reduction + epilogue
   const long long n_elems = (long long)n_particles * plan->nmax;
   if (mode == 2) {
-    reduce_dot_kernel<double><<<1024, 256, 0, stream>>>(
-        n_elems, lay.chunks, partial, reinterpret_cast<const double2*>(x), dots, err);
+    YASF_COUNTED(reduce_dot_kernel<double><<<1024, 256, 0, stream>>>(
+        n_elems, lay.chunks, partial, reinterpret_cast<const double2*>(x), dots, err));
     YASF_CUDA_TRY(cudaGetLastError());
   } else {
     const int blocks = (int)std::min<long long>((n_elems + 255) / 256, 4096);
     if (precision == YASF_C64)
-      reduce_kernel<float><<<blocks, 256, 0, stream>>>(
+      YASF_COUNTED(reduce_kernel<float><<<blocks, 256, 0, stream>>>(
           n_elems, lay.chunks, partial, reinterpret_cast<const double2*>(x),
-          reinterpret_cast<const double2*>(tmat), reinterpret_cast<double2*>(y), mode, err);
+          reinterpret_cast<const double2*>(tmat), reinterpret_cast<double2*>(y), mode, err));
     else
-      reduce_kernel<double><<<blocks, 256, 0, stream>>>(
+      YASF_COUNTED(reduce_kernel<double><<<blocks, 256, 0, stream>>>(
           n_elems, lay.chunks, partial, reinterpret_cast<const double2*>(x),
-          reinterpret_cast<const double2*>(tmat), reinterpret_cast<double2*>(y), mode, err);
+          reinterpret_cast<const double2*>(tmat), reinterpret_cast<double2*>(y), mode, err));
     YASF_CUDA_TRY(cudaGetLastError());
   }
   return YASF_OK;
@@ -230,6 +234,10 @@ extern "C" const char* yasf_status_string(int status) {
 }
 
 extern "C" const char* yasf_last_cuda_error(void) { return g_last_error.c_str(); }
+
+extern "C" unsigned long long yasf_kernel_launches(void) {
+  return g_launches.load(std::memory_order_relaxed);
+}
 
 // Build the bundle streams from the dense a5/b5 table. The stream order is the one the
 // contraction kernel walks (yasf_common.cuh: bundle_stream_length).
@@ -461,7 +469,7 @@ extern "C" int yasf_scattering_bilinear(const yasf_plan* plan, int n_particles,
   const CouplingLayout lay = coupling_layout(plan, n_particles, YASF_C128);
   const double2* dots = reinterpret_cast<const double2*>(static_cast<char*>(workspace) +
                                                          lay.v_bytes + lay.partial_bytes);
-  final_sum_kernel<<<1, 256, 0, s>>>(1024, dots, out);
+  YASF_COUNTED(final_sum_kernel<<<1, 256, 0, s>>>(1024, dots, out));
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
 }
@@ -474,10 +482,10 @@ extern "C" int yasf_dotc(long long n, const double* a, const double* b, double* 
     return YASF_ERR_ALIGNMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double2* parts = static_cast<double2*>(workspace);
-  dotc_blocks_kernel<<<1024, 256, 0, s>>>(n, reinterpret_cast<const double2*>(a),
-                                           reinterpret_cast<const double2*>(b), parts);
+  YASF_COUNTED(dotc_blocks_kernel<<<1024, 256, 0, s>>>(n, reinterpret_cast<const double2*>(a),
+                                           reinterpret_cast<const double2*>(b), parts));
   YASF_CUDA_TRY(cudaGetLastError());
-  final_sum_kernel<<<1, 256, 0, s>>>(1024, parts, out);
+  YASF_COUNTED(final_sum_kernel<<<1, 256, 0, s>>>(1024, parts, out));
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
 }

@@ -32,6 +32,7 @@ struct yasf_plan {
 namespace yasf {
 
 void set_cuda_error(cudaError_t e);
+
 void set_error_text(const std::string& s);
 
 #define YASF_CUDA_TRY(expr)                   \

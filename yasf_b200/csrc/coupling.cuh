@@ -25,6 +25,10 @@
 
 namespace yasf {
 
+// Process-wide count of kernels launched by this library (instrumentation for benchmarks).
+void count_launch();
+#define YASF_COUNTED(...) (::yasf::count_launch(), (__VA_ARGS__))
+
 // Legendre recurrence constants (CELES form, yasfpy/functions/legendre_normalized_trigon.py:61-91)
 // live in plan-owned device memory, row stride YASF_PMAX_MAX + 1:
 //   Pn_{l+1}^m = alpha[l][m] ct Pn_l^m - beta[l][m] Pn_{l-1}^m,   Pn_m^m = start[m] st^m.

@@ -21,17 +21,17 @@ cudaError_t launch_contract<YASF_INST_L>(int precision, bool regular, const Cont
     e = cudaFuncSetAttribute(contract_kernel<L, double, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage64);
     if (e != cudaSuccess) return e;
-    contract_kernel<L, double, true><<<grid, threads, stage64, stream>>>(a);
+    YASF_COUNTED(contract_kernel<L, double, true><<<grid, threads, stage64, stream>>>(a));
   } else if (precision == YASF_C64) {
     e = cudaFuncSetAttribute(contract_kernel<L, float, false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage32);
     if (e != cudaSuccess) return e;
-    contract_kernel<L, float, false><<<grid, threads, stage32, stream>>>(a);
+    YASF_COUNTED(contract_kernel<L, float, false><<<grid, threads, stage32, stream>>>(a));
   } else {
     e = cudaFuncSetAttribute(contract_kernel<L, double, false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage64);
     if (e != cudaSuccess) return e;
-    contract_kernel<L, double, false><<<grid, threads, stage64, stream>>>(a);
+    YASF_COUNTED(contract_kernel<L, double, false><<<grid, threads, stage64, stream>>>(a));
   }
   return cudaGetLastError();
 }

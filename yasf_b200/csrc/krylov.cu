@@ -303,7 +303,7 @@ static int psolve(const Operator& op, int precision, const double2* x, double2* 
   if (op.pc)
     return yasf_precond_apply(op.pc, reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y),
                               1, n, precision, op.s);
-  copy_kernel<<<1024, 256, 0, op.s>>>(n, x, y);
+  YASF_COUNTED(copy_kernel<<<1024, 256, 0, op.s>>>(n, x, y));
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
 }
@@ -333,9 +333,9 @@ struct Counters {
 };
 
 static int norm_into(long long n, const double2* v, double2* part, double* dst, cudaStream_t s) {
-  mdot_kernel<<<kDotBlocks, 256, 0, s>>>(n, v, n, 1, v, part);
+  YASF_COUNTED(mdot_kernel<<<kDotBlocks, 256, 0, s>>>(n, v, n, 1, v, part));
   YASF_CUDA_TRY(cudaGetLastError());
-  mdot_final_kernel<<<1, 256, 0, s>>>(1, kDotBlocks, part, nullptr, 0, dst);
+  YASF_COUNTED(mdot_final_kernel<<<1, 256, 0, s>>>(1, kDotBlocks, part, nullptr, 0, dst));
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
 }
@@ -377,9 +377,9 @@ static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, 
     if ((st = op_apply(op, prec, x, t)) != YASF_OK) return st;
     cnt.mv_inner += (prec == YASF_C128) ? 0 : 1;
     cnt.mv64 += (prec == YASF_C128) ? 1 : 0;
-    sub_kernel<<<1024, 256, 0, s>>>(n, b, t, r);
+    YASF_COUNTED(sub_kernel<<<1024, 256, 0, s>>>(n, b, t, r));
   } else {
-    copy_kernel<<<1024, 256, 0, s>>>(n, b, r);
+    YASF_COUNTED(copy_kernel<<<1024, 256, 0, s>>>(n, b, r));
   }
   YASF_CUDA_TRY(cudaGetLastError());
   if ((st = norm_into(n, r, part, scal + SL_NORM, s)) != YASF_OK) return st;
@@ -396,8 +396,8 @@ static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, 
     // v0 = psolve(r) / ||.||
     if ((st = psolve(op, prec, r, Q, n)) != YASF_OK) return st;
     if ((st = norm_into(n, Q, part, scal + SL_NORM, s)) != YASF_OK) return st;
-    scale_kernel<<<1024, 256, 0, s>>>(n, Q, scal + SL_NORM, Q);
-    cycle_start_kernel<<<1, 256, 0, s>>>(m, S, scal);
+    YASF_COUNTED(scale_kernel<<<1024, 256, 0, s>>>(n, Q, scal + SL_NORM, Q));
+    YASF_COUNTED(cycle_start_kernel<<<1, 256, 0, s>>>(m, S, scal));
     YASF_CUDA_TRY(cudaGetLastError());
     bool breakdown = false;
     int col = 0;
@@ -410,19 +410,19 @@ static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, 
       if ((st = norm_into(n, w, part, scal + SL_H0, s)) != YASF_OK) return st;
       // CGS2: two projection sweeps
       for (int pass = 0; pass < 2; ++pass) {
-        mdot_kernel<<<kDotBlocks, 256, 0, s>>>(n, Q, n, col + 1, w, part);
-        mdot_final_kernel<<<col + 1, 256, 0, s>>>(col + 1, kDotBlocks, part, pass == 0 ? hcol : yv,
-                                                   0, nullptr);
-        update_kernel<<<1024, 256, 0, s>>>(n, Q, n, col + 1, pass == 0 ? hcol : yv, -1.0, w);
+        YASF_COUNTED(mdot_kernel<<<kDotBlocks, 256, 0, s>>>(n, Q, n, col + 1, w, part));
+        YASF_COUNTED(mdot_final_kernel<<<col + 1, 256, 0, s>>>(col + 1, kDotBlocks, part, pass == 0 ? hcol : yv,
+                                                   0, nullptr));
+        YASF_COUNTED(update_kernel<<<1024, 256, 0, s>>>(n, Q, n, col + 1, pass == 0 ? hcol : yv, -1.0, w));
         if (pass == 1) {
           // second-sweep coefficients are still in `part`: fold them into the column, h += h2
-          mdot_final_kernel<<<col + 1, 256, 0, s>>>(col + 1, kDotBlocks, part, hcol, 1, nullptr);
+          YASF_COUNTED(mdot_final_kernel<<<col + 1, 256, 0, s>>>(col + 1, kDotBlocks, part, hcol, 1, nullptr));
         }
         YASF_CUDA_TRY(cudaGetLastError());
       }
       if ((st = norm_into(n, w, part, scal + SL_H1, s)) != YASF_OK) return st;
-      scale_kernel<<<1024, 256, 0, s>>>(n, w, scal + SL_H1, Q + (size_t)(col + 1) * n);
-      givens_kernel<<<1, 1, 0, s>>>(col, m, H, gc, gs, S, scal, eps);
+      YASF_COUNTED(scale_kernel<<<1024, 256, 0, s>>>(n, w, scal + SL_H1, Q + (size_t)(col + 1) * n));
+      YASF_COUNTED(givens_kernel<<<1, 1, 0, s>>>(col, m, H, gc, gs, S, scal, eps));
       YASF_CUDA_TRY(cudaGetLastError());
       if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
       if (hs[SL_NONFINITE] != 0.0) return YASF_ERR_NOT_FINITE;
@@ -432,12 +432,12 @@ static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, 
       if (presid <= ptol || breakdown) break;
     }
     if (col == m) col = m - 1;
-    backsolve_kernel<<<1, 1, 0, s>>>(col, m, H, S, yv);
-    update_kernel<<<1024, 256, 0, s>>>(n, Q, n, col + 1, yv, 1.0, x);
+    YASF_COUNTED(backsolve_kernel<<<1, 1, 0, s>>>(col, m, H, S, yv));
+    YASF_COUNTED(update_kernel<<<1024, 256, 0, s>>>(n, Q, n, col + 1, yv, 1.0, x));
     YASF_CUDA_TRY(cudaGetLastError());
     if ((st = op_apply(op, prec, x, t)) != YASF_OK) return st;
     if (prec == YASF_C128) cnt.mv64++; else cnt.mv_inner++;
-    sub_kernel<<<1024, 256, 0, s>>>(n, b, t, r);
+    YASF_COUNTED(sub_kernel<<<1024, 256, 0, s>>>(n, b, t, r));
     YASF_CUDA_TRY(cudaGetLastError());
     if ((st = norm_into(n, r, part, scal + SL_NORM, s)) != YASF_OK) return st;
     if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
@@ -504,7 +504,7 @@ extern "C" int yasf_gmres_solve(const yasf_plan* plan, int n_particles, const do
   int info = 0;
   double rnorm = 0.0;
   if (bnrm2 == 0.0) {
-    copy_kernel<<<1024, 256, 0, s>>>(n, bb, xx);
+    YASF_COUNTED(copy_kernel<<<1024, 256, 0, s>>>(n, bb, xx));
     YASF_CUDA_TRY(cudaGetLastError());
     YASF_CUDA_TRY(cudaStreamSynchronize(s));
   } else if (inner_precision == YASF_C128) {
@@ -523,7 +523,7 @@ extern "C" int yasf_gmres_solve(const yasf_plan* plan, int n_particles, const do
     for (int it = 0;; ++it) {
       if ((st = op_apply(op, YASF_C128, xx, t)) != YASF_OK) return st;
       cnt.mv64++;
-      sub_kernel<<<1024, 256, 0, s>>>(n, bb, t, r);
+      YASF_COUNTED(sub_kernel<<<1024, 256, 0, s>>>(n, bb, t, r));
       YASF_CUDA_TRY(cudaGetLastError());
       if ((st = norm_into(n, r, part, scal + SL_NORM, s)) != YASF_OK) return st;
       if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
@@ -535,12 +535,12 @@ extern "C" int yasf_gmres_solve(const yasf_plan* plan, int n_particles, const do
       YASF_CUDA_TRY(cudaMemsetAsync(d, 0, n * sizeof(double2), s));
       // gmres_core overwrites r/t; keep the residual as the inner rhs in Q's last slot? use w.
       double2* rhs = reinterpret_cast<double2*>(ws + L.o_w);
-      copy_kernel<<<1024, 256, 0, s>>>(n, r, rhs);
+      YASF_COUNTED(copy_kernel<<<1024, 256, 0, s>>>(n, r, rhs));
       YASF_CUDA_TRY(cudaGetLastError());
       // rhs lives in w, which the core uses as scratch; move it to the tail of d's neighbour: use
       // the basis' last column as stable storage for the inner rhs.
       double2* rhs_store = reinterpret_cast<double2*>(ws + L.o_Q) + (size_t)m * n;
-      copy_kernel<<<1024, 256, 0, s>>>(n, rhs, rhs_store);
+      YASF_COUNTED(copy_kernel<<<1024, 256, 0, s>>>(n, rhs, rhs_store));
       YASF_CUDA_TRY(cudaGetLastError());
       int inner_info = 0;
       double inner_rn = 0.0;
@@ -549,7 +549,7 @@ extern "C" int yasf_gmres_solve(const yasf_plan* plan, int n_particles, const do
       st = gmres_core(op, L, ws, YASF_C64, rhs_store, d, rnorm, inner_atol,
                       std::max(1, m - 1), maxiter, false, cnt, &inner_info, &inner_rn);
       if (st != YASF_OK) return st;
-      add_kernel<<<1024, 256, 0, s>>>(n, d, xx);
+      YASF_COUNTED(add_kernel<<<1024, 256, 0, s>>>(n, d, xx));
       YASF_CUDA_TRY(cudaGetLastError());
       cnt.refine++;
     }

@@ -322,7 +322,7 @@ extern "C" int yasf_precond_assemble(yasf_precond* pc, const double* positions, 
     YASF_CUDA_TRY(cudaFuncSetAttribute(assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  assemble_kernel<<<pc->n_particles, 256, smem, s>>>(a);
+  YASF_COUNTED(assemble_kernel<<<pc->n_particles, 256, smem, s>>>(a));
   YASF_CUDA_TRY(cudaGetLastError());
   pc->assembled = true;
   pc->prepared = false;
@@ -348,7 +348,7 @@ extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
       return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
     }
   }
-  to_c64_kernel<<<2048, 256, 0, s>>>(pc->mat_elems, pc->d_mat, pc->d_mat32);
+  YASF_COUNTED(to_c64_kernel<<<2048, 256, 0, s>>>(pc->mat_elems, pc->d_mat, pc->d_mat32));
   YASF_CUDA_TRY(cudaGetLastError());
   pc->prepared = true;
   return YASF_OK;
@@ -366,17 +366,17 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int blocks = (pc->total_rows + 7) / 8;
   if (precision == YASF_C64)
-    apply_kernel<float2><<<blocks, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld,
+    YASF_COUNTED(apply_kernel<float2><<<blocks, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld,
                                                  pc->d_row_block, pc->d_row_local, pc->d_block_ptr,
                                                  pc->d_particles, pc->d_mat_off, pc->d_mat32,
                                                  reinterpret_cast<const double2*>(x),
-                                                 reinterpret_cast<double2*>(y));
+                                                 reinterpret_cast<double2*>(y)));
   else if (precision == YASF_C128)
-    apply_kernel<double2><<<blocks, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld,
+    YASF_COUNTED(apply_kernel<double2><<<blocks, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld,
                                                   pc->d_row_block, pc->d_row_local, pc->d_block_ptr,
                                                   pc->d_particles, pc->d_mat_off, pc->d_mat,
                                                   reinterpret_cast<const double2*>(x),
-                                                  reinterpret_cast<double2*>(y));
+                                                  reinterpret_cast<double2*>(y)));
   else
     return YASF_ERR_INVALID_ARGUMENT;
   YASF_CUDA_TRY(cudaGetLastError());
