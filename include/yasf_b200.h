@@ -33,7 +33,8 @@ enum yasf_status {
   YASF_ERR_OUT_OF_MEMORY = 5,    /* a device allocation made by the library failed */
   YASF_ERR_WORKSPACE = 6,        /* workspace smaller than the size query returned */
   YASF_ERR_NOT_FINITE = 7,       /* NaN/Inf in the right-hand side or the iteration */
-  YASF_ERR_NOT_PREPARED = 8      /* preconditioner used before prepare */
+  YASF_ERR_NOT_PREPARED = 8,     /* preconditioner used before prepare */
+  YASF_ERR_SCRATCH_LIMIT = 9     /* problem larger than the static scratch of the no-alloc call */
 };
 
 enum yasf_precision { YASF_C128 = 0, YASF_C64 = 1 };
@@ -79,6 +80,19 @@ int yasf_coupling_workspace_size(const yasf_plan* plan, int n_particles, int nrh
 int yasf_coupling_matvec(const yasf_plan* plan, int n_particles, const double* positions,
                          double k_medium, const double* x, double* y, int nrhs, long long ld,
                          int precision, void* workspace, size_t workspace_bytes, void* stream);
+
+/* No counterpart in the reference. For callers that cannot allocate device memory when they
+ * call (all device memory reserved at start-up, an embedding runtime that owns the allocator, or
+ * only fixed buffers to hand over): the same y = W x as yasf_coupling_matvec for one right-hand
+ * side, with all scratch in one static device array of YASF_STATIC_SCRATCH_BYTES, so nothing is
+ * allocated. Returns YASF_ERR_SCRATCH_LIMIT when yasf_coupling_workspace_size exceeds that size.
+ * All calls on a device share the array: calls that overlap on the GPU race, so order them on
+ * one stream. The first call on each device looks up the array (with that device current); make
+ * it before any stream capture. Every GPU that loads the library holds the array until exit. */
+#define YASF_STATIC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int yasf_coupling_matvec_noalloc(const yasf_plan* plan, int n_particles, const double* positions,
+                                 double k_medium, const double* x, double* y, int precision,
+                                 void* stream);
 
 /* y = x - T (.) (W x): the master operator of yasfpy/matrix_apply.py:66-120 fused into the
  * reduction epilogue. tmat is (n_particles*nmax) complex128: T[s,n] = mie[sidx[s], n, w]. */

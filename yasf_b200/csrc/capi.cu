@@ -229,6 +229,7 @@ extern "C" const char* yasf_status_string(int status) {
     case YASF_ERR_WORKSPACE: return "workspace too small";
     case YASF_ERR_NOT_FINITE: return "non-finite value";
     case YASF_ERR_NOT_PREPARED: return "preconditioner not prepared";
+    case YASF_ERR_SCRATCH_LIMIT: return "problem exceeds the static scratch of the no-alloc call";
     default: return "unknown status";
   }
 }

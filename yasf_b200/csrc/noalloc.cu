@@ -1,0 +1,74 @@
+// Coupling matvec for callers that must not allocate device memory.
+//
+// Some host programs cannot call cudaMalloc at the point where they want a matvec: a code that
+// reserves all of its device memory once at start-up and forbids allocation inside its time loop,
+// an embedding runtime that owns the CUDA allocator, or a caller that only hands out fixed
+// input/output buffers. yasf_coupling_matvec_noalloc computes the same y = W x as
+// yasf_coupling_matvec, but its scratch (the per-source V stream, the per-chunk partial sums and
+// the stage-timeout word) lives in one file-scope device array of YASF_STATIC_SCRATCH_BYTES, so
+// the call allocates nothing. The caller still passes the plan, positions, x and y.
+//
+// Limits and sharing:
+// - Problems whose scratch exceeds the array are rejected with YASF_ERR_SCRATCH_LIMIT before any
+//   device work (yasf_coupling_workspace_size gives the bytes a problem needs).
+// - Every call on a device uses the same array, which keeps the previous call's contents. The
+//   only word that must start at zero (the stage-timeout flag) is cleared by each call; the
+//   stream and partial sums are fully overwritten. Calls that overlap on the GPU (different
+//   streams, or different host threads on one device) race on the array and corrupt each other;
+//   order them on one stream.
+// - The first call on each device looks up the array's device address with that device current
+//   (cudaGetSymbolAddress, which may load the module); make that first call before any stream
+//   capture begins.
+#include <mutex>
+
+#include "capi_internal.h"
+
+namespace yasf {
+
+static __device__ __align__(256) unsigned char g_static_scratch[YASF_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_ptr[kMaxDevices] = {nullptr};
+
+// Device address of the static scratch for the current device (looked up once per device).
+int static_scratch(void** out) {
+  int dev = -1;
+  YASF_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return YASF_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    YASF_CUDA_TRY(cudaGetSymbolAddress(&p, g_static_scratch));
+    if (!p) return YASF_ERR_CUDA;
+    g_scratch_ptr[dev] = p;
+  }
+  *out = g_scratch_ptr[dev];
+  return YASF_OK;
+}
+}  // namespace
+
+}  // namespace yasf
+
+using namespace yasf;
+
+extern "C" int yasf_coupling_matvec_noalloc(const yasf_plan* plan, int n_particles,
+                                            const double* positions, double k_medium,
+                                            const double* x, double* y, int precision,
+                                            void* stream) {
+  int st = validate_coupling(plan, n_particles, positions, k_medium, precision);
+  if (st != YASF_OK) return st;
+  if (!x || !y || x == y) return YASF_ERR_INVALID_ARGUMENT;
+  if (!aligned16(x) || !aligned16(y)) return YASF_ERR_ALIGNMENT;
+  const size_t need = coupling_layout(plan, n_particles, precision).total;
+  if (need > (size_t)YASF_STATIC_SCRATCH_BYTES) {
+    set_error_text("problem needs more scratch than the static array holds");
+    return YASF_ERR_SCRATCH_LIMIT;
+  }
+  void* scratch = nullptr;
+  if ((st = static_scratch(&scratch)) != YASF_OK) return st;
+  return coupling_column(plan, n_particles, positions, k_medium, nullptr, x, y, precision, 0,
+                         scratch, (size_t)YASF_STATIC_SCRATCH_BYTES,
+                         static_cast<cudaStream_t>(stream));
+}
