@@ -101,6 +101,19 @@ int yasf_master_matvec(const yasf_plan* plan, int n_particles, const double* pos
                        long long ld, int precision, void* workspace, size_t workspace_bytes,
                        void* stream);
 
+/* ---- multi-right-hand-side panel on the tensor cores ----------------------------------------
+ * The batched form of the coupling matvec for R right-hand sides (incidence directions x
+ * polarisations), replacing the multi-channel particle_interaction loop
+ * (yasfpy/functions/cpu_numba.py:99-181) for the inner solves of the refined, batched GMRES:
+ * every pair block W_ij is generated once in complex64 and applied to the nmax x R panel of the
+ * source on tcgen05 tensor cores (TF32 inputs, FP32 accumulation). y = x - T (.) (W x) when tmat
+ * is non-NULL, else y = W x; columns are stored with leading dimension ld. lmax <= 6
+ * (YASF_ERR_UNSUPPORTED otherwise). */
+int yasf_panel_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, size_t* bytes);
+int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const double* positions,
+                      double k_medium, const double* tmat, const double* x, double* y, int nrhs,
+                      long long ld, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- cross sections (yasfpy/optics.py:55-156) ------------------------------------------------
  * out[0..1] (device) <- sum_{s,n} conj(b) (W_reg b), the bilinear form of
  * compute_scattering_cross_section (yasfpy/functions/cpu_numba.py:410-457): regular spherical

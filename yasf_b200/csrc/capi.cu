@@ -331,6 +331,26 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     }
   plan->pair_terms = (long long)pair_p.size();
 
+  // Direct-form terms for the tensor-core panel path: block a (tau1 = tau2 = 1) then block b
+  // (tau1 = 1, tau2 = 2), entry (n1', n2') = receiver/source mode inside one tau half.
+  const int H = L * (L + 2);
+  std::vector<int> w_ptr(1, 0);
+  std::vector<unsigned char> w_p;
+  std::vector<float2> w_coef;
+  for (int blk = 0; blk < 2; ++blk)
+    for (int q1 = 0; q1 < H; ++q1)
+      for (int q2 = 0; q2 < H; ++q2) {
+        for (int p = 0; p < P; ++p) {
+          double re, im;
+          A(q1, blk * H + q2, p, &re, &im);
+          if (re != 0.0 || im != 0.0) {
+            w_p.push_back((unsigned char)p);
+            w_coef.push_back(make_float2((float)re, (float)im));
+          }
+        }
+        w_ptr.push_back((int)w_p.size());
+      }
+
   // Legendre recurrence constants (CELES normalisation).
   LegendreTables leg;
   std::memset(&leg, 0, sizeof(leg));
@@ -360,6 +380,9 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     cudaFree(plan->d_pair_ptr);
     cudaFree(plan->d_pair_p);
     cudaFree(plan->d_pair_coef);
+    cudaFree(plan->d_w_ptr);
+    cudaFree(plan->d_w_p);
+    cudaFree(plan->d_w_coef);
     delete plan;
     return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
   };
@@ -379,6 +402,9 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
   YASF_UPLOAD(plan->d_pair_ptr, pair_ptr);
   YASF_UPLOAD(plan->d_pair_p, pair_p);
   YASF_UPLOAD(plan->d_pair_coef, pair_coef);
+  YASF_UPLOAD(plan->d_w_ptr, w_ptr);
+  YASF_UPLOAD(plan->d_w_p, w_p);
+  YASF_UPLOAD(plan->d_w_coef, w_coef);
 #undef YASF_UPLOAD
   if ((e = cudaMalloc(reinterpret_cast<void**>(&plan->d_leg), sizeof(LegendreTables))) != cudaSuccess)
     return fail(e);
@@ -397,6 +423,9 @@ extern "C" int yasf_plan_destroy(yasf_plan* plan) {
   cudaFree(plan->d_pair_ptr);
   cudaFree(plan->d_pair_p);
   cudaFree(plan->d_pair_coef);
+  cudaFree(plan->d_w_ptr);
+  cudaFree(plan->d_w_p);
+  cudaFree(plan->d_w_coef);
   delete plan;
   return YASF_OK;
 }

@@ -27,6 +27,11 @@ struct yasf_plan {
   int* d_pair_p = nullptr;        // p of each term
   double2* d_pair_coef = nullptr; // A[n2][n1][p]
   long long pair_terms = 0;
+  // direct-form generation terms of the tau blocks Wa (a5) and Wb (b5), CSR over
+  // (block, n1', n2') with n1', n2' < lmax*(lmax+2): order p and complex64 coefficient
+  int* d_w_ptr = nullptr;
+  unsigned char* d_w_p = nullptr;
+  float2* d_w_coef = nullptr;
 };
 
 namespace yasf {

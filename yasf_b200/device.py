@@ -152,6 +152,18 @@ class CouplingDevice:
                  _ptr(cols), _ptr(y), R, self.n, precision, _ptr(ws), wsb, s)
         return y.reshape(x.shape)
 
+    def panel(self, x: torch.Tensor, tmat: torch.Tensor | None = None, out: torch.Tensor | None = None):
+        """Tensor-core panel: (R, n) columns -> W x (or x - T W x), TF32 inputs, FP32 accumulation."""
+        cols = x.reshape(-1, self.n).contiguous()
+        R = cols.shape[0]
+        y = out if out is not None else torch.empty_like(cols)
+        nb = ctypes.c_size_t()
+        call("yasf_panel_workspace_size", self.plan.handle, self.n_particles, R, ctypes.byref(nb))
+        ws = self.ws.get(nb.value)
+        call("yasf_panel_matvec", self.plan.handle, self.n_particles, _ptr(self.pos), self.k, _ptr(tmat),
+             _ptr(cols), _ptr(y), R, self.n, _ptr(ws), nb.value, _stream_ptr())
+        return y.reshape(x.shape)
+
     def scattering_bilinear(self, b: torch.Tensor) -> complex:
         """sum conj(b) (W_reg b) with the regular (j_p) translation, self pairs included."""
         b = b.reshape(-1).contiguous()
