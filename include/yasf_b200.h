@@ -107,12 +107,34 @@ int yasf_master_matvec(const yasf_plan* plan, int n_particles, const double* pos
  * (yasfpy/functions/cpu_numba.py:99-181) for the inner solves of the refined, batched GMRES:
  * every pair block W_ij is generated once in complex64 and applied to the nmax x R panel of the
  * source on tcgen05 tensor cores (TF32 inputs, FP32 accumulation). y = x - T (.) (W x) when tmat
- * is non-NULL, else y = W x; columns are stored with leading dimension ld. lmax <= 6
+ * is non-NULL, else y = W x; x and y columns have leading dimensions ldx and ldy. lmax <= 6
  * (YASF_ERR_UNSUPPORTED otherwise). */
 int yasf_panel_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, size_t* bytes);
 int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const double* positions,
                       double k_medium, const double* tmat, const double* x, double* y, int nrhs,
-                      long long ld, void* workspace, size_t workspace_bytes, void* stream);
+                      long long ldx, long long ldy, void* workspace, size_t workspace_bytes,
+                      void* stream);
+
+/* ---- batched right-hand sides: refined lockstep GMRES -----------------------------------------
+ * (I - T W) X = B for nrhs columns (incidence directions x polarisations; the reference solves one
+ * incidence per Simulation, yasfpy/scattered_field_coefficients.py:95-144 with
+ * yasfpy/solver.py:108-121). Float64 iterative refinement: residuals B - A X in float64, inner
+ * left-preconditioned GMRES cycles (restart steps, each column its own float64 Krylov basis, all
+ * live columns sharing one operator application per step) to inner_rtol on the reduced-precision
+ * operator inner_kind: 0 tensor-core TF32 panel (lmax <= 6), 1 complex64 coupling kernel,
+ * 2 complex128 coupling kernel. X0 = 0. Columns leave when ||B_c - A X_c|| <= rtol ||B_c||.
+ * stats (host, may be NULL): [0] lockstep inner steps, [1] panel applications, [2] column
+ * applications of kinds 1/2, [3] float64 residual matvecs, [4] worst relative residual,
+ * [5] unconverged columns, [6] refinement steps. column_residuals (host, may be NULL): nrhs
+ * final relative residuals. Synchronous. */
+int yasf_batched_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, int restart,
+                                int inner_kind, size_t* bytes);
+int yasf_batched_solve(const yasf_plan* plan, int n_particles, const double* positions,
+                       double k_medium, const double* tmat, const yasf_precond* pc,
+                       const double* b, double* x, int nrhs, double rtol, int restart,
+                       int max_refine, double inner_rtol, int inner_kind, void* workspace,
+                       size_t workspace_bytes, double* stats, double* column_residuals,
+                       void* stream);
 
 /* ---- cross sections (yasfpy/optics.py:55-156) ------------------------------------------------
  * out[0..1] (device) <- sum_{s,n} conj(b) (W_reg b), the bilinear form of

@@ -66,7 +66,10 @@ SIGNATURES = {
     "yasf_master_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],
     "yasf_coupling_matvec_noalloc": [_vp, _i, _vp, _d, _vp, _vp, _i, _vp],
     "yasf_panel_workspace_size": [_vp, _i, _i, _c.POINTER(_sz)],
-    "yasf_panel_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _vp, _sz, _vp],
+    "yasf_panel_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _ll, _vp, _sz, _vp],
+    "yasf_batched_workspace_size": [_vp, _i, _i, _i, _i, _c.POINTER(_sz)],
+    "yasf_batched_solve": [_vp, _i, _vp, _d, _vp, _vp, _vp, _vp, _i, _d, _i, _i, _d, _i, _vp, _sz,
+                           _dp, _dp, _vp],
     "yasf_scattering_bilinear": [_vp, _i, _vp, _d, _vp, _vp, _vp, _sz, _vp],
     "yasf_dotc": [_ll, _vp, _vp, _vp, _vp, _sz, _vp],
     "yasf_precond_create": [_vp, _i, _i, _vp, _vp, _c.POINTER(_vp)],

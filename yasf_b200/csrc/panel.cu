@@ -49,14 +49,14 @@ extern "C" int yasf_panel_workspace_size(const yasf_plan* plan, int n_particles,
 
 extern "C" int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const double* positions,
                                  double k_medium, const double* tmat, const double* x, double* y,
-                                 int nrhs, long long ld, void* workspace, size_t workspace_bytes,
-                                 void* stream) {
+                                 int nrhs, long long ldx, long long ldy, void* workspace,
+                                 size_t workspace_bytes, void* stream) {
   int st = validate_coupling(plan, n_particles, positions, k_medium, YASF_C64);
   if (st != YASF_OK) return st;
   if (!x || !y || x == y || nrhs <= 0) return YASF_ERR_INVALID_ARGUMENT;
   const long long n = (long long)n_particles * plan->nmax;
-  if (nrhs == 1) ld = n;
-  if (ld < n) return YASF_ERR_INVALID_ARGUMENT;
+  if (nrhs == 1) ldx = ldy = n;
+  if (ldx < n || ldy < n) return YASF_ERR_INVALID_ARGUMENT;
   if (!aligned16(x) || !aligned16(y) || (tmat && !aligned16(tmat)) || !aligned16(workspace))
     return YASF_ERR_ALIGNMENT;
   size_t need = 0;
@@ -70,7 +70,8 @@ extern "C" int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const d
   pa.n_particles = n_particles;
   pa.nmax = plan->nmax;
   pa.nrhs = nrhs;
-  pa.ld = ld;
+  pa.ld = ldx;
+  pa.ldy = ldy;
   pa.k = k_medium;
   pa.pos = positions;
   pa.leg = plan->d_leg;

@@ -62,7 +62,8 @@ struct PanelArgs {
   int n_particles;
   int nmax;
   int nrhs;
-  long long ld;                  // column stride of x / y (elements)
+  long long ld;                  // column stride of x (elements)
+  long long ldy;                 // column stride of y (elements)
   double k;
   const double* pos;
   const LegendreTables* leg;
@@ -365,11 +366,11 @@ __global__ void __launch_bounds__(160, 1) panel_kernel(PanelArgs a) {
             yi = (double)v[2 * half + 1][u];
           }
           if (aborted || !ok) { yr = nan(""); yi = nan(""); }
-          const size_t gi = (size_t)col * a.ld + (size_t)i * a.nmax + nn;
+          const size_t gi = (size_t)col * a.ldy + (size_t)i * a.nmax + nn;
           double2 out;
           if (a.tmat) {
             const double2 tv = a.tmat[(size_t)i * a.nmax + nn];
-            const double2 xv = a.x[gi];
+            const double2 xv = a.x[(size_t)col * a.ld + (size_t)i * a.nmax + nn];
             out = make_double2(xv.x - (tv.x * yr - tv.y * yi), xv.y - (tv.x * yi + tv.y * yr));
           } else {
             out = make_double2(yr, yi);

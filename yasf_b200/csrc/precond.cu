@@ -172,8 +172,9 @@ __global__ void to_c64_kernel(size_t n, const double2* in, float2* out) {
     out[i] = make_float2((float)in[i].x, (float)in[i].y);
 }
 
-// y[rows of block] = Minv_B x[rows of block]; one warp per flattened row, up to 4 columns per pass.
-template <typename MT>
+// y[rows of block] = Minv_B x[rows of block]; one warp per flattened row. The row of the inverse
+// is streamed once per group of CPP columns (CPP = 16 when several right-hand sides are applied).
+template <typename MT, int CPP>
 __global__ void __launch_bounds__(256) apply_kernel(int total_rows, int nmax, int nrhs, long long ld,
                                                     const int* row_block, const int* row_local,
                                                     const int* block_ptr, const int* particles,
@@ -188,15 +189,17 @@ __global__ void __launch_bounds__(256) apply_kernel(int total_rows, int nmax, in
   const int dim = (block_ptr[b + 1] - p0) * nmax;
   const MT* row = mat + mat_off[b] + (size_t)i * dim;
   const int gi = particles[p0 + i / nmax] * nmax + i % nmax;
-  for (int c0 = 0; c0 < nrhs; c0 += 4) {
-    const int nc = min(4, nrhs - c0);
-    double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+  for (int c0 = 0; c0 < nrhs; c0 += CPP) {
+    const int nc = min(CPP, nrhs - c0);
+    double ar[CPP], ai[CPP];
+#pragma unroll
+    for (int q = 0; q < CPP; ++q) { ar[q] = 0.0; ai[q] = 0.0; }
     for (int c = lane; c < dim; c += 32) {
       const MT m = row[c];
       const double mr = (double)m.x, mi = (double)m.y;
       const int gc = particles[p0 + c / nmax] * nmax + c % nmax;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < CPP; ++q) {
         if (q < nc) {
           const double2 xv = x[(size_t)(c0 + q) * ld + gc];
           ar[q] += mr * xv.x - mi * xv.y;
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(256) apply_kernel(int total_rows, int nmax, in
       }
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < CPP; ++q) {
       for (int off = 16; off > 0; off >>= 1) {
         ar[q] += __shfl_down_sync(0xffffffffu, ar[q], off);
         ai[q] += __shfl_down_sync(0xffffffffu, ai[q], off);
@@ -365,20 +368,24 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
   if (!aligned16(x) || !aligned16(y)) return YASF_ERR_ALIGNMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int blocks = (pc->total_rows + 7) / 8;
-  if (precision == YASF_C64)
-    YASF_COUNTED(apply_kernel<float2><<<blocks, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld,
-                                                 pc->d_row_block, pc->d_row_local, pc->d_block_ptr,
-                                                 pc->d_particles, pc->d_mat_off, pc->d_mat32,
-                                                 reinterpret_cast<const double2*>(x),
-                                                 reinterpret_cast<double2*>(y)));
-  else if (precision == YASF_C128)
-    YASF_COUNTED(apply_kernel<double2><<<blocks, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld,
-                                                  pc->d_row_block, pc->d_row_local, pc->d_block_ptr,
-                                                  pc->d_particles, pc->d_mat_off, pc->d_mat,
-                                                  reinterpret_cast<const double2*>(x),
-                                                  reinterpret_cast<double2*>(y)));
-  else
+  const double2* xx = reinterpret_cast<const double2*>(x);
+  double2* yy = reinterpret_cast<double2*>(y);
+#define YASF_APPLY(MT, CPP, MAT)                                                                    \
+  YASF_COUNTED(apply_kernel<MT, CPP><<<blocks, 256, 0, s>>>(                                        \
+      pc->total_rows, pc->plan->nmax, nrhs, ld, pc->d_row_block, pc->d_row_local, pc->d_block_ptr, \
+      pc->d_particles, pc->d_mat_off, MAT, xx, yy))
+  if (precision == YASF_C64) {
+    if (nrhs == 1) YASF_APPLY(float2, 1, pc->d_mat32);
+    else if (nrhs <= 4) YASF_APPLY(float2, 4, pc->d_mat32);
+    else YASF_APPLY(float2, 16, pc->d_mat32);
+  } else if (precision == YASF_C128) {
+    if (nrhs == 1) YASF_APPLY(double2, 1, pc->d_mat);
+    else if (nrhs <= 4) YASF_APPLY(double2, 4, pc->d_mat);
+    else YASF_APPLY(double2, 16, pc->d_mat);
+  } else {
     return YASF_ERR_INVALID_ARGUMENT;
+  }
+#undef YASF_APPLY
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
 }

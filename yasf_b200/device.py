@@ -161,8 +161,35 @@ class CouplingDevice:
         call("yasf_panel_workspace_size", self.plan.handle, self.n_particles, R, ctypes.byref(nb))
         ws = self.ws.get(nb.value)
         call("yasf_panel_matvec", self.plan.handle, self.n_particles, _ptr(self.pos), self.k, _ptr(tmat),
-             _ptr(cols), _ptr(y), R, self.n, _ptr(ws), nb.value, _stream_ptr())
+             _ptr(cols), _ptr(y), R, self.n, self.n, _ptr(ws), nb.value, _stream_ptr())
         return y.reshape(x.shape)
+
+    INNER_KINDS = {"tf32": 0, "c64": 1, "c128": 2}
+
+    def batched_solve(self, tmat: torch.Tensor, B: torch.Tensor, rtol: float, restart: int = 50,
+                      max_refine: int = 8, inner_rtol: float = 1e-3, inner: str = "tf32",
+                      precond=None) -> tuple[torch.Tensor, dict]:
+        """Refined lockstep GMRES for the columns of B (R, n); returns (X, stats)."""
+        cols = B.reshape(-1, self.n).contiguous()
+        R = cols.shape[0]
+        kind = self.INNER_KINDS[inner]
+        restart = int(max(1, min(restart, 512, self.n)))
+        nb = ctypes.c_size_t()
+        call("yasf_batched_workspace_size", self.plan.handle, self.n_particles, R, restart, kind,
+             ctypes.byref(nb))
+        ws = self.ws.get(nb.value)
+        X = torch.empty_like(cols)
+        stats = (ctypes.c_double * 8)()
+        colres = (ctypes.c_double * R)()
+        pc = precond.handle if precond is not None else ctypes.c_void_p(0)
+        call("yasf_batched_solve", self.plan.handle, self.n_particles, _ptr(self.pos), self.k, _ptr(tmat), pc,
+             _ptr(cols), _ptr(X), R, float(rtol), restart, int(max_refine), float(inner_rtol), kind,
+             _ptr(ws), nb.value, stats, colres, _stream_ptr())
+        info = {"inner_steps": int(stats[0]), "panel_matvecs": int(stats[1]),
+                "column_matvecs": int(stats[2]), "matvecs_f64": int(stats[3]),
+                "worst_relative_residual": float(stats[4]), "unconverged": int(stats[5]),
+                "refinement_steps": int(stats[6]), "column_residuals": list(colres)}
+        return X.reshape(B.shape), info
 
     def scattering_bilinear(self, b: torch.Tensor) -> complex:
         """sum conj(b) (W_reg b) with the regular (j_p) translation, self pairs included."""
