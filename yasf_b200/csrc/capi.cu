@@ -331,25 +331,17 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     }
   plan->pair_terms = (long long)pair_p.size();
 
-  // Direct-form terms for the tensor-core panel path: block a (tau1 = tau2 = 1) then block b
-  // (tau1 = 1, tau2 = 2), entry (n1', n2') = receiver/source mode inside one tau half.
-  const int H = L * (L + 2);
-  std::vector<int> w_ptr(1, 0);
-  std::vector<unsigned char> w_p;
-  std::vector<float2> w_coef;
-  for (int blk = 0; blk < 2; ++blk)
-    for (int q1 = 0; q1 < H; ++q1)
-      for (int q2 = 0; q2 < H; ++q2) {
-        for (int p = 0; p < P; ++p) {
-          double re, im;
-          A(q1, blk * H + q2, p, &re, &im);
-          if (re != 0.0 || im != 0.0) {
-            w_p.push_back((unsigned char)p);
-            w_coef.push_back(make_float2((float)re, (float)im));
-          }
-        }
-        w_ptr.push_back((int)w_p.size());
-      }
+  // Generation terms for the tensor-core panel path (lmax <= 6).
+  std::vector<float> gen_c1;
+  std::vector<unsigned> gen_meta;
+  {
+    const int bst = panel_build_terms(L, ab5, gen_c1, gen_meta);
+    if (bst != YASF_OK) {
+      delete plan;
+      set_error_text("internal: panel generation terms do not fit");
+      return bst;
+    }
+  }
 
   // Legendre recurrence constants (CELES normalisation).
   LegendreTables leg;
@@ -380,9 +372,8 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     cudaFree(plan->d_pair_ptr);
     cudaFree(plan->d_pair_p);
     cudaFree(plan->d_pair_coef);
-    cudaFree(plan->d_w_ptr);
-    cudaFree(plan->d_w_p);
-    cudaFree(plan->d_w_coef);
+    cudaFree(plan->d_gen_c1);
+    cudaFree(plan->d_gen_meta);
     delete plan;
     return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
   };
@@ -402,9 +393,10 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
   YASF_UPLOAD(plan->d_pair_ptr, pair_ptr);
   YASF_UPLOAD(plan->d_pair_p, pair_p);
   YASF_UPLOAD(plan->d_pair_coef, pair_coef);
-  YASF_UPLOAD(plan->d_w_ptr, w_ptr);
-  YASF_UPLOAD(plan->d_w_p, w_p);
-  YASF_UPLOAD(plan->d_w_coef, w_coef);
+  if (!gen_c1.empty()) {
+    YASF_UPLOAD(plan->d_gen_c1, gen_c1);
+    YASF_UPLOAD(plan->d_gen_meta, gen_meta);
+  }
 #undef YASF_UPLOAD
   if ((e = cudaMalloc(reinterpret_cast<void**>(&plan->d_leg), sizeof(LegendreTables))) != cudaSuccess)
     return fail(e);
@@ -423,9 +415,8 @@ extern "C" int yasf_plan_destroy(yasf_plan* plan) {
   cudaFree(plan->d_pair_ptr);
   cudaFree(plan->d_pair_p);
   cudaFree(plan->d_pair_coef);
-  cudaFree(plan->d_w_ptr);
-  cudaFree(plan->d_w_p);
-  cudaFree(plan->d_w_coef);
+  cudaFree(plan->d_gen_c1);
+  cudaFree(plan->d_gen_meta);
   delete plan;
   return YASF_OK;
 }

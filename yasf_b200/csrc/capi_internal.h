@@ -27,11 +27,10 @@ struct yasf_plan {
   int* d_pair_p = nullptr;        // p of each term
   double2* d_pair_coef = nullptr; // A[n2][n1][p]
   long long pair_terms = 0;
-  // direct-form generation terms of the tau blocks Wa (a5) and Wb (b5), CSR over
-  // (block, n1', n2') with n1', n2' < lmax*(lmax+2): order p and complex64 coefficient
-  int* d_w_ptr = nullptr;
-  unsigned char* d_w_p = nullptr;
-  float2* d_w_coef = nullptr;
+  // direct-form generation terms of the tau blocks Wa (a5) and Wb (b5) for the tensor-core panel,
+  // one fixed list per generator thread ([term][thread]); null when lmax > 6
+  float* d_gen_c1 = nullptr;
+  unsigned* d_gen_meta = nullptr;
 };
 
 namespace yasf {
@@ -76,5 +75,7 @@ int dispatch_contract(int lmax, int precision, bool regular, const ContractArgs&
 
 int validate_coupling(const yasf_plan* plan, int n_particles, const double* positions,
                       double k, int precision);
+
+int panel_build_terms(int L, const double* ab5, std::vector<float>& c1, std::vector<unsigned>& meta);
 
 }  // namespace yasf

@@ -1,8 +1,78 @@
 // C-ABI entry points of the multi-right-hand-side tensor-core coupling (see panel.cuh).
+#include <algorithm>
+#include <cmath>
+
 #include "capi_internal.h"
 #include "panel.cuh"
 
 namespace yasf {
+
+// Generation terms of the W blocks for the panel kernel, balanced over the 256 generator threads
+// (longest-processing-time assignment of whole entries) and laid out [term][thread].
+int panel_build_terms(int L, const double* ab5, std::vector<float>& c1, std::vector<unsigned>& meta) {
+  c1.clear();
+  meta.clear();
+  if (L < 1 || L > 6) return YASF_OK;  // no tensor-core panel beyond lmax 6
+  const int nmax = 2 * L * (L + 2), P = 2 * L + 1, DW = 4 * L + 1;
+  const int H = L * (L + 2), HP = pad8(H);
+  const int W_PLANE_F = (HP / 4) * (HP / 8) * 128 / 4;
+  const int TM = gen_terms_max(L);
+  auto m_of = [](int q) {
+    int l = 1;
+    while ((l + 1) * (l + 1) - 1 <= q) ++l;
+    return q + 1 - l * l - l;
+  };
+  struct Term { float c; unsigned meta; };
+  std::vector<std::vector<Term>> entries;
+  double cmax = 0.0;  // terms below 1e-12 of the largest coefficient cannot change a TF32 entry
+  for (size_t q = 0; q < (size_t)nmax * nmax * P * 2; ++q) cmax = std::max(cmax, std::fabs(ab5[q]));
+  const double cut = 1e-12 * cmax;
+  for (int which = 0; which < 2; ++which)
+    for (int q1 = 0; q1 < H; ++q1)
+      for (int q2 = 0; q2 < H; ++q2) {
+        std::vector<Term> ts;
+        const int delta = m_of(q2) - m_of(q1) + 2 * L;
+        const unsigned dst = (unsigned)(which * 2 * W_PLANE_F + kmajor_offset(q1, q2, HP) / 4);
+        for (int p = 0; p < P; ++p) {
+          // coefficient A[(tau1=1,q1), (tau2=which+1,q2), p] = translation_ab5[n2][n1][p]
+          const size_t idx = ((size_t)(which * H + q2) * nmax + q1) * P + p;
+          double cr = ab5[2 * idx], ci = ab5[2 * idx + 1];
+          if (std::fabs(cr) <= cut) cr = 0.0;
+          if (std::fabs(ci) <= cut) ci = 0.0;
+          if (cr == 0.0 && ci == 0.0) continue;
+          if (cr != 0.0 && ci != 0.0) return YASF_ERR_INVALID_ARGUMENT;  // not real x i^k
+          const bool odd = cr == 0.0;
+          Term t;
+          t.c = (float)(odd ? -ci : cr);
+          t.meta = (unsigned)(p * DW + delta) | (odd ? kMetaOdd : 0u);
+          ts.push_back(t);
+        }
+        if (ts.empty()) continue;
+        ts.front().meta |= kMetaFirst;
+        ts.back().meta |= kMetaLast | (dst << 13);
+        entries.push_back(ts);
+      }
+  std::vector<int> order(entries.size());
+  for (size_t e = 0; e < entries.size(); ++e) order[e] = (int)e;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return entries[x].size() > entries[y].size(); });
+  std::vector<std::vector<Term>> per(kGenThreads);
+  for (int e : order) {
+    int best = 0;
+    for (int th = 1; th < kGenThreads; ++th)
+      if (per[th].size() < per[best].size()) best = th;
+    per[best].insert(per[best].end(), entries[e].begin(), entries[e].end());
+    if ((int)per[best].size() > TM) return YASF_ERR_UNSUPPORTED;
+  }
+  c1.assign((size_t)TM * kGenThreads, 0.f);
+  meta.assign((size_t)TM * kGenThreads, 0u);
+  for (int th = 0; th < kGenThreads; ++th)
+    for (size_t t = 0; t < per[th].size(); ++t) {
+      c1[t * kGenThreads + th] = per[th][t].c;
+      meta[t * kGenThreads + th] = per[th][t].meta;
+    }
+  return YASF_OK;
+}
 
 template <int L>
 static int launch_panel(const PanelArgs& pa, int groups, cudaStream_t s) {
@@ -16,7 +86,7 @@ static int launch_panel(const PanelArgs& pa, int groups, cudaStream_t s) {
   YASF_CUDA_TRY(cudaFuncSetAttribute(panel_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      G::SMEM));
   const dim3 grid(pa.n_particles, groups);
-  YASF_COUNTED(panel_kernel<L><<<grid, 160, G::SMEM, s>>>(pa));
+  YASF_COUNTED(panel_kernel<L><<<grid, kPanelThreads, G::SMEM, s>>>(pa));
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
 }
@@ -76,9 +146,9 @@ extern "C" int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const d
   pa.pos = positions;
   pa.leg = plan->d_leg;
   pa.xp = reinterpret_cast<const float*>(ws);
-  pa.w_ptr = plan->d_w_ptr;
-  pa.w_p = plan->d_w_p;
-  pa.w_coef = plan->d_w_coef;
+  if (!plan->d_gen_c1) return YASF_ERR_UNSUPPORTED;
+  pa.gen_c1 = plan->d_gen_c1;
+  pa.gen_meta = plan->d_gen_meta;
   pa.x = reinterpret_cast<const double2*>(x);
   pa.tmat = reinterpret_cast<const double2*>(tmat);
   pa.y = reinterpret_cast<double2*>(y);

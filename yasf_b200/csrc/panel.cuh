@@ -44,6 +44,7 @@ struct PanelGeom {
   static constexpr int G_STAGE = P * DW * 8;    // pair table (float2)
   static constexpr int TMEM_COLS = 4 * HP <= 32 ? 32 : (4 * HP <= 64 ? 64 : (4 * HP <= 128 ? 128 : 256));
   static constexpr int SMEM = 2 * X_STAGE + 2 * W_STAGE + 2 * G_STAGE + 256;
+  static constexpr int W_PLANE_F = W_PLANE / 4;
 };
 
 // Byte offset of element (row, k) in a canonical K-major no-swizzle operand with `rows` rows.
@@ -68,9 +69,8 @@ struct PanelArgs {
   const double* pos;
   const LegendreTables* leg;
   const float* xp;               // source panels, [group][source][X_STAGE bytes]
-  const int* w_ptr;              // [2*H*H + 1] term lists of the a (first H*H) and b entries
-  const unsigned char* w_p;      // order p of each term
-  const float2* w_coef;          // complex coefficient of each term
+  const float* gen_c1;           // [TM][256] generation coefficients, thread-minor
+  const unsigned* gen_meta;      // [TM][256] generation meta words
   const double2* x;              // input columns (for the master epilogue)
   const double2* tmat;           // T (N*nmax), master epilogue when non-null
   double2* y;                    // output columns
@@ -144,47 +144,70 @@ __device__ __forceinline__ bool wait_or_abort(unsigned long long* bar, unsigned 
 }
 
 // ---- the kernel ---------------------------------------------------------------------------
+// Threads: warps 0-7 generate W (256 threads, each with a fixed, register-resident list of
+// generation terms: coefficient, pair-table offset, rotation, first/last flags, destination);
+// warps 0-3 also read the accumulators at the end. Warp 8 owns tensor memory and issues the
+// MMAs. Warp 9 issues the source-panel copies and computes the pair table one pair ahead.
+constexpr int kGenThreads = 256;
+constexpr int kPanelThreads = 320;
+__host__ __device__ constexpr int gen_terms_max(int L) {
+  return L <= 1 ? 2 : (L == 2 ? 4 : (L == 3 ? 8 : (L == 4 ? 12 : (L == 5 ? 28 : 56))));
+}
+// meta word: [0,10) pair-table offset, 10 rotate (multiply by i), 11 first term of an entry,
+// 12 last term of an entry, [13,32) destination float index in the W stage (real part; the
+// imaginary part is one plane further).
+constexpr unsigned kMetaOdd = 1u << 10, kMetaFirst = 1u << 11, kMetaLast = 1u << 12;
+
 template <int L>
-__global__ void __launch_bounds__(160, 1) panel_kernel(PanelArgs a) {
+__global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   using G = PanelGeom<L>;
   constexpr int H = G::H, HP = G::HP, M = G::M, P = G::P, DW = G::DW;
+  constexpr int TM = gen_terms_max(L);
+  constexpr int PW = G::W_PLANE / 4;  // floats per W plane
   extern __shared__ __align__(1024) unsigned char panel_smem[];
-  unsigned char* xs = panel_smem;                             // [2][X_STAGE]
-  unsigned char* ws = xs + 2 * G::X_STAGE;                    // [2][W_STAGE]
+  unsigned char* xs = panel_smem;                               // [2][X_STAGE]
+  unsigned char* ws = xs + 2 * G::X_STAGE;                      // [2][W_STAGE]
   float2* gt = reinterpret_cast<float2*>(ws + 2 * G::W_STAGE);  // [2][P*DW]
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(
       reinterpret_cast<unsigned char*>(gt) + 2 * G::G_STAGE);
-  unsigned long long* full_x = bars;      // [2]
-  unsigned long long* full_w = bars + 2;  // [2]
-  unsigned long long* empty = bars + 4;   // [2]
-  unsigned long long* accum = bars + 6;   // [1]
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 8);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 9);
-  volatile int* gen_stop = reinterpret_cast<volatile int*>(bars + 10);  // written by thread 0 only
-  volatile int* last_issued = reinterpret_cast<volatile int*>(bars + 11);
-  __shared__ signed char m_of[96];
+  unsigned long long* xfull = bars;       // [2] source panel landed
+  unsigned long long* wfull = bars + 2;   // [2] W generated
+  unsigned long long* empty = bars + 4;   // [2] MMAs of the stage done (X and W reusable)
+  unsigned long long* gfull = bars + 6;   // [2] pair table ready
+  unsigned long long* gempty = bars + 8;  // [2] pair table consumed
+  unsigned long long* accum = bars + 10;  // accumulators final
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 12);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 13);
+  volatile int* gen_stop = reinterpret_cast<volatile int*>(bars + 14);
+  volatile int* last_issued = reinterpret_cast<volatile int*>(bars + 15);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int i = blockIdx.x;      // receiving sphere
-  const int grp = blockIdx.y;    // right-hand-side group of 64
+  const int i = blockIdx.x;    // receiving sphere
+  const int grp = blockIdx.y;  // right-hand-side group of 64
   const int N = a.n_particles;
+  const int n_iter = N - 1;    // every source but the receiver itself
 
-  // zero both W stages once (padding rows/columns stay zero), mode table, barriers
+  // generation terms of this thread (registers)
+  float gc[TM];
+  unsigned gm[TM];
+  if (tid < kGenThreads) {
+#pragma unroll
+    for (int t = 0; t < TM; ++t) {
+      gc[t] = __ldg(a.gen_c1 + t * kGenThreads + tid);
+      gm[t] = __ldg(a.gen_meta + t * kGenThreads + tid);
+    }
+  }
   for (int o = tid; o < (2 * G::W_STAGE) / 16; o += blockDim.x)
     reinterpret_cast<float4*>(ws)[o] = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int q = tid; q < H; q += blockDim.x) {
-    const int l = (int)floorf(sqrtf((float)q + 1.0f) + 1e-4f);
-    m_of[q] = (signed char)(q + 1 - l * l - l);
-  }
   if (tid == 0) {
-    for (int b = 0; b < 7; ++b) mbar_init(&bars[b], 1);
+    for (int b = 0; b < 11; ++b) mbar_init(&bars[b], 1);
     *abort_flag = 0;
     *gen_stop = 0;
     *last_issued = -1;
     mbar_fence_init();
   }
-  if (warp == 4) {  // tensor memory for the four accumulators (Y1r, Y1i, Y2r, Y2i)
+  if (warp == 8) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(tmem_slot)),
                  "r"(G::TMEM_COLS)
@@ -196,133 +219,80 @@ __global__ void __launch_bounds__(160, 1) panel_kernel(PanelArgs a) {
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
-  const int n_iter = N - 1;  // every source but the receiver itself
 
-  if (warp < 4) {
-    // ===================== generators =====================
-    const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
+  if (warp < 8) {
+    // ===================== W generation =====================
     for (int t = 0; t < n_iter; ++t) {
       const int s = t & 1;
-      const int j = t < i ? t : t + 1;
-      // Only thread 0 waits for the stage to drain; the decision reaches the other generators
-      // through gen_stop after the named barrier, so all 128 leave the loop together.
+      const unsigned k = (unsigned)(t >> 1);
       if (tid == 0) {
-        if (t >= 2 && !wait_or_abort(&empty[s], (unsigned)(((t >> 1) - 1) & 1), abort_flag)) {
-          *gen_stop = 1;
-        } else {
-          const unsigned char* src =
-              reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)grp * N + j) * G::X_STAGE;
-          bulk_load(xs + s * G::X_STAGE, src, G::X_STAGE, &full_x[s]);
-          *last_issued = t;
-        }
+        bool ok = t < 2 || wait_or_abort(&empty[s], (k - 1) & 1, abort_flag);
+        ok = ok && wait_or_abort(&gfull[s], k & 1, abort_flag);
+        if (!ok) *gen_stop = 1;
       }
-      named_sync(1, 128);
+      named_sync(1, kGenThreads);
       if (*gen_stop) break;
-      // pair table: lane d of warp 0 handles |delta| = d
-      float2* g = gt + s * (P * DW);
-      if (warp == 0 && lane < P) {
-        const int d = lane;
-        const double dx = xi - a.pos[3 * j], dy = yi - a.pos[3 * j + 1], dz = zi - a.pos[3 * j + 2];
-        const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        double ct = dz / r;
-        ct = fmin(1.0, fmax(-1.0, ct));
-        const double st = sqrt(1.0 - ct * ct);
-        const double rho = sqrt(dx * dx + dy * dy);
-        const double phi = (rho > 0.0) ? atan2(dy, dx) : 0.0;
-        double sdp, cdp;
-        sincos(d * phi, &sdp, &cdp);
-        const double x = a.k * r;
-        double sx, cx;
-        sincos(x, &sx, &cx);
-        const double ix = 1.0 / x;
-        double hr0 = sx * ix, hi0 = -cx * ix;
-        double hr1 = (sx - x * cx) * ix * ix, hi1 = -(cx + x * sx) * ix * ix;
-        // advance the Hankel recurrence to order d
-        for (int q = 0; q < d; ++q) {
-          const double f = (2 * q + 3) * ix;
-          const double nr = f * hr1 - hr0, ni = f * hi1 - hi0;
-          hr0 = hr1; hi0 = hi1; hr1 = nr; hi1 = ni;
+      const float2* g = gt + s * (P * DW);
+      float* wst = reinterpret_cast<float*>(ws + s * G::W_STAGE);
+      float ar = 0.f, ai = 0.f;
+#pragma unroll
+      for (int q = 0; q < TM; ++q) {
+        const unsigned mt = gm[q];
+        const float2 gv = g[mt & 1023u];
+        const bool odd = (mt & kMetaOdd) != 0;
+        const float av = odd ? gv.y : gv.x;
+        const float bv = odd ? -gv.x : gv.y;
+        if (mt & kMetaFirst) { ar = 0.f; ai = 0.f; }
+        ar = fmaf(gc[q], av, ar);
+        ai = fmaf(gc[q], bv, ai);
+        if (mt & kMetaLast) {
+          const unsigned dst = mt >> 13;
+          wst[dst] = to_tf32(ar);
+          wst[dst + PW] = to_tf32(ai);
         }
-        double stp = 1.0;
-        for (int q = 0; q < d; ++q) stp *= st;
-        double Pp = 0.0, Pc = a.leg->start[d] * stp;
-        for (int p = d; p < P; ++p) {
-          const double gr = Pc * hr0, gi = Pc * hi0;
-          g[p * DW + (2 * L + d)] = make_float2((float)(gr * cdp - gi * sdp), (float)(gr * sdp + gi * cdp));
-          g[p * DW + (2 * L - d)] = make_float2((float)(gr * cdp + gi * sdp), (float)(gi * cdp - gr * sdp));
-          if (p + 1 < P) {
-            const double Pn = a.leg->alpha[p * kLegStride + d] * ct * Pc - a.leg->beta[p * kLegStride + d] * Pp;
-            Pp = Pc;
-            Pc = Pn;
-            const double f = (2 * p + 3) * ix;
-            const double nr = f * hr1 - hr0, ni = f * hi1 - hi0;
-            hr0 = hr1; hi0 = hi1; hr1 = nr; hi1 = ni;
-          }
-        }
-      }
-      named_sync(1, 128);
-      // W entries: a block (e < H*H) and b block, row n1' (receiver), column n2' (source)
-      unsigned char* wst = ws + s * G::W_STAGE;
-      for (int e = tid; e < 2 * H * H; e += 128) {
-        const int which = e >= H * H;
-        const int ee = e - which * H * H;
-        const int n1 = ee / H, n2 = ee - (ee / H) * H;
-        const int col = m_of[n2] - m_of[n1] + 2 * L;
-        float wr = 0.f, wi = 0.f;
-        const int t0 = __ldg(a.w_ptr + e), t1 = __ldg(a.w_ptr + e + 1);
-        for (int q = t0; q < t1; ++q) {
-          const float2 c = __ldg(a.w_coef + q);
-          const float2 gv = g[__ldg(a.w_p + q) * DW + col];
-          wr = fmaf(c.x, gv.x, wr);
-          wr = fmaf(-c.y, gv.y, wr);
-          wi = fmaf(c.x, gv.y, wi);
-          wi = fmaf(c.y, gv.x, wi);
-        }
-        const int off = kmajor_offset(n1, n2, HP);
-        *reinterpret_cast<float*>(wst + (2 * which) * G::W_PLANE + off) = to_tf32(wr);
-        *reinterpret_cast<float*>(wst + (2 * which + 1) * G::W_PLANE + off) = to_tf32(wi);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      named_sync(1, 128);
-      if (tid == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&full_w[s])) : "memory");
+      named_sync(1, kGenThreads);
+      if (tid == 0) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&wfull[s])) : "memory");
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&gempty[s])) : "memory");
+      }
     }
-  } else {
-    // ===================== MMA issuer (one thread of warp 4) =====================
+  } else if (warp == 8) {
+    // ===================== MMA issuer =====================
     if (lane == 0) {
-      constexpr int KS = HP / 8;  // K steps of 8 (tf32)
-      const unsigned idesc = umma_idesc_tf32(M, HP, false);
-      const unsigned idesc_neg = umma_idesc_tf32(M, HP, true);
-      const unsigned xbase = smem_addr(xs), wbase = smem_addr(ws);
+      constexpr int KS = HP / 8;
+      constexpr unsigned idesc = umma_idesc_tf32(M, HP, false);
+      constexpr unsigned idesc_neg = umma_idesc_tf32(M, HP, true);
+      unsigned long long dx0[4], dw0[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        dx0[q] = umma_desc(smem_addr(xs) + q * G::X_PLANE, G::X_LBO, 128);
+        dw0[q] = umma_desc(smem_addr(ws) + q * G::W_PLANE, G::W_LBO, 128);
+      }
+      constexpr unsigned long long xs_step = (unsigned long long)(G::X_STAGE >> 4);
+      constexpr unsigned long long ws_step = (unsigned long long)(G::W_STAGE >> 4);
+      constexpr unsigned long long xk = (unsigned long long)((2 * G::X_LBO) >> 4);
+      constexpr unsigned long long wk = (unsigned long long)((2 * G::W_LBO) >> 4);
       for (int t = 0; t < n_iter; ++t) {
         const int s = t & 1;
         const unsigned ph = (unsigned)((t >> 1) & 1);
-        if (!wait_or_abort(&full_x[s], ph, abort_flag)) break;
-        if (!wait_or_abort(&full_w[s], ph, abort_flag)) break;
+        if (!wait_or_abort(&xfull[s], ph, abort_flag)) break;
+        if (!wait_or_abort(&wfull[s], ph, abort_flag)) break;
         tc_fence_after();
-        const unsigned xb = xbase + s * G::X_STAGE, wb = wbase + s * G::W_STAGE;
-        // planes: X: 0 X1r, 1 X1i, 2 X2r, 3 X2i ; W: 0 War, 1 Wai, 2 Wbr, 3 Wbi
-        // out regions (TMEM columns): 0 Y1r, 1 Y1i, 2 Y2r, 3 Y2i
-        // Y1 = Wa X1 + Wb X2 ; Y2 = Wb X1 + Wa X2 ; (Xr + i Xi)(Wr + i Wi)
-        struct Term { int xpl, wpl, out, neg; };
-        const Term terms[16] = {
-            {0, 0, 0, 0}, {1, 1, 0, 1}, {2, 2, 0, 0}, {3, 3, 0, 1},   // Y1r
-            {0, 1, 1, 0}, {1, 0, 1, 0}, {2, 3, 1, 0}, {3, 2, 1, 0},   // Y1i
-            {0, 2, 2, 0}, {1, 3, 2, 1}, {2, 0, 2, 0}, {3, 1, 2, 1},   // Y2r
-            {0, 3, 3, 0}, {1, 2, 3, 0}, {2, 1, 3, 0}, {3, 0, 3, 0}};  // Y2i
-#pragma unroll 1
+        // (x plane, w plane, accumulator region, negate A): Y1 = Wa X1 + Wb X2, Y2 = Wb X1 + Wa X2
+        constexpr int XP[16] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3};
+        constexpr int WP[16] = {0, 1, 2, 3, 1, 0, 3, 2, 2, 3, 0, 1, 3, 2, 1, 0};
+        constexpr int NG[16] = {0, 1, 0, 1, 0, 0, 0, 0, 0, 1, 0, 1, 0, 0, 0, 0};
+#pragma unroll
         for (int q = 0; q < 16; ++q) {
-          const Term tm = terms[q];
-          const unsigned dcol = tmem + (unsigned)(tm.out * HP);
-          const unsigned id = tm.neg ? idesc_neg : idesc;
-#pragma unroll 1
+          const unsigned dcol = tmem + (unsigned)((q >> 2) * HP);
+          const unsigned long long da0 = dx0[XP[q]] + (unsigned long long)s * xs_step;
+          const unsigned long long db0 = dw0[WP[q]] + (unsigned long long)s * ws_step;
+#pragma unroll
           for (int kk = 0; kk < KS; ++kk) {
-            const unsigned long long da =
-                umma_desc(xb + tm.xpl * G::X_PLANE + kk * 2 * G::X_LBO, G::X_LBO, 128);
-            const unsigned long long db =
-                umma_desc(wb + tm.wpl * G::W_PLANE + kk * 2 * G::W_LBO, G::W_LBO, 128);
-            // the first product into each region on the first source overwrites it
             const unsigned acc = (t == 0 && (q & 3) == 0 && kk == 0) ? 0u : 1u;
-            umma_tf32(dcol, da, db, id, acc);
+            umma_tf32(dcol, da0 + kk * xk, db0 + kk * wk, NG[q] ? idesc_neg : idesc, acc);
           }
         }
         umma_commit(&empty[s]);
@@ -330,16 +300,83 @@ __global__ void __launch_bounds__(160, 1) panel_kernel(PanelArgs a) {
       umma_commit(accum);
     }
     __syncwarp();
+  } else {
+    // ===================== source panels + pair table =====================
+    const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
+    for (int t = 0; t < n_iter; ++t) {
+      const int s = t & 1;
+      const unsigned k = (unsigned)(t >> 1);
+      const int j = t < i ? t : t + 1;
+      int ok = 1;
+      if (lane == 0) {
+        ok = t < 2 || wait_or_abort(&empty[s], (k - 1) & 1, abort_flag);
+        if (ok) {
+          const unsigned char* src =
+              reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)grp * N + j) * G::X_STAGE;
+          bulk_load(xs + s * G::X_STAGE, src, G::X_STAGE, &xfull[s]);
+          *last_issued = t;
+          ok = t < 2 || wait_or_abort(&gempty[s], (k - 1) & 1, abort_flag);
+        }
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      float2* g = gt + s * (P * DW);
+      if (lane < P) {
+        const int d = lane;
+        const double dx = xi - a.pos[3 * j], dy = yi - a.pos[3 * j + 1], dz = zi - a.pos[3 * j + 2];
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        double ctd = dz / r;
+        ctd = fmin(1.0, fmax(-1.0, ctd));
+        const float ct = (float)ctd;
+        const float st = (float)sqrt(1.0 - ctd * ctd);
+        const double rho = sqrt(dx * dx + dy * dy);
+        const double phi = (rho > 0.0) ? atan2(dy, dx) : 0.0;
+        float sdp, cdp;
+        sincosf((float)(d * phi), &sdp, &cdp);
+        const double xd = a.k * r;
+        double sxd, cxd;
+        sincos(xd, &sxd, &cxd);
+        const float x = (float)xd, sx = (float)sxd, cx = (float)cxd;
+        const float ix = 1.0f / x;
+        float hr0 = sx * ix, hi0 = -cx * ix;
+        float hr1 = (sx - x * cx) * ix * ix, hi1 = -(cx + x * sx) * ix * ix;
+        for (int q = 0; q < d; ++q) {
+          const float f = (float)(2 * q + 3) * ix;
+          const float nr = f * hr1 - hr0, ni = f * hi1 - hi0;
+          hr0 = hr1; hi0 = hi1; hr1 = nr; hi1 = ni;
+        }
+        float stp = 1.f;
+        for (int q = 0; q < d; ++q) stp *= st;
+        float Pp = 0.f, Pc = (float)a.leg->start[d] * stp;
+        for (int p = d; p < P; ++p) {
+          const float gr = Pc * hr0, gi = Pc * hi0;
+          g[p * DW + (2 * L + d)] = make_float2(gr * cdp - gi * sdp, gr * sdp + gi * cdp);
+          g[p * DW + (2 * L - d)] = make_float2(gr * cdp + gi * sdp, gi * cdp - gr * sdp);
+          if (p + 1 < P) {
+            const float Pn = (float)a.leg->alpha[p * kLegStride + d] * ct * Pc -
+                             (float)a.leg->beta[p * kLegStride + d] * Pp;
+            Pp = Pc;
+            Pc = Pn;
+            const float f = (float)(2 * p + 3) * ix;
+            const float nr = f * hr1 - hr0, ni = f * hi1 - hi0;
+            hr0 = hr1; hi0 = hi1; hr1 = nr; hi1 = ni;
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&gfull[s])) : "memory");
+    }
   }
 
   // ===================== epilogue =====================
   if (warp < 4) {
-    // Always wait (bounded) for the MMAs in flight, aborted or not, before reading or freeing TMEM.
-    bool ok = n_iter == 0 || mbar_wait(accum, 0);
-    if (tid == 0 && *last_issued >= 0) {  // and for the last source copies issued
+    // wait (bounded) for the MMAs and source copies in flight before reading or freeing TMEM
+    const bool ok = n_iter == 0 || mbar_wait(accum, 0);
+    if (tid == 0 && *last_issued >= 0) {
       const int tl = *last_issued;
-      (void)mbar_wait(&full_x[tl & 1], (unsigned)((tl >> 1) & 1));
-      if (tl >= 1) (void)mbar_wait(&full_x[(tl - 1) & 1], (unsigned)(((tl - 1) >> 1) & 1));
+      (void)mbar_wait(&xfull[tl & 1], (unsigned)((tl >> 1) & 1));
+      if (tl >= 1) (void)mbar_wait(&xfull[(tl - 1) & 1], (unsigned)(((tl - 1) >> 1) & 1));
     }
     tc_fence_after();
     const bool aborted = *abort_flag != 0;
@@ -382,7 +419,7 @@ __global__ void __launch_bounds__(160, 1) panel_kernel(PanelArgs a) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 4) {
+  if (warp == 8) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(G::TMEM_COLS)
