@@ -18,6 +18,19 @@ Reported:
   cpu_baseline     the oracle (plain-C restatement of the reference CPU matvec) on host cores,
                    row-sampled, converted to solves/s with this solve's matvec count
 
+Other workloads (--workload):
+  c1     100 spheres, lmax 4, rtol 1e-8, no preconditioner (the reference's CPU-sized case)
+  c3     the C2 aggregate with R = 128 right-hand sides (64 seeded Fibonacci directions x TE/TM):
+         one step = one batched solve (TF32 tensor-core panel inner GMRES, float64 refinement to
+         rtol 1e-8); value = right-hand sides solved per second; C_ext / coefficient errors
+         against float64 solves of sampled columns
+  serve  the serving stream (Poisson arrivals at 20 req/s; N in [50, 3000], lmax 3..8, R in
+         {1, 2, 16, 64}); one step = one request of the stream's prefix (--steps requests, the
+         first of the 512-request stream); warm-up = requests drawn from the same distribution
+         with other seeds; value = right-hand sides solved per second over the makespan, with
+         p50/p99 request latency and the C_ext error of sampled requests against float64 solves
+  c5     20000 spheres, lmax 4, rtol 1e-6, 8x8x8 block-Jacobi
+
 --impl reference times the reference's CPU algorithm (the oracle port, all host threads) on the
 same workload and prints the same metric with "impl": "reference".
 """
@@ -40,6 +53,9 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "solves/s (C2: 2000 spheres, lmax 6, FP64, GMRES rtol 1e-8, 4x4x4 block-Jacobi); matvec/s"
+METRIC_C3 = ("solves/s (C3: 2000 spheres, lmax 6, R=128 incidences, TF32 panel inner GMRES in FP64 "
+             "refinement to rtol 1e-8)")
+METRIC_SERVE = "solves/s + p50/p99 latency (serving stream, mixed precision, C_ext err vs FP64 GPU)"
 UNIT = "solves/s"
 FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12  # B200: 148 SMs x 64 FP64 FMA/clk at 1965 MHz
 T_NZ = {1: 20, 2: 314, 3: 1578, 4: 4904, 5: 12302, 6: 26700, 7: 52178, 8: 94160}
@@ -62,6 +78,8 @@ def workload(name: str):
         return aggregate_c2(seed=0), 1e-8, 4
     if name == "c5":
         return aggregate_c5(seed=0), 1e-6, 8
+    if name == "c3":
+        return aggregate_c2(seed=0), 1e-8, None
     raise ValueError(name)
 
 
@@ -399,6 +417,258 @@ def run_b200(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------
+def cross_sections(dev, a_col, x_col, k: float) -> tuple[float, float]:
+    """(C_ext, C_sca) of one solved column, on the device (optics.py formulas)."""
+    c_ext = -np.real(dev.dotc(a_col, x_col)) / k**2 * np.pi
+    c_sca = abs(dev.scattering_bilinear(x_col)) / k**2 * np.pi
+    return float(c_ext), float(c_sca)
+
+
+def fp64_column(dev, tmat, b_col, rtol=1e-10):
+    """Plain float64 device GMRES (no preconditioner) of one column: the float64 reference."""
+    x = b_col.clone()
+    st = dev.gmres(tmat, b_col, x, rtol, 100, 50)
+    return x, st
+
+
+def run_batched(args, rank: int, world: int) -> None:
+    """C3: one batched solve of the C2 aggregate's 128 incidences per step (ranks are replicas)."""
+    import torch
+
+    from yasf_b200 import _lib
+    from yasf_b200.device import CouplingDevice
+    from yasf_b200.incident import plane_wave_block
+    from yasf_b200.mie import mie_tmatrix_per_sphere
+    from yasf_b200.numerics import cached_translation_table
+    from yasf_b200.workloads import incidences
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    agg, rtol, _ = workload("c3")
+    polar, azim, pol = incidences(64, rotation_seed=0)
+    R = len(pol)
+    tm = mie_tmatrix_per_sphere(agg.lmax, agg.k, agg.radii, agg.refractive_index)
+    a = plane_wave_block(agg.lmax, agg.positions, agg.k, polar, azim, pol)
+    A = np.ascontiguousarray(np.moveaxis(a, 2, 0).reshape(R, -1))
+    B_host = torch.from_numpy(np.ascontiguousarray(A * tm[None, :])).pin_memory()
+    dev = CouplingDevice(agg.lmax, cached_translation_table(agg.lmax), agg.positions, agg.k, device)
+    tmat = torch.from_numpy(tm).to(device)
+    B = B_host.to(device)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+    kw = dict(rtol=rtol, restart=args.restart_batched, max_refine=8, inner_rtol=1e-3, inner="tf32")
+
+    for _ in range(args.warmup):
+        dev.batched_solve(tmat, B, **kw)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.yasf_kernel_launches()
+    per_ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            X, st = dev.batched_solve(tmat, B, **kw)
+            e1.record()
+            e1.synchronize()
+            per_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = lib.yasf_kernel_launches() - launches0
+    if dist is not None:
+        dist.barrier()
+    tot = torch.tensor([sum(per_ms)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    max_total_ms = float(tot.item())
+    value = world * R * args.steps / (max_total_ms / 1e3)
+
+    # e2e: pinned host B -> device, solve, X -> host
+    X_host = torch.empty_like(B_host).pin_memory()
+    flush.zero_()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Bd = B_host.to(device, non_blocking=True)
+    Xe, _ = dev.batched_solve(tmat, Bd, **kw)
+    X_host.copy_(Xe, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    del Bd, Xe
+
+    # errors against float64 solves of sampled columns
+    samples = []
+    worst = {"c_ext": 0.0, "c_sca": 0.0, "coef": 0.0}
+    for c in sorted({0, R // 2 - 1, R - 1})[: args.error_samples]:
+        x64, st64 = fp64_column(dev, tmat, B[c].contiguous())
+        ac = torch.from_numpy(A[c]).to(device)
+        ce, cs = cross_sections(dev, ac, X[c].contiguous(), agg.k)
+        ce64, cs64 = cross_sections(dev, ac, x64, agg.k)
+        coef = float(torch.linalg.vector_norm(X[c] - x64) / torch.linalg.vector_norm(x64))
+        e = {"column": c, "c_ext": ce, "c_ext_fp64": ce64, "c_ext_rel_err": abs(ce - ce64) / abs(ce64),
+             "c_sca_rel_err": abs(cs - cs64) / abs(cs64), "coef_rel_err": coef, "fp64_info": st64["info"],
+             "fp64_residual": st64["relative_residual"]}
+        samples.append(e)
+        worst["c_ext"] = max(worst["c_ext"], e["c_ext_rel_err"])
+        worst["c_sca"] = max(worst["c_sca"], e["c_sca_rel_err"])
+        worst["coef"] = max(worst["coef"], coef)
+    colres = st.pop("column_residuals")
+
+    if rank != 0:
+        return
+    nbytes = R * dev.n * 16
+    lat = sorted(per_ms)
+    line = {
+        "metric": METRIC_C3, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "tf32 inner / c128 refinement",
+        "data": "synthetic (seeded RSA aggregate, seeded Fibonacci incidences, no dataset)",
+        "config": {"workload": agg.name + "-R128", "n_spheres": agg.n, "lmax": agg.lmax,
+                   "unknowns": dev.n, "nrhs": R, "rtol": rtol, "restart": args.restart_batched,
+                   "inner": "TF32 tensor-core panel, inner_rtol 1e-3", "preconditioner": None,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "flushed (256 MB write) before every timed solve"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "solve_stats": st,
+        "fp64_residual_all_columns": {"max": max(colres), "median": statistics.median(colres)},
+        "error_vs_fp64": {"worst": worst, "samples": samples},
+        "e2e": {"value": world * R / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, rank: int, world: int) -> None:
+    """Serving stream prefix; requests are dealt round-robin to ranks (replicas, no exchange)."""
+    import torch
+
+    from yasf_b200 import _lib
+    from yasf_b200.device import CouplingDevice
+    from yasf_b200.incident import plane_wave_block
+    from yasf_b200.mie import mie_tmatrix_per_sphere
+    from yasf_b200.numerics import cached_translation_table
+    from yasf_b200.serve import ServeConfig, Server, summarize
+    from yasf_b200.workloads import serving_requests
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    stream = serving_requests(args.steps)
+    mine = [r for r in stream if r.rid % world == rank]
+    # warm-up: small requests from the same distribution (other seeds), one per lmax in use
+    # at least, so that every plan and kernel variant is set up before the timed stream
+    lmaxes = sorted({r.aggregate.lmax for r in mine})
+    warm = []
+    for i in range(max(args.warmup, len(lmaxes))):
+        lm = (lmaxes[i % len(lmaxes)],) if lmaxes else (3,)
+        warm += serving_requests(1, seed=7 + i, n_range=(50, 300), lmax_choices=lm, param_seed=100_000 + i)
+    cfg = ServeConfig(max_slots=args.slots, rtol=args.serve_rtol)
+    server = Server(cfg, device=device)
+    server.run(warm, realtime=False)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.yasf_kernel_launches()
+    with ClockSampler(local) as clk:
+        results = server.run(mine, realtime=True)
+    torch.cuda.synchronize()
+    launches = lib.yasf_kernel_launches() - launches0
+    summ = summarize(results)
+    if dist is not None:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, [(r.rid, r.nrhs, r.latency, r.finished, r.error) for r in results])
+        flat = [t for g in gathered for t in g]
+    else:
+        flat = [(r.rid, r.nrhs, r.latency, r.finished, r.error) for r in results]
+    ok = [t for t in flat if t[4] is None]
+    makespan = max(t[3] for t in flat) - min(r.arrival for r in stream)
+    rhs = sum(t[1] for t in ok)
+    lat = np.array([t[2] for t in ok]) if ok else np.zeros(1)
+
+    # C_ext of sampled requests against float64 solves (outside the timed region)
+    errs = []
+    for r in results[: args.error_samples]:
+        if r.error is not None:
+            continue
+        req = next(q for q in mine if q.rid == r.rid)
+        agg = req.aggregate
+        dev = CouplingDevice(agg.lmax, cached_translation_table(agg.lmax), agg.positions, agg.k, device)
+        tmh = mie_tmatrix_per_sphere(agg.lmax, agg.k, agg.radii, agg.refractive_index)
+        a = plane_wave_block(agg.lmax, agg.positions, agg.k, req.polar[:1], req.azimuthal[:1], req.pol[:1])
+        a0 = np.ascontiguousarray(a[:, :, 0].ravel())
+        tmat = torch.from_numpy(tmh).to(device)
+        b0 = torch.from_numpy(a0 * tmh).to(device)
+        x64, st64 = fp64_column(dev, tmat, b0)
+        ce64 = -np.real(np.vdot(a0, x64.cpu().numpy())) / agg.k**2 * np.pi
+        errs.append({"rid": r.rid, "n": agg.n, "lmax": agg.lmax, "nrhs": r.nrhs,
+                     "c_ext_rel_err": abs(r.c_ext[0] - ce64) / abs(ce64), "fp64_info": st64["info"]})
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC_SERVE, "value": rhs / makespan, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": makespan * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "tf32 inner (lmax<=6) / c64 inner (lmax 7-8), c128 refinement",
+        "data": "synthetic (seeded request stream, no dataset)",
+        "config": {"workload": f"serving stream, first {args.steps} of 512 requests (Poisson 20 req/s)",
+                   "requests": args.steps, "slots": args.slots, "rtol": args.serve_rtol,
+                   "parallelism": "requests dealt round-robin to replicas" if world > 1 else "single GPU",
+                   "l2": "inputs of a request larger than L2 for most requests; no flush between requests"},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "requests_completed": len(ok), "requests_failed": len(flat) - len(ok), "rhs_solves": rhs,
+        "makespan_s": makespan, "rank0_summary": summ,
+        "c_ext_error_vs_fp64": {"max": max((e["c_ext_rel_err"] for e in errs), default=None),
+                                "samples": errs},
+        "e2e": {"value": rhs / makespan, "unit": UNIT,
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "each request enters as host arrays (geometry, incidences) and returns C_ext "
+                        "and the solution to the host: the serving loop is end to end"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def panel_probe(args) -> None:
+    """Four panel matvecs (the first is warm-up) on the first N spheres with --nrhs columns."""
+    import torch
+
+    from yasf_b200.device import CouplingDevice
+    from yasf_b200.numerics import cached_translation_table
+
+    agg, _, _ = workload("c2")
+    n = min(args.panel_probe, agg.n)
+    dev = CouplingDevice(agg.lmax, cached_translation_table(agg.lmax), agg.positions[:n], agg.k,
+                         torch.device("cuda", 0))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(args.nrhs, dev.n, dtype=torch.complex128, device=dev.device, generator=g)
+    tmat = torch.randn(dev.n, dtype=torch.complex128, device=dev.device, generator=g) * 0.1
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    y = dev.panel(x, tmat)
+    e0.record()
+    for _ in range(3):
+        y = dev.panel(x, tmat)
+    e1.record()
+    e1.synchronize()
+    print(json.dumps({"probe": "panel", "n": n, "nrhs": args.nrhs, "ms": e0.elapsed_time(e1) / 3,
+                      "max_abs": float(y.abs().max())}))
+
+
 def matvec_probe(args) -> None:
     """Four coupling matvecs (the first is warm-up) on the first N spheres of the workload."""
     import torch
@@ -425,7 +695,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["c1", "c2", "c5"], default="c2")
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "serve", "c5"], default="c2")
     ap.add_argument("--restart", type=int, default=100)
     ap.add_argument("--no-precond", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
@@ -434,9 +704,19 @@ def main() -> None:
     ap.add_argument("--matvec-probe", type=int, default=0, metavar="N",
                     help="profiling aid: run 4 coupling matvecs on the first N spheres and exit")
     ap.add_argument("--precision", choices=["c128", "c64"], default="c128")
+    ap.add_argument("--panel-probe", type=int, default=0, metavar="N",
+                    help="profiling aid: run 4 TF32 panel matvecs on the first N spheres and exit")
+    ap.add_argument("--nrhs", type=int, default=128, help="columns of --panel-probe")
+    ap.add_argument("--restart-batched", type=int, default=50, help="inner GMRES cycle length (c3)")
+    ap.add_argument("--slots", type=int, default=4, help="serving slots (serve)")
+    ap.add_argument("--serve-rtol", type=float, default=1e-6, help="serving refinement tolerance")
+    ap.add_argument("--error-samples", type=int, default=3, help="float64 check solves (c3, serve)")
     args = ap.parse_args()
     if args.matvec_probe:
         matvec_probe(args)
+        return
+    if args.panel_probe:
+        panel_probe(args)
         return
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
@@ -456,6 +736,10 @@ def main() -> None:
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "c3":
+            run_batched(args, rank, world)
+        elif args.workload == "serve":
+            run_serve(args, rank, world)
         else:
             run_b200(args, rank, world)
     finally:

@@ -54,3 +54,41 @@ def compute_mie_coefficients(lmax: int, omega: np.ndarray, k_medium: np.ndarray,
             mie[u, s2:s2 + w, :] = t2[li, :]
             ratio[u, s2:s2 + w, :] = r2[li, :]
     return mie, ratio
+
+
+def mie_tmatrix_per_sphere(lmax: int, k_medium: float, radii: np.ndarray,
+                           refractive_index: complex | np.ndarray) -> np.ndarray:
+    """Diagonal T for every sphere at once, (N*nmax,) complex128 in the unknowns' order.
+
+    The same formulas as ``compute_mie_coefficients`` (yasfpy/mie_coefficients.py:87-161),
+    vectorised over spheres instead of looping over unique (radius, index) pairs.
+    """
+    radii = np.asarray(radii, dtype=float)
+    N = radii.size
+    m = np.broadcast_to(np.asarray(refractive_index, dtype=complex), (N,))
+    nmax = 2 * lmax * (lmax + 2)
+    lg = np.arange(1, lmax + 1)[:, None]
+    x = (k_medium * radii)[None, :]
+    mx = (k_medium * m * radii)[None, :]
+    jx = spherical_jn(lg, x)
+    jxp = spherical_jn(lg, x, derivative=True)
+    yx = spherical_yn(lg, x)
+    yxp = spherical_yn(lg, x, derivative=True)
+    jmx = spherical_jn(lg, mx)
+    jmxp = spherical_jn(lg, mx, derivative=True)
+    hx = jx + 1j * yx
+    hxp = jxp + 1j * yxp
+    djx = jx + x * jxp
+    djmx = jmx + mx * jmxp
+    dhx = hx + x * hxp
+    mm = m[None, :]
+    t1 = -(jmx * djx - jx * djmx) / (jmx * dhx - hx * djmx)
+    t2 = -(mm**2 * jmx * djx - jx * djmx) / (mm**2 * jmx * dhx - hx * djmx)
+    out = np.zeros((N, nmax), dtype=complex)
+    for li, l in enumerate(range(1, lmax + 1)):
+        w = 2 * l + 1
+        s1 = l * l - 1
+        s2 = lmax * (lmax + 2) + l * l - 1
+        out[:, s1:s1 + w] = t1[li, :, None]
+        out[:, s2:s2 + w] = t2[li, :, None]
+    return out.ravel()

@@ -1,0 +1,214 @@
+"""Serving: a continuous-batching request loop for T-matrix solves of different sizes.
+
+Each request carries an aggregate (spheres, refractive index, wavelength, lmax) and a set of
+incidences (directions x polarisations = R right-hand sides). The loop:
+
+- admits a request once its arrival time has passed, a slot is free and its device footprint
+  (the Krylov bases of its R columns, its panels and workspaces) fits in the HBM budget that the
+  requests in flight leave; a request that can never fit is rejected with an error;
+- runs every admitted request on its own CUDA stream, so the kernels of in-flight solves
+  interleave on the device while their GMRES state stays resident there;
+- solves in mixed precision: the batched refined solve (yasf_batched_solve) with the tensor-core
+  TF32 panel as the inner operator (complex64 coupling kernel beyond lmax 6), float64 residuals,
+  stopping at rtol (1e-6 by default, which keeps the extinction cross section well inside 1e-6 of
+  the float64 solution);
+- reports per-request latency (completion - arrival, queueing included), p50/p99 and solves/s.
+
+The kernels are deterministic (no atomics in any reduction), so a request's result does not depend
+on what else is in flight: ``solve_request`` alone and inside the loop give the same numbers.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+import time
+from collections import deque
+from concurrent.futures import FIRST_COMPLETED, ThreadPoolExecutor, wait
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from yasf_b200._lib import call
+from yasf_b200.device import CouplingDevice
+from yasf_b200.incident import plane_wave_block
+from yasf_b200.mie import mie_tmatrix_per_sphere
+from yasf_b200.numerics import cached_translation_table
+from yasf_b200.workloads import Request
+
+
+@dataclass
+class ServeConfig:
+    max_slots: int = 4
+    hbm_budget_bytes: int | None = None   # default: 80 % of the free device memory at start
+    rtol: float = 1e-6
+    restart: int = 30
+    max_refine: int = 8
+    inner_rtol: float = 1e-3
+    keep_solutions: bool = False
+
+
+@dataclass
+class RequestResult:
+    rid: int
+    n_spheres: int
+    lmax: int
+    nrhs: int
+    c_ext: np.ndarray | None = None
+    stats: dict = field(default_factory=dict)
+    arrival: float = 0.0
+    admitted: float = 0.0
+    finished: float = 0.0
+    error: str | None = None
+    x: np.ndarray | None = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def inner_kind(lmax: int) -> str:
+    return "tf32" if lmax <= 6 else "c64"
+
+
+def footprint_bytes(req: Request, cfg: ServeConfig, dev_plan_handle=None) -> int:
+    """Device bytes a request holds while in flight (workspace + its vectors)."""
+    agg = req.aggregate
+    nmax = 2 * agg.lmax * (agg.lmax + 2)
+    n = agg.n * nmax
+    R = len(req.pol)
+    restart = min(cfg.restart, n)
+    # Krylov bases and panels dominate: R (m+1) n + 6 R n complex128 + source panels + V stream
+    basis = R * (restart + 1) * n * 16
+    panels = 6 * R * n * 16
+    v_stream = agg.n * nmax * 150 * 16 // 2  # per-source V stream (complex128), generous
+    return int(basis + panels + v_stream + (64 << 20))
+
+
+def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> RequestResult:
+    """One request, start to finish, on the current stream of the calling thread."""
+    agg = req.aggregate
+    R = len(req.pol)
+    res = RequestResult(req.rid, agg.n, agg.lmax, R)
+    table = cached_translation_table(agg.lmax)
+    tm = mie_tmatrix_per_sphere(agg.lmax, agg.k, agg.radii, agg.refractive_index)
+    a = plane_wave_block(agg.lmax, agg.positions, agg.k, req.polar, req.azimuthal, req.pol)
+    A = np.ascontiguousarray(np.moveaxis(a, 2, 0).reshape(R, -1))
+    B = A * tm[None, :]
+    dev = CouplingDevice(agg.lmax, table, agg.positions, agg.k, device)
+    tmat = torch.from_numpy(tm).to(device)
+    Bt = torch.from_numpy(B).to(device)
+    X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
+                              inner_rtol=cfg.inner_rtol, inner=inner_kind(agg.lmax))
+    Xh = X.cpu().numpy()
+    res.c_ext = -np.real(np.einsum("rn,rn->r", A.conj(), Xh)) / agg.k**2 * np.pi
+    st.pop("column_residuals", None)
+    res.stats = st
+    if cfg.keep_solutions:
+        res.x = Xh
+    return res
+
+
+class Server:
+    """Continuous-batching loop over a request stream on one GPU."""
+
+    def __init__(self, cfg: ServeConfig | None = None, device: torch.device | str | None = None,
+                 solve_fn=None, footprint_fn=None):
+        self.cfg = cfg or ServeConfig()
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        if self.cfg.hbm_budget_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            self.cfg.hbm_budget_bytes = int(0.8 * free)
+        self._solve = solve_fn or solve_request
+        self._footprint = footprint_fn or footprint_bytes
+        self._tls = threading.local()
+
+    def _worker(self, req: Request, t0: float) -> RequestResult:
+        if self.device.type != "cuda":  # host-only solve functions (tests of the loop itself)
+            try:
+                res = self._solve(req, self.cfg, self.device)
+            except Exception as e:
+                agg = req.aggregate
+                res = RequestResult(req.rid, agg.n, agg.lmax, len(req.pol), error=f"{type(e).__name__}: {e}")
+            res.finished = time.perf_counter() - t0
+            return res
+        stream = getattr(self._tls, "stream", None)
+        if stream is None:
+            stream = torch.cuda.Stream(device=self.device)
+            self._tls.stream = stream
+        with torch.cuda.device(self.device), torch.cuda.stream(stream):
+            try:
+                res = self._solve(req, self.cfg, self.device)
+            except Exception as e:  # a failed request reports its error, the loop goes on
+                agg = req.aggregate
+                res = RequestResult(req.rid, agg.n, agg.lmax, len(req.pol), error=f"{type(e).__name__}: {e}")
+            stream.synchronize()
+        res.finished = time.perf_counter() - t0
+        return res
+
+    def run(self, requests: list[Request], realtime: bool = True) -> list[RequestResult]:
+        """Serve the requests (arrival times in seconds from the start); returns results by rid."""
+        for lmax in sorted({r.aggregate.lmax for r in requests}):
+            cached_translation_table(lmax)  # tables are host setup shared by all requests
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        inflight: dict = {}
+        used = 0
+        results: list[RequestResult] = []
+        budget = self.cfg.hbm_budget_bytes
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=self.cfg.max_slots) as pool:
+            while pending or inflight:
+                now = time.perf_counter() - t0
+                while pending and (not realtime or pending[0].arrival <= now) and len(inflight) < self.cfg.max_slots:
+                    req = pending[0]
+                    fp = self._footprint(req, self.cfg)
+                    if fp > budget:
+                        pending.popleft()
+                        agg = req.aggregate
+                        r = RequestResult(req.rid, agg.n, agg.lmax, len(req.pol),
+                                          error=f"needs {fp} bytes, budget {budget}")
+                        r.arrival = req.arrival
+                        r.finished = now
+                        results.append(r)
+                        continue
+                    if used + fp > budget:
+                        break  # wait for memory to free up
+                    pending.popleft()
+                    used += fp
+                    fut = pool.submit(self._worker, req, t0)
+                    inflight[fut] = (req, fp, now)
+                if pending and realtime and pending[0].arrival > now:
+                    timeout = pending[0].arrival - now
+                else:
+                    timeout = 0.05
+                if not inflight:
+                    time.sleep(max(0.0, min(timeout, 0.05)))
+                    continue
+                done, _ = wait(list(inflight.keys()), timeout=max(0.0, timeout), return_when=FIRST_COMPLETED)
+                for f in done:
+                    req, fp, admitted = inflight.pop(f)
+                    used -= fp
+                    r = f.result()
+                    r.arrival = req.arrival if realtime else 0.0
+                    r.admitted = admitted
+                    results.append(r)
+        return sorted(results, key=lambda r: r.rid)
+
+
+def summarize(results: list[RequestResult]) -> dict:
+    ok = [r for r in results if r.error is None]
+    lat = np.array([r.latency for r in ok]) if ok else np.array([0.0])
+    makespan = max((r.finished for r in results), default=0.0) - min((r.arrival for r in results), default=0.0)
+    rhs = sum(r.nrhs for r in ok)
+    return {
+        "requests": len(results),
+        "completed": len(ok),
+        "failed": len(results) - len(ok),
+        "rhs_solves": rhs,
+        "makespan_s": makespan,
+        "solves_per_s": rhs / makespan if makespan > 0 else 0.0,
+        "requests_per_s": len(ok) / makespan if makespan > 0 else 0.0,
+        "latency_p50_s": float(np.percentile(lat, 50)),
+        "latency_p99_s": float(np.percentile(lat, 99)),
+    }

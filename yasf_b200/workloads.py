@@ -45,8 +45,14 @@ class Aggregate:
         return 2 * math.pi / self.wavelength
 
 
-def _rsa(radii: np.ndarray, sampler, rng: np.random.Generator, max_attempts: int) -> np.ndarray:
-    """Random sequential addition with a uniform-grid neighbour search."""
+def _rsa(radii: np.ndarray, sampler, rng: np.random.Generator, max_attempts: int,
+         largest_first: bool = False) -> np.ndarray:
+    """Random sequential addition with a uniform-grid neighbour search.
+
+    Spheres are inserted in index order, or largest first (the usual way to reach dense
+    polydisperse packings: small spheres still fit in the gaps the large ones leave); sphere i
+    keeps radius radii[i] either way.
+    """
     N = radii.size
     rmax = float(radii.max())
     cell = 2.0 * rmax
@@ -54,7 +60,8 @@ def _rsa(radii: np.ndarray, sampler, rng: np.random.Generator, max_attempts: int
     pos = np.zeros((N, 3))
     attempts = 0
     batch = 256
-    for i in range(N):
+    order = np.argsort(-radii, kind="stable") if largest_first else range(N)
+    for i in order:
         placed = False
         while not placed:
             cand = sampler(radii[i], batch)
@@ -87,18 +94,18 @@ def _rsa(radii: np.ndarray, sampler, rng: np.random.Generator, max_attempts: int
 
 
 def rsa_cube(radii: np.ndarray, volume_fraction: float, rng: np.random.Generator,
-             max_attempts: int = 50_000_000) -> np.ndarray:
+             max_attempts: int = 50_000_000, largest_first: bool = False) -> np.ndarray:
     """Centres in a cube of side L = (sum 4/3 pi r^3 / phi)^(1/3), each sphere inside the cube."""
     side = (np.sum(4.0 / 3.0 * np.pi * radii**3) / volume_fraction) ** (1.0 / 3.0)
 
     def sampler(r, n):
         return rng.uniform(r, side - r, size=(n, 3))
 
-    return _rsa(radii, sampler, rng, max_attempts)
+    return _rsa(radii, sampler, rng, max_attempts, largest_first)
 
 
 def rsa_ball(radii: np.ndarray, volume_fraction: float, rng: np.random.Generator,
-             max_attempts: int = 50_000_000) -> np.ndarray:
+             max_attempts: int = 50_000_000, largest_first: bool = False) -> np.ndarray:
     """Centres in a ball of radius R = (sum r^3 / phi)^(1/3), each sphere inside the ball."""
     R = (np.sum(radii**3) / volume_fraction) ** (1.0 / 3.0)
 
@@ -108,7 +115,7 @@ def rsa_ball(radii: np.ndarray, volume_fraction: float, rng: np.random.Generator
         rad = (R - r) * rng.uniform(0.0, 1.0, size=(n, 1)) ** (1.0 / 3.0)
         return v * rad
 
-    return _rsa(radii, sampler, rng, max_attempts)
+    return _rsa(radii, sampler, rng, max_attempts, largest_first)
 
 
 def aggregate_c1(seed: int = 0, n: int = 100) -> Aggregate:
@@ -167,14 +174,17 @@ class Request:
 
 def serving_requests(n_requests: int = 512, rate: float = 20.0, seed: int = 0,
                      n_range=(50, 3000), lmax_choices=(3, 4, 5, 6, 7, 8),
-                     rhs_choices=(1, 2, 16, 64)) -> list[Request]:
-    """The serving stream: Poisson arrivals; per-request parameters from seed 1000 + i."""
+                     rhs_choices=(1, 2, 16, 64), param_seed: int = 1000) -> list[Request]:
+    """The serving stream: Poisson arrivals; per-request parameters from seed param_seed + i.
+
+    Request i of a shorter stream is request i of the 512-request stream (same arrival, same
+    parameters), so a prefix is served by asking for fewer requests."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, size=n_requests)
     arrivals = np.cumsum(gaps) - gaps[0]
     reqs = []
     for i in range(n_requests):
-        r = np.random.default_rng(1000 + i)
+        r = np.random.default_rng(param_seed + i)
         n = int(r.integers(n_range[0], n_range[1] + 1))
         lmax = int(r.choice(lmax_choices))
         phi = float(r.uniform(0.05, 0.30))
@@ -182,8 +192,8 @@ def serving_requests(n_requests: int = 512, rate: float = 20.0, seed: int = 0,
         wl = float(r.uniform(0.4, 0.8))
         m = complex(r.uniform(1.3, 1.8), 10 ** r.uniform(-4, -1))
         R = int(r.choice(rhs_choices))
-        pos = rsa_cube(radii, phi, r)
-        agg = Aggregate(f"req{i}", pos, radii, m, wl, lmax, 1000 + i, {"phi": phi})
+        pos = rsa_cube(radii, phi, r, largest_first=True)
+        agg = Aggregate(f"req{i}", pos, radii, m, wl, lmax, param_seed + i, {"phi": phi})
         ndir = max(1, R // 2) if R > 1 else 1
         polar, azim, pol = incidences(ndir)
         if R == 1:
