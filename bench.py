@@ -52,6 +52,8 @@ import numpy as np
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
+from yasf_b200.replicas import gather_records, max_over_ranks, serving_totals, shard_requests  # noqa: E402
+
 METRIC = "solves/s (C2: 2000 spheres, lmax 6, FP64, GMRES rtol 1e-8, 4x4x4 block-Jacobi); matvec/s"
 METRIC_C3 = ("solves/s (C3: 2000 spheres, lmax 6, R=128 incidences, TF32 panel inner GMRES in FP64 "
              "refinement to rtol 1e-8)")
@@ -290,11 +292,7 @@ def run_b200(args, rank: int, world: int) -> None:
     launches = lib.yasf_kernel_launches() - launches0
     if dist is not None:
         dist.barrier()
-    total_ms = sum(per_ms)
-    tot = torch.tensor([total_ms], dtype=torch.float64, device=device)
-    if dist is not None:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    max_total_ms = float(tot.item())
+    max_total_ms = max_over_ranks(sum(per_ms), device)
     value = world * args.steps / (max_total_ms / 1e3)
 
     # ---- cross sections of the timed solution ----------------------------------------------
@@ -485,10 +483,7 @@ def run_batched(args, rank: int, world: int) -> None:
     launches = lib.yasf_kernel_launches() - launches0
     if dist is not None:
         dist.barrier()
-    tot = torch.tensor([sum(per_ms)], dtype=torch.float64, device=device)
-    if dist is not None:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    max_total_ms = float(tot.item())
+    max_total_ms = max_over_ranks(sum(per_ms), device)
     value = world * R * args.steps / (max_total_ms / 1e3)
 
     # e2e: pinned host B -> device, solve, X -> host
@@ -567,7 +562,7 @@ def run_serve(args, rank: int, world: int) -> None:
     if world > 1:
         import torch.distributed as dist  # noqa: F811
     stream = serving_requests(args.steps)
-    mine = [r for r in stream if r.rid % world == rank]
+    mine = shard_requests(stream, rank, world)
     # warm-up: small requests from the same distribution (other seeds), one per lmax in use
     # at least, so that every plan and kernel variant is set up before the timed stream
     lmaxes = sorted({r.aggregate.lmax for r in mine})
@@ -588,16 +583,8 @@ def run_serve(args, rank: int, world: int) -> None:
     torch.cuda.synchronize()
     launches = lib.yasf_kernel_launches() - launches0
     summ = summarize(results)
-    if dist is not None:
-        gathered = [None] * world
-        dist.all_gather_object(gathered, [(r.rid, r.nrhs, r.latency, r.finished, r.error) for r in results])
-        flat = [t for g in gathered for t in g]
-    else:
-        flat = [(r.rid, r.nrhs, r.latency, r.finished, r.error) for r in results]
-    ok = [t for t in flat if t[4] is None]
-    makespan = max(t[3] for t in flat) - min(r.arrival for r in stream)
-    rhs = sum(t[1] for t in ok)
-    lat = np.array([t[2] for t in ok]) if ok else np.zeros(1)
+    flat = gather_records([(r.rid, r.nrhs, r.latency, r.finished, r.error) for r in results])
+    tot = serving_totals(flat, min(r.arrival for r in stream))
 
     # C_ext of sampled requests against float64 solves (outside the timed region)
     errs = []
@@ -619,8 +606,8 @@ def run_serve(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     line = {
-        "metric": METRIC_SERVE, "value": rhs / makespan, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": makespan * 1e3 / args.steps,
+        "metric": METRIC_SERVE, "value": tot["solves_per_s"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot["makespan_s"] * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "tf32 inner (lmax<=6) / c64 inner (lmax 7-8), c128 refinement",
         "data": "synthetic (seeded request stream, no dataset)",
@@ -628,12 +615,12 @@ def run_serve(args, rank: int, world: int) -> None:
                    "requests": args.steps, "slots": args.slots, "rtol": args.serve_rtol,
                    "parallelism": "requests dealt round-robin to replicas" if world > 1 else "single GPU",
                    "l2": "inputs of a request larger than L2 for most requests; no flush between requests"},
-        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-        "requests_completed": len(ok), "requests_failed": len(flat) - len(ok), "rhs_solves": rhs,
-        "makespan_s": makespan, "rank0_summary": summ,
+        "latency_s": {"p50": tot["latency_p50_s"], "p99": tot["latency_p99_s"]},
+        "requests_completed": tot["completed"], "requests_failed": tot["failed"],
+        "rhs_solves": tot["rhs_solves"], "makespan_s": tot["makespan_s"], "rank0_summary": summ,
         "c_ext_error_vs_fp64": {"max": max((e["c_ext_rel_err"] for e in errs), default=None),
                                 "samples": errs},
-        "e2e": {"value": rhs / makespan, "unit": UNIT,
+        "e2e": {"value": tot["solves_per_s"], "unit": UNIT,
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "note": "each request enters as host arrays (geometry, incidences) and returns C_ext "
                         "and the solution to the host: the serving loop is end to end"},
