@@ -1,0 +1,94 @@
+"""The build-time W-generation schedule of the tensor-core panel, checked on the host.
+
+- structure: every entry of both W blocks is produced, and every warp's stores of a step hit 32
+  different banks (primary entries; mirrors up to a few lanes that recompute padding),
+- arithmetic: emulating the kernel's generation in float64 from the schedule (items of an entry
+  and its mirror, the A[p][|d|] table, phases e^{i d phi}, P = Wa + Wb, Q = Wa - Wb) and its
+  tau-symmetric product (S = X1 + X2, D = X1 - X2, Y1 = (U + V) / 2, Y2 = (U - V) / 2) reproduces
+  the oracle's two-sphere coupling W_ij x_j to rounding.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import restate as R
+from yasf_b200.panel_sched import WARPS, _lm, mirror, schedule
+from yasf_b200.wigner import translation_table_ab5
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 4, 5, 6])
+def test_schedule_structure(L):
+    steps, table = schedule(L)
+    H = L * (L + 2)
+    covered = set()
+    collisions = 0
+    for w in range(WARPS):
+        for k in range(len(steps)):
+            row = table[w][k]
+            assert len({(q1 & 7, q2 & 3) for q1, q2 in row}) == 32
+            mcls = [((mirror(q1) & 7, mirror(q2) & 3) if q1 < H and q2 < H else (q1 & 7, q2 & 3))
+                    for q1, q2 in row]
+            collisions += 32 - len(set(mcls))
+            for q1, q2 in row:
+                if q1 < H and q2 < H:
+                    covered.add((q1, q2))
+                    covered.add((mirror(q1), mirror(q2)))
+    assert len(covered) == H * H
+    assert collisions <= 4 * WARPS * len(steps)  # a few lanes per step, padding recomputation only
+
+
+def _emulate_wx(L, table_ab5, ri, rj, k, xj):
+    H = L * (L + 2)
+    P = 2 * L + 1
+    d = np.asarray(ri) - np.asarray(rj)
+    r = np.linalg.norm(d)
+    ct, st = d[2] / r, np.hypot(d[0], d[1]) / r
+    phi = np.arctan2(d[1], d[0])
+    j, y = R.sph_bessel(P - 1, k * r)
+    h = j + 1j * y
+    leg = R.legendre(P - 1, ct, st)
+    A = np.array([[leg[p, dd] * h[p] if dd <= p else 0 for dd in range(P)] for p in range(P)])
+    steps, sched = schedule(L)
+    Pm = np.full((H, H), np.nan, dtype=complex)
+    Qm = np.full((H, H), np.nan, dtype=complex)
+    tab = np.asarray(table_ab5)
+    for w in range(WARPS):
+        for kk in range(len(steps)):
+            for q1, q2 in sched[w][kk]:
+                if q1 >= H or q2 >= H:
+                    continue
+                l1, m1 = _lm(q1)
+                l2, m2 = _lm(q2)
+                dl = m2 - m1
+                pmin = max(abs(l1 - l2), abs(dl))
+                Sa = Sb = 0j
+                for p in range(pmin, l1 + l2 + 1):
+                    if (l1 + l2 + p) % 2 == 0:
+                        Sa += tab[q2, q1, p].real * A[p, abs(dl)]
+                    else:
+                        Sb += tab[H + q2, q1, p].imag * A[p, abs(dl)]
+                E = np.exp(1j * dl * phi)
+                Wa, Wb = E * Sa, 1j * E * Sb
+                Pm[q1, q2], Qm[q1, q2] = Wa + Wb, Wa - Wb
+                Wa2, Wb2 = np.conj(E) * Sa, -1j * np.conj(E) * Sb
+                Pm[mirror(q1), mirror(q2)], Qm[mirror(q1), mirror(q2)] = Wa2 + Wb2, Wa2 - Wb2
+    assert not np.isnan(Pm).any() and not np.isnan(Qm).any()
+    x1, x2 = xj[:H], xj[H:]
+    U, V = Pm @ (x1 + x2), Qm @ (x1 - x2)
+    return np.concatenate([(U + V) / 2, (U - V) / 2])
+
+
+@pytest.mark.parametrize("L", [2, 4, 6])
+def test_generation_algebra_matches_oracle(L):
+    rng = np.random.default_rng(L)
+    tab = translation_table_ab5(L)
+    k = 2 * np.pi / 0.55
+    pos = np.array([[0.0, 0.0, 0.0], rng.normal(size=3) * 0.4])
+    nmax = 2 * L * (L + 2)
+    x = np.zeros(2 * nmax, dtype=complex)
+    x[nmax:] = rng.normal(size=nmax) + 1j * rng.normal(size=nmax)
+    ref = R.coupling_matvec_rows(L, pos, k, tab, x, 0, 1)
+    got = _emulate_wx(L, tab, pos[0], pos[1], k, x[nmax:])
+    assert np.max(np.abs(got - ref)) <= 1e-11 * np.max(np.abs(ref))

@@ -19,6 +19,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = BUILD / "libyasf_b200.so"
 INCLUDE = PKG.parent / "include"
+GEN = BUILD / "gen"  # build-time generated headers (panel_sched.h)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
@@ -43,7 +44,7 @@ def _nvcc() -> str:
 def _sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(
         INCLUDE.glob("*.h")
-    )
+    ) + [PKG / "panel_sched.py"]
 
 
 def _units() -> list[tuple[Path, list[str], Path]]:
@@ -70,11 +71,14 @@ def build(verbose: bool = False, force: bool = False, jobs: int | None = None) -
         return LIB
     nvcc = _nvcc()
     BUILD.mkdir(parents=True, exist_ok=True)
+    from yasf_b200.panel_sched import write_header
+
+    write_header(GEN / "panel_sched.h")
     units = _units()
 
     def compile_one(unit):
         src, extra, obj = unit
-        cmd = [nvcc, *NVCC_FLAGS, *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        cmd = [nvcc, *NVCC_FLAGS, *extra, "-I", str(INCLUDE), "-I", str(GEN), "-c", str(src), "-o", str(obj)]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src.name} {extra}:\n{res.stderr}")

@@ -333,12 +333,12 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
 
   // Generation terms for the tensor-core panel path (lmax <= 6).
   std::vector<float> gen_c1;
-  std::vector<unsigned> gen_meta;
+  std::vector<unsigned> gen_meta, gen_dst;
   {
-    const int bst = panel_build_terms(L, ab5, gen_c1, gen_meta);
+    const int bst = panel_build_terms(L, ab5, gen_c1, gen_meta, gen_dst);
     if (bst != YASF_OK) {
       delete plan;
-      set_error_text("internal: panel generation terms do not fit");
+      set_error_text("translation table does not follow the a5/b5 selection rules of the panel schedule");
       return bst;
     }
   }
@@ -374,6 +374,7 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     cudaFree(plan->d_pair_coef);
     cudaFree(plan->d_gen_c1);
     cudaFree(plan->d_gen_meta);
+    cudaFree(plan->d_gen_dst);
     delete plan;
     return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
   };
@@ -396,6 +397,7 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
   if (!gen_c1.empty()) {
     YASF_UPLOAD(plan->d_gen_c1, gen_c1);
     YASF_UPLOAD(plan->d_gen_meta, gen_meta);
+    YASF_UPLOAD(plan->d_gen_dst, gen_dst);
   }
 #undef YASF_UPLOAD
   if ((e = cudaMalloc(reinterpret_cast<void**>(&plan->d_leg), sizeof(LegendreTables))) != cudaSuccess)
@@ -417,6 +419,7 @@ extern "C" int yasf_plan_destroy(yasf_plan* plan) {
   cudaFree(plan->d_pair_coef);
   cudaFree(plan->d_gen_c1);
   cudaFree(plan->d_gen_meta);
+  cudaFree(plan->d_gen_dst);
   delete plan;
   return YASF_OK;
 }

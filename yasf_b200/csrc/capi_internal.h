@@ -29,8 +29,9 @@ struct yasf_plan {
   long long pair_terms = 0;
   // direct-form generation terms of the tau blocks Wa (a5) and Wb (b5) for the tensor-core panel,
   // one fixed list per generator thread ([term][thread]); null when lmax > 6
-  float* d_gen_c1 = nullptr;
-  unsigned* d_gen_meta = nullptr;
+  float* d_gen_c1 = nullptr;       // panel generation coefficients [slot][gen thread]
+  unsigned* d_gen_meta = nullptr;  // panel pair-table byte offsets [slot][gen thread]
+  unsigned* d_gen_dst = nullptr;   // panel store and phase offsets [3][step][gen thread]
 };
 
 namespace yasf {
@@ -76,6 +77,7 @@ int dispatch_contract(int lmax, int precision, bool regular, const ContractArgs&
 int validate_coupling(const yasf_plan* plan, int n_particles, const double* positions,
                       double k, int precision);
 
-int panel_build_terms(int L, const double* ab5, std::vector<float>& c1, std::vector<unsigned>& meta);
+int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::vector<unsigned>& goff,
+                      std::vector<unsigned>& dst);
 
 }  // namespace yasf

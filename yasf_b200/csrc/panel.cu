@@ -7,71 +7,118 @@
 
 namespace yasf {
 
-// Generation terms of the W blocks for the panel kernel, balanced over the 256 generator threads
-// (longest-processing-time assignment of whole entries) and laid out [term][thread].
-int panel_build_terms(int L, const double* ab5, std::vector<float>& c1, std::vector<unsigned>& meta) {
-  c1.clear();
-  meta.clear();
-  if (L < 1 || L > 6) return YASF_OK;  // no tensor-core panel beyond lmax 6
-  const int nmax = 2 * L * (L + 2), P = 2 * L + 1, DW = 4 * L + 1;
+// Generation data of the panel kernel from the build-time schedule (panel_sched.h). For every
+// generator thread and slot: the real coefficient and the byte offset of A[p][|d|] of one term of
+// the thread's item; for every step: the W-stage byte offsets of the P_r rows of the item's entry
+// and of its mirror, and the byte offset of the entry's phase e^{i d phi}. Wa coefficients are
+// real and Wb coefficients purely imaginary (a5 / b5 of the plan); the Wb value stored is b / i.
+// The mirror entry's coefficients are not stored: they equal the entry's (Wa) or their negatives
+// (Wb), which the kernel applies. Terms below 1e-12 of the largest coefficient cannot change a
+// TF32 entry and are dropped.
+template <int L>
+static int build_terms_for(const double* ab5, const unsigned short* entry, const unsigned char* wa,
+                           const unsigned char* wb, std::vector<float>& coef,
+                           std::vector<unsigned>& goff, std::vector<unsigned>& dst) {
+  using Sched = PanelSched<L>;
+  constexpr int S = Sched::kSlots, NS = Sched::kSteps;
+  const int nmax = 2 * L * (L + 2), P = 2 * L + 1;
   const int H = L * (L + 2), HP = pad8(H);
-  const int W_PLANE_F = (HP / 4) * (HP / 8) * 128 / 4;
-  const int TM = gen_terms_max(L);
-  auto m_of = [](int q) {
-    int l = 1;
+  auto lm = [](int q, int& l, int& m) {
+    l = 1;
     while ((l + 1) * (l + 1) - 1 <= q) ++l;
-    return q + 1 - l * l - l;
+    m = q + 1 - l * l - l;
   };
-  struct Term { float c; unsigned meta; };
-  std::vector<std::vector<Term>> entries;
-  double cmax = 0.0;  // terms below 1e-12 of the largest coefficient cannot change a TF32 entry
+  auto mirror = [&](int q) {
+    int l, m;
+    lm(q, l, m);
+    return l * l + l - 1 - m;
+  };
+  double cmax = 0.0;
   for (size_t q = 0; q < (size_t)nmax * nmax * P * 2; ++q) cmax = std::max(cmax, std::fabs(ab5[q]));
   const double cut = 1e-12 * cmax;
+  auto coefficient = [&](int which, int q1, int q2, int p, double& cr, double& ci) {
+    // A[(tau1=1,q1), (tau2=which+1,q2), p] = translation_ab5[n2][n1][p]
+    const size_t idx = ((size_t)(which * H + q2) * nmax + q1) * P + p;
+    cr = ab5[2 * idx];
+    ci = ab5[2 * idx + 1];
+    if (std::fabs(cr) <= cut) cr = 0.0;
+    if (std::fabs(ci) <= cut) ci = 0.0;
+  };
+  // the schedule relies on: coefficients only inside the selection rules, Wa real, Wb imaginary,
+  // and the mirror entry carrying the same Wa and the negated Wb coefficients
   for (int which = 0; which < 2; ++which)
     for (int q1 = 0; q1 < H; ++q1)
       for (int q2 = 0; q2 < H; ++q2) {
-        std::vector<Term> ts;
-        const int delta = m_of(q2) - m_of(q1) + 2 * L;
-        const unsigned dst = (unsigned)(which * 2 * W_PLANE_F + kmajor_offset(q1, q2, HP) / 4);
+        int l1, m1, l2, m2;
+        lm(q1, l1, m1);
+        lm(q2, l2, m2);
+        const int pmin = std::max(std::abs(l1 - l2), std::abs(m2 - m1));
         for (int p = 0; p < P; ++p) {
-          // coefficient A[(tau1=1,q1), (tau2=which+1,q2), p] = translation_ab5[n2][n1][p]
-          const size_t idx = ((size_t)(which * H + q2) * nmax + q1) * P + p;
-          double cr = ab5[2 * idx], ci = ab5[2 * idx + 1];
-          if (std::fabs(cr) <= cut) cr = 0.0;
-          if (std::fabs(ci) <= cut) ci = 0.0;
-          if (cr == 0.0 && ci == 0.0) continue;
-          if (cr != 0.0 && ci != 0.0) return YASF_ERR_INVALID_ARGUMENT;  // not real x i^k
-          const bool odd = cr == 0.0;
-          Term t;
-          t.c = (float)(odd ? -ci : cr);
-          t.meta = (unsigned)(p * DW + delta) | (odd ? kMetaOdd : 0u);
-          ts.push_back(t);
+          double cr, ci, mr, mi;
+          coefficient(which, q1, q2, p, cr, ci);
+          coefficient(which, mirror(q1), mirror(q2), p, mr, mi);
+          const bool in_rule = p >= pmin && p <= l1 + l2 && ((l1 + l2 + p) % 2 == 0) == (which == 0);
+          if (!in_rule && (cr != 0.0 || ci != 0.0)) return YASF_ERR_INVALID_ARGUMENT;
+          if ((which == 0 && ci != 0.0) || (which == 1 && cr != 0.0)) return YASF_ERR_INVALID_ARGUMENT;
+          const double sgn = which == 0 ? 1.0 : -1.0;
+          const double tol = 1e-12 * std::max(1.0, std::fabs(cr) + std::fabs(ci));
+          if (std::fabs(mr - sgn * cr) > tol || std::fabs(mi - sgn * ci) > tol)
+            return YASF_ERR_INVALID_ARGUMENT;
         }
-        if (ts.empty()) continue;
-        ts.front().meta |= kMetaFirst;
-        ts.back().meta |= kMetaLast | (dst << 13);
-        entries.push_back(ts);
       }
-  std::vector<int> order(entries.size());
-  for (size_t e = 0; e < entries.size(); ++e) order[e] = (int)e;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int x, int y) { return entries[x].size() > entries[y].size(); });
-  std::vector<std::vector<Term>> per(kGenThreads);
-  for (int e : order) {
-    int best = 0;
-    for (int th = 1; th < kGenThreads; ++th)
-      if (per[th].size() < per[best].size()) best = th;
-    per[best].insert(per[best].end(), entries[e].begin(), entries[e].end());
-    if ((int)per[best].size() > TM) return YASF_ERR_UNSUPPORTED;
-  }
-  c1.assign((size_t)TM * kGenThreads, 0.f);
-  meta.assign((size_t)TM * kGenThreads, 0u);
-  for (int th = 0; th < kGenThreads; ++th)
-    for (size_t t = 0; t < per[th].size(); ++t) {
-      c1[t * kGenThreads + th] = per[th][t].c;
-      meta[t * kGenThreads + th] = per[th][t].meta;
+  coef.assign((size_t)S * kGenThreads, 0.f);
+  goff.assign((size_t)S * kGenThreads, 0u);
+  dst.assign((size_t)3 * NS * kGenThreads, 0u);
+  for (int th = 0; th < kGenThreads; ++th) {
+    const int w = th >> 5, lane = th & 31;
+    int base = 0;
+    for (int k = 0; k < NS; ++k) {
+      const unsigned e = entry[((size_t)w * NS + k) * 32 + lane];
+      const int q1 = (int)(e >> 8), q2 = (int)(e & 255);
+      const bool real = q1 < H && q2 < H;
+      const int mq1 = real ? mirror(q1) : q1, mq2 = real ? mirror(q2) : q2;
+      int l1 = 0, m1 = 0, l2 = 0, m2 = 0;
+      if (real) {
+        lm(q1, l1, m1);
+        lm(q2, l2, m2);
+      }
+      dst[(size_t)k * kGenThreads + th] = (unsigned)kmajor_offset(q1, q2, 2 * HP);
+      dst[(size_t)(NS + k) * kGenThreads + th] = (unsigned)kmajor_offset(mq1, mq2, 2 * HP);
+      dst[(size_t)(2 * NS + k) * kGenThreads + th] = (unsigned)((P * P + 2 * L + (m2 - m1)) * 8);
+      if (real) {
+        const int pmin = std::max(std::abs(l1 - l2), std::abs(m2 - m1));
+        int na = 0, nb = 0;
+        for (int p = pmin; p <= l1 + l2; ++p) {
+          const int which = ((l1 + l2 + p) % 2 == 0) ? 0 : 1;
+          double cr, ci;
+          coefficient(which, q1, q2, p, cr, ci);
+          const int slot = which == 0 ? base + na++ : base + wa[k] + nb++;
+          if (na > wa[k] || nb > wb[k]) return YASF_ERR_INVALID_ARGUMENT;
+          coef[(size_t)slot * kGenThreads + th] = (float)(which == 0 ? cr : ci);
+          goff[(size_t)slot * kGenThreads + th] = (unsigned)((p * P + std::abs(m2 - m1)) * 8);
+        }
+      }
+      base += wa[k] + wb[k];
     }
+    if (base != S) return YASF_ERR_INVALID_ARGUMENT;
+  }
   return YASF_OK;
+}
+
+int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::vector<unsigned>& goff,
+                      std::vector<unsigned>& dst) {
+  coef.clear();
+  goff.clear();
+  dst.clear();
+  switch (L) {
+    case 1: return build_terms_for<1>(ab5, kPanelEntry1, kPanelStepWa1, kPanelStepWb1, coef, goff, dst);
+    case 2: return build_terms_for<2>(ab5, kPanelEntry2, kPanelStepWa2, kPanelStepWb2, coef, goff, dst);
+    case 3: return build_terms_for<3>(ab5, kPanelEntry3, kPanelStepWa3, kPanelStepWb3, coef, goff, dst);
+    case 4: return build_terms_for<4>(ab5, kPanelEntry4, kPanelStepWa4, kPanelStepWb4, coef, goff, dst);
+    case 5: return build_terms_for<5>(ab5, kPanelEntry5, kPanelStepWa5, kPanelStepWb5, coef, goff, dst);
+    case 6: return build_terms_for<6>(ab5, kPanelEntry6, kPanelStepWa6, kPanelStepWb6, coef, goff, dst);
+    default: return YASF_OK;  // no tensor-core panel beyond lmax 6
+  }
 }
 
 template <int L>
@@ -146,9 +193,10 @@ extern "C" int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const d
   pa.pos = positions;
   pa.leg = plan->d_leg;
   pa.xp = reinterpret_cast<const float*>(ws);
-  if (!plan->d_gen_c1) return YASF_ERR_UNSUPPORTED;
-  pa.gen_c1 = plan->d_gen_c1;
-  pa.gen_meta = plan->d_gen_meta;
+  if (!plan->d_gen_c1 || !plan->d_gen_dst) return YASF_ERR_UNSUPPORTED;
+  pa.gen_coef = plan->d_gen_c1;
+  pa.gen_goff = plan->d_gen_meta;
+  pa.gen_dst = plan->d_gen_dst;
   pa.x = reinterpret_cast<const double2*>(x);
   pa.tmat = reinterpret_cast<const double2*>(tmat);
   pa.y = reinterpret_cast<double2*>(y);

@@ -1,50 +1,81 @@
 // Multi-right-hand-side coupling on the 5th-generation tensor cores (tcgen05, kind::tf32).
 //
 // For a panel of R right-hand sides the direct form of the translation is used: every pair block
-// W_ij is generated once (complex64, from the pair table G[p][delta] = Pn_p^{|delta|} h_p
+// W_ij is generated once (FP32, from A[p][d] = Pn_p^d(cos theta) h_p(k r), the phases
 // e^{i delta phi} and the a5/b5 coefficients, yasfpy/functions/cpu_numba.py:50-93) and applied to
-// the whole nmax x R panel of the source's coefficients. With the a5 (tau1 == tau2) and b5
-// (tau1 != tau2) blocks Wa, Wb of W_ij = [[Wa, Wb], [Wb, Wa]], the receiver's panel obeys
-//   Y1 += Wa X1 + Wb X2,   Y2 += Wb X1 + Wa X2        (X1, X2: the tau = 1, 2 halves).
-// The MMA computes the transposed products Y^T[r][n1] += X^T[r][n2] W[n1][n2]: the right-hand
-// sides are the M dimension (64 per block), the receiving modes the N dimension, the source modes
-// K. Complex products are four real products; the imaginary-part subtraction uses the MMA's
-// A-negate bit. Accumulators stay in tensor memory for the whole source loop.
+// the whole nmax x 64 panel of the source's coefficients. With the a5 (tau1 == tau2) and b5
+// (tau1 != tau2) blocks Wa, Wb of W_ij = [[Wa, Wb], [Wb, Wa]],
+//   Y1 = Wa X1 + Wb X2,  Y2 = Wb X1 + Wa X2   (X1, X2: the tau = 1, 2 halves)
+// is computed from two products instead of four:
+//   U = P S, V = Q D  with  P = Wa + Wb, Q = Wa - Wb, S = X1 + X2, D = X1 - X2,
+//   Y1 = (U + V) / 2, Y2 = (U - V) / 2.
+// The MMAs compute transposed products D^T[m][n] += A[m][k] B[n][k] with M = 128 rows
+// A = [S_r; S_i] (64 right-hand sides, real parts then imaginary parts), N = 2 HP rows
+// B = [P_r; P_i] and K = HP source modes, so one MMA yields all four real products of the complex
+// product; the epilogue combines them (U_r = S_r P_r - S_i P_i, U_i = S_r P_i + S_i P_r).
+// Accumulators stay in tensor memory for the whole source loop.
 //
-// Roles (160 threads): warps 0-3 generate the pair table and W_ij into shared memory (canonical
-// K-major no-swizzle layout, values rounded to TF32) and finally read the accumulators; warp 4
-// owns tensor memory and its elected thread issues the MMAs. Source panels X_j arrive by
-// cp.async.bulk; two stages of (X_j, W_ij) are in flight. Every wait is bounded: a timeout sets
+// Roles (640 threads): warps 0-15 generate P and Q of W_ij into shared memory (canonical K-major
+// no-swizzle layout, values rounded to TF32) following the build-time schedule of panel_sched.h:
+// every thread keeps its coefficients and pair-table offsets in registers, computes an entry and
+// its mirror (l, -m) from one set of loads, and a warp's 32 stores of a step hit 32 different
+// banks; warps 0-3 also read the accumulators at the end. Warp 16 owns tensor memory and its
+// elected thread issues the MMAs. Warps 17 and 18 compute the pair tables of alternate pairs;
+// warp 19 issues the cp.async.bulk copies of the source panels. Three source-panel stages, two W
+// stages and four pair-table stages are in flight. Every wait is bounded in time: a timeout sets
 // the error word, every role stops, the result is written as NaN and tensor memory is freed.
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include "coupling.cuh"
+#include "panel_sched.h"
 
 namespace yasf {
 
 __host__ __device__ constexpr int half_modes(int L) { return L * (L + 2); }
 __host__ __device__ constexpr int pad8(int v) { return (v + 7) & ~7; }
+__host__ __device__ constexpr int tmem_cols(int c) {
+  return c <= 32 ? 32 : (c <= 64 ? 64 : (c <= 128 ? 128 : (c <= 256 ? 256 : 512)));
+}
 
-// Panel geometry for lmax L (all sizes in bytes unless noted).
+// Panel geometry for lmax L (sizes in bytes unless noted).
 template <int L>
 struct PanelGeom {
-  static constexpr int H = half_modes(L);       // modes per tau half
-  static constexpr int HP = pad8(H);            // padded to the MMA granularity
-  static constexpr int M = 64;                  // right-hand sides per block
-  static constexpr int P = 2 * L + 1;           // orders p
-  static constexpr int DW = 4 * L + 1;          // deltas
-  static constexpr int X_LBO = (M / 8) * 128;   // K-chunk stride of an X plane
-  static constexpr int X_PLANE = (HP / 4) * X_LBO;
-  static constexpr int X_STAGE = 4 * X_PLANE;   // X1r, X1i, X2r, X2i
-  static constexpr int W_LBO = (HP / 8) * 128;  // K-chunk stride of a W plane
-  static constexpr int W_PLANE = (HP / 4) * W_LBO;
-  static constexpr int W_STAGE = 4 * W_PLANE;   // War, Wai, Wbr, Wbi
-  static constexpr int G_STAGE = P * DW * 8;    // pair table (float2)
-  static constexpr int TMEM_COLS = 4 * HP <= 32 ? 32 : (4 * HP <= 64 ? 64 : (4 * HP <= 128 ? 128 : 256));
-  static constexpr int SMEM = 2 * X_STAGE + 2 * W_STAGE + 2 * G_STAGE + 256;
-  static constexpr int W_PLANE_F = W_PLANE / 4;
+  static constexpr int H = half_modes(L);        // modes per tau half
+  static constexpr int HP = pad8(H);             // padded to the MMA granularity
+  static constexpr int M = 64;                   // right-hand sides per block
+  static constexpr int P = 2 * L + 1;            // orders p
+  static constexpr int KS = HP / 8;              // K steps of 8 TF32 columns
+  // A operands [S_r; S_i], [D_r; D_i]: 128 rows x HP columns
+  static constexpr int A_ROWS = 128;
+  static constexpr int A_LBO = (A_ROWS / 8) * 128;   // bytes between 4-column K chunks
+  static constexpr int A_BYTES = A_ROWS * HP * 4;
+  static constexpr int X_STAGE = 2 * A_BYTES;        // one source panel (S and D operands)
+  static constexpr int X_STAGES = 3;
+  // B operands [P_r; P_i], [Q_r; Q_i]: 2 HP rows x HP columns
+  static constexpr int B_ROWS = 2 * HP;
+  static constexpr int B_LBO = (B_ROWS / 8) * 128;
+  static constexpr int B_BYTES = B_ROWS * HP * 4;
+  static constexpr int W_STAGE = 2 * B_BYTES;
+  static constexpr int W_STAGES = 2;
+  static constexpr int IM_OFF = (HP / 8) * 128;      // row HP + q of a B operand vs row q
+  // pair table: A[p][d] at p*P + d, e^{i delta phi} at P*P + 2L + delta (float2)
+  static constexpr int G_STAGE = (P * P + 4 * L + 1) * 8;
+  static constexpr int G_STAGES = 4;
+  static constexpr int LEG_BYTES = ((2 * P * P + P) * 4 + 15) & ~15;
+  static constexpr int TMEM_COLS = tmem_cols(4 * HP);
+  static constexpr int X_OFF = 0;
+  static constexpr int W_OFF = X_OFF + X_STAGES * X_STAGE;
+  static constexpr int G_OFF = W_OFF + W_STAGES * W_STAGE;
+  static constexpr int LEG_OFF = G_OFF + G_STAGES * G_STAGE;
+  static constexpr int BAR_OFF = (LEG_OFF + LEG_BYTES + 15) & ~15;
+  static constexpr int SMEM = BAR_OFF + 256;
+  static_assert(SMEM <= 232448, "panel shared memory exceeds the per-block limit");
+  static_assert(X_STAGE % 1024 == 0 && W_STAGE % 1024 == 0, "operand stages must stay aligned");
+  // epilogue exchange of the imaginary-row accumulators (reuses the source-panel stages)
+  static constexpr int XCH_STRIDE = 4 * HP + 1;  // floats per row (odd: conflict-free)
+  static_assert(64 * XCH_STRIDE * 4 <= X_STAGES * X_STAGE, "exchange buffer does not fit");
 };
 
 // Byte offset of element (row, k) in a canonical K-major no-swizzle operand with `rows` rows.
@@ -59,6 +90,13 @@ __device__ __forceinline__ float to_tf32(float v) {
   return __uint_as_float(r);
 }
 
+constexpr int kGenWarps = 16;
+constexpr int kGenThreads = 32 * kGenWarps;
+constexpr int kMmaWarp = 16;
+constexpr int kGeomWarp0 = 17;  // warps 17, 18: pair tables of alternate pairs
+constexpr int kLoadWarp = 19;   // source-panel copies
+constexpr int kPanelThreads = 640;
+
 struct PanelArgs {
   int n_particles;
   int nmax;
@@ -69,8 +107,10 @@ struct PanelArgs {
   const double* pos;
   const LegendreTables* leg;
   const float* xp;               // source panels, [group][source][X_STAGE bytes]
-  const float* gen_c1;           // [TM][256] generation coefficients, thread-minor
-  const unsigned* gen_meta;      // [TM][256] generation meta words
+  const float* gen_coef;         // [slot][gen thread] generation coefficients (Wa real, Wb / i)
+  const unsigned* gen_goff;      // [slot][gen thread] pair-table byte offsets
+  const unsigned* gen_dst;       // [3][step][gen thread] W-stage byte offsets of the item's entry
+                                 // and mirror P_r rows, pair-table byte offset of its phase
   const double2* x;              // input columns (for the master epilogue)
   const double2* tmat;           // T (N*nmax), master epilogue when non-null
   double2* y;                    // output columns
@@ -120,6 +160,10 @@ __device__ __forceinline__ void named_sync(int id, int threads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 template <int N>
 __device__ __forceinline__ void tmem_ld32(unsigned addr, float* v);
 template <>
@@ -134,52 +178,162 @@ __device__ __forceinline__ void tmem_ld32<8>(unsigned addr, float* v) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for phase `parity` of `bar`, bounded in time (about one second) rather than in polls.
+// Each try_wait may suspend the thread for up to 2 us (it resumes when the phase completes), so
+// waiting warps take few issue slots.
+__device__ __forceinline__ bool panel_wait(unsigned long long* bar, unsigned parity) {
+  const unsigned a = smem_addr(bar);
+  unsigned long long t0 = 0;
+#pragma unroll 1
+  for (unsigned spin = 0;; ++spin) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity), "r"(2000u)
+        : "memory");
+    if (done) return true;
+    if (spin == 0) {
+      t0 = global_ns();
+    } else if ((spin & 7) == 0 && global_ns() - t0 > 1000000000ull) {
+      return false;
+    }
+  }
+}
+
 // Bounded wait that also gives up when another role has already aborted.
 __device__ __forceinline__ bool wait_or_abort(unsigned long long* bar, unsigned parity,
                                               volatile int* abort_flag) {
   if (*abort_flag) return false;
-  if (mbar_wait(bar, parity)) return true;
+  if (panel_wait(bar, parity)) return true;
   *abort_flag = 1;
   return false;
 }
 
-// ---- the kernel ---------------------------------------------------------------------------
-// Threads: warps 0-7 generate W (256 threads, each with a fixed, register-resident list of
-// generation terms: coefficient, pair-table offset, rotation, first/last flags, destination);
-// warps 0-3 also read the accumulators at the end. Warp 8 owns tensor memory and issues the
-// MMAs. Warp 9 issues the source-panel copies and computes the pair table one pair ahead.
-constexpr int kGenThreads = 256;
-constexpr int kPanelThreads = 320;
-__host__ __device__ constexpr int gen_terms_max(int L) {
-  return L <= 1 ? 2 : (L == 2 ? 4 : (L == 3 ? 8 : (L == 4 ? 12 : (L == 5 ? 28 : 56))));
+// Pair-table load. Not volatile: the address operand carries the ordering (it is derived from a
+// value produced after the stage's mbarrier wait), so the compiler may batch these loads ahead of
+// the previous step's stores.
+__device__ __forceinline__ float2 lds_f2(unsigned addr) {
+  float2 v;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
 }
-// meta word: [0,10) pair-table offset, 10 rotate (multiply by i), 11 first term of an entry,
-// 12 last term of an entry, [13,32) destination float index in the W stage (real part; the
-// imaginary part is one plane further).
-constexpr unsigned kMetaOdd = 1u << 10, kMetaFirst = 1u << 11, kMetaLast = 1u << 12;
+__device__ __forceinline__ void sts_f32(unsigned addr, float v) {
+  asm volatile("st.shared.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
+// Opaque copy: values derived from it cannot be computed before this point in program order.
+__device__ __forceinline__ unsigned after_wait(unsigned v) {
+  unsigned r;
+  asm volatile("mov.b32 %0, %1;" : "=r"(r) : "r"(v));
+  return r;
+}
 
+// One schedule step of W generation for this thread: the item's TA Wa terms and TB Wb terms
+// (real coefficients on A[p][|d|]) into Sa, Sb; then, with E = e^{i d phi},
+//   entry:  Wa = E Sa,       Wb = i E Sb
+//   mirror: Wa' = conj(E) Sa, Wb' = -i conj(E) Sb
+// and P = Wa + Wb, Q = Wa - Wb of both to their four operand rows each.
+template <int BASE, int TA, int TB, int S, int IM_OFF, int B_BYTES>
+__device__ __forceinline__ void gen_step(const float (&gc)[S], const unsigned (&go)[S], unsigned gbase,
+                                         unsigned eoff, unsigned dst, unsigned dstm) {
+  float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
+#pragma unroll
+  for (int q = 0; q < TA; ++q) {
+    const float2 g = lds_f2(gbase + go[BASE + q]);
+    ar = fmaf(gc[BASE + q], g.x, ar);
+    ai = fmaf(gc[BASE + q], g.y, ai);
+  }
+#pragma unroll
+  for (int q = 0; q < TB; ++q) {
+    const float2 g = lds_f2(gbase + go[BASE + TA + q]);
+    br = fmaf(gc[BASE + TA + q], g.x, br);
+    bi = fmaf(gc[BASE + TA + q], g.y, bi);
+  }
+  const float2 e = lds_f2(gbase + eoff);
+  {
+    const float ur = e.x * ar - e.y * ai, ui = e.x * ai + e.y * ar;
+    const float vr = e.x * br - e.y * bi, vi = e.x * bi + e.y * br;
+    sts_f32(dst, to_tf32(ur - vi));
+    sts_f32(dst + IM_OFF, to_tf32(ui + vr));
+    sts_f32(dst + B_BYTES, to_tf32(ur + vi));
+    sts_f32(dst + B_BYTES + IM_OFF, to_tf32(ui - vr));
+  }
+  {
+    const float ur = e.x * ar + e.y * ai, ui = e.x * ai - e.y * ar;
+    const float vr = e.x * br + e.y * bi, vi = e.x * bi - e.y * br;
+    sts_f32(dstm, to_tf32(ur + vi));
+    sts_f32(dstm + IM_OFF, to_tf32(ui - vr));
+    sts_f32(dstm + B_BYTES, to_tf32(ur - vi));
+    sts_f32(dstm + B_BYTES + IM_OFF, to_tf32(ui + vr));
+  }
+}
+
+// The pair table of one pair, lane d (< P): A[p][d] = Pn_p^d(cos theta) h_p(x) for p >= d at
+// p*P + d, and the phases e^{+-i d phi} at P*P + 2L +- d.
+template <int L>
+__device__ __forceinline__ void pair_table(float2* g, int d, float ct, float st, float cdp, float sdp,
+                                           float x, float sx, float cx, const float* legA,
+                                           const float* legB, const float* legS) {
+  constexpr int P = 2 * L + 1;
+  g[P * P + 2 * L + d] = make_float2(cdp, sdp);
+  if (d) g[P * P + 2 * L - d] = make_float2(cdp, -sdp);
+  const float ix = __fdividef(1.0f, x);
+  float hr0 = sx * ix, hi0 = -cx * ix;                                         // h_0
+  float hr1 = (sx - x * cx) * ix * ix, hi1 = -(cx + x * sx) * ix * ix;         // h_1
+  float Pp = 0.f, Pc = 0.f, stp = 1.f;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    if (p == d) Pc = legS[d] * stp;
+    if (p < d) stp *= st;
+    if (p >= d) {
+      g[p * P + d] = make_float2(Pc * hr0, Pc * hi0);
+      if (p + 1 < P) {
+        const float Pn = legA[p * P + d] * ct * Pc - legB[p * P + d] * Pp;
+        Pp = Pc;
+        Pc = Pn;
+      }
+    }
+    if (p + 1 < P) {
+      const float f = (float)(2 * p + 3) * ix;
+      const float nr = f * hr1 - hr0, ni = f * hi1 - hi0;
+      hr0 = hr1; hi0 = hi1; hr1 = nr; hi1 = ni;
+    }
+  }
+}
+
+// ---- the kernel ---------------------------------------------------------------------------
 template <int L>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   using G = PanelGeom<L>;
-  constexpr int H = G::H, HP = G::HP, M = G::M, P = G::P, DW = G::DW;
-  constexpr int TM = gen_terms_max(L);
-  constexpr int PW = G::W_PLANE / 4;  // floats per W plane
+  using Sched = PanelSched<L>;
+  static_assert(Sched::kWarps == kGenWarps, "schedule built for another warp count");
+  constexpr int H = G::H, HP = G::HP, P = G::P, KS = G::KS;
+  constexpr int S = Sched::kSlots, NS = Sched::kSteps;
   extern __shared__ __align__(1024) unsigned char panel_smem[];
-  unsigned char* xs = panel_smem;                               // [2][X_STAGE]
-  unsigned char* ws = xs + 2 * G::X_STAGE;                      // [2][W_STAGE]
-  float2* gt = reinterpret_cast<float2*>(ws + 2 * G::W_STAGE);  // [2][P*DW]
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(
-      reinterpret_cast<unsigned char*>(gt) + 2 * G::G_STAGE);
-  unsigned long long* xfull = bars;       // [2] source panel landed
-  unsigned long long* wfull = bars + 2;   // [2] W generated
-  unsigned long long* empty = bars + 4;   // [2] MMAs of the stage done (X and W reusable)
-  unsigned long long* gfull = bars + 6;   // [2] pair table ready
-  unsigned long long* gempty = bars + 8;  // [2] pair table consumed
-  unsigned long long* accum = bars + 10;  // accumulators final
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 12);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 13);
-  volatile int* gen_stop = reinterpret_cast<volatile int*>(bars + 14);
-  volatile int* last_issued = reinterpret_cast<volatile int*>(bars + 15);
+  unsigned char* xs = panel_smem + G::X_OFF;                                  // [3][X_STAGE]
+  unsigned char* ws = panel_smem + G::W_OFF;                                  // [2][W_STAGE]
+  unsigned char* gt = panel_smem + G::G_OFF;                                  // [4][G_STAGE]
+  float* legA = reinterpret_cast<float*>(panel_smem + G::LEG_OFF);            // [P][P]
+  float* legB = legA + P * P;
+  float* legS = legB + P * P;
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(panel_smem + G::BAR_OFF);
+  unsigned long long* xfull = bars;        // [3] source panel landed
+  unsigned long long* xempty = bars + 3;   // [3] MMAs of the panel done
+  unsigned long long* wfull = bars + 6;    // [2] W generated (one arrival per generator warp)
+  unsigned long long* wempty = bars + 8;   // [2] MMAs of the W stage done
+  unsigned long long* gfull = bars + 10;   // [4] pair table ready
+  unsigned long long* gempty = bars + 14;  // [4] pair table consumed (one arrival per generator warp)
+  unsigned long long* accum = bars + 18;   // accumulators final
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 19);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 20);
+  volatile int* issued = reinterpret_cast<volatile int*>(bars + 21);  // [3] newest pair loaded per stage
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -188,26 +342,45 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   const int N = a.n_particles;
   const int n_iter = N - 1;    // every source but the receiver itself
 
-  // generation terms of this thread (registers)
-  float gc[TM];
-  unsigned gm[TM];
+  // generation data of this thread (registers)
+  float gc[S];
+  unsigned go[S];
+  unsigned gd[NS], gm[NS], ge[NS];
   if (tid < kGenThreads) {
 #pragma unroll
-    for (int t = 0; t < TM; ++t) {
-      gc[t] = __ldg(a.gen_c1 + t * kGenThreads + tid);
-      gm[t] = __ldg(a.gen_meta + t * kGenThreads + tid);
+    for (int q = 0; q < S; ++q) {
+      gc[q] = __ldg(a.gen_coef + q * kGenThreads + tid);
+      go[q] = __ldg(a.gen_goff + q * kGenThreads + tid);
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      gd[k] = smem_addr(ws) + __ldg(a.gen_dst + k * kGenThreads + tid);
+      gm[k] = smem_addr(ws) + __ldg(a.gen_dst + (NS + k) * kGenThreads + tid);
+      ge[k] = __ldg(a.gen_dst + (2 * NS + k) * kGenThreads + tid);
     }
   }
-  for (int o = tid; o < (2 * G::W_STAGE) / 16; o += blockDim.x)
+  // zero both W stages (padding rows and columns stay zero), Legendre tables to shared memory
+  for (int o = tid; o < (G::W_STAGES * G::W_STAGE) / 16; o += blockDim.x)
     reinterpret_cast<float4*>(ws)[o] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int o = tid; o < P * P; o += blockDim.x) {
+    const int p = o / P, d = o - (o / P) * P;
+    legA[o] = (float)a.leg->alpha[p * kLegStride + d];
+    legB[o] = (float)a.leg->beta[p * kLegStride + d];
+  }
+  for (int o = tid; o < P; o += blockDim.x) legS[o] = (float)a.leg->start[o];
   if (tid == 0) {
-    for (int b = 0; b < 11; ++b) mbar_init(&bars[b], 1);
+    for (int b = 0; b < 3; ++b) mbar_init(&xfull[b], 1);
+    for (int b = 0; b < 3; ++b) mbar_init(&xempty[b], 1);
+    for (int b = 0; b < 2; ++b) mbar_init(&wfull[b], kGenWarps);
+    for (int b = 0; b < 2; ++b) mbar_init(&wempty[b], 1);
+    for (int b = 0; b < 4; ++b) mbar_init(&gfull[b], 1);
+    for (int b = 0; b < 4; ++b) mbar_init(&gempty[b], kGenWarps);
+    mbar_init(accum, 1);
     *abort_flag = 0;
-    *gen_stop = 0;
-    *last_issued = -1;
+    for (int b = 0; b < 3; ++b) issued[b] = -1;
     mbar_fence_init();
   }
-  if (warp == 8) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(tmem_slot)),
                  "r"(G::TMEM_COLS)
@@ -220,206 +393,205 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
 
-  if (warp < 8) {
+  if (warp < kGenWarps) {
     // ===================== W generation =====================
+    const unsigned gt0 = smem_addr(gt);
     for (int t = 0; t < n_iter; ++t) {
-      const int s = t & 1;
-      const unsigned k = (unsigned)(t >> 1);
-      if (tid == 0) {
-        bool ok = t < 2 || wait_or_abort(&empty[s], (k - 1) & 1, abort_flag);
-        ok = ok && wait_or_abort(&gfull[s], k & 1, abort_flag);
-        if (!ok) *gen_stop = 1;
+      const int sw = t & 1, sg = t & 3;
+      int ok = 1;
+      if (lane == 0) {
+        ok = (t < 2 || wait_or_abort(&wempty[sw], (unsigned)(((t >> 1) - 1) & 1), abort_flag)) &&
+             wait_or_abort(&gfull[sg], (unsigned)((t >> 2) & 1), abort_flag);
       }
-      named_sync(1, kGenThreads);
-      if (*gen_stop) break;
-      const float2* g = gt + s * (P * DW);
-      float* wst = reinterpret_cast<float*>(ws + s * G::W_STAGE);
-      float ar = 0.f, ai = 0.f;
-#pragma unroll
-      for (int q = 0; q < TM; ++q) {
-        const unsigned mt = gm[q];
-        const float2 gv = g[mt & 1023u];
-        const bool odd = (mt & kMetaOdd) != 0;
-        const float av = odd ? gv.y : gv.x;
-        const float bv = odd ? -gv.x : gv.y;
-        if (mt & kMetaFirst) { ar = 0.f; ai = 0.f; }
-        ar = fmaf(gc[q], av, ar);
-        ai = fmaf(gc[q], bv, ai);
-        if (mt & kMetaLast) {
-          const unsigned dst = mt >> 13;
-          wst[dst] = to_tf32(ar);
-          wst[dst + PW] = to_tf32(ai);
-        }
-      }
+      __syncwarp();  // orders the other lanes' reads after lane 0's acquire
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      const unsigned gbase = after_wait(gt0 + (unsigned)(sg * G::G_STAGE));
+      const unsigned woff = (unsigned)(sw * G::W_STAGE);
+#define YASF_GEN_STEP(k, base, ta, tb) \
+  gen_step<base, ta, tb, S, G::IM_OFF, G::B_BYTES>(gc, go, gbase, ge[k], gd[k] + woff, gm[k] + woff);
+      if constexpr (L == 1) { YASF_PANEL_STEPS_1(YASF_GEN_STEP) }
+      if constexpr (L == 2) { YASF_PANEL_STEPS_2(YASF_GEN_STEP) }
+      if constexpr (L == 3) { YASF_PANEL_STEPS_3(YASF_GEN_STEP) }
+      if constexpr (L == 4) { YASF_PANEL_STEPS_4(YASF_GEN_STEP) }
+      if constexpr (L == 5) { YASF_PANEL_STEPS_5(YASF_GEN_STEP) }
+      if constexpr (L == 6) { YASF_PANEL_STEPS_6(YASF_GEN_STEP) }
+#undef YASF_GEN_STEP
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      named_sync(1, kGenThreads);
-      if (tid == 0) {
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&wfull[s])) : "memory");
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&gempty[s])) : "memory");
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&wfull[sw]);
+        mbar_arrive(&gempty[sg]);
       }
     }
-  } else if (warp == 8) {
+  } else if (warp == kMmaWarp) {
     // ===================== MMA issuer =====================
     if (lane == 0) {
-      constexpr int KS = HP / 8;
-      constexpr unsigned idesc = umma_idesc_tf32(M, HP, false);
-      constexpr unsigned idesc_neg = umma_idesc_tf32(M, HP, true);
-      unsigned long long dx0[4], dw0[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        dx0[q] = umma_desc(smem_addr(xs) + q * G::X_PLANE, G::X_LBO, 128);
-        dw0[q] = umma_desc(smem_addr(ws) + q * G::W_PLANE, G::W_LBO, 128);
-      }
-      constexpr unsigned long long xs_step = (unsigned long long)(G::X_STAGE >> 4);
-      constexpr unsigned long long ws_step = (unsigned long long)(G::W_STAGE >> 4);
-      constexpr unsigned long long xk = (unsigned long long)((2 * G::X_LBO) >> 4);
-      constexpr unsigned long long wk = (unsigned long long)((2 * G::W_LBO) >> 4);
+      constexpr unsigned idesc = umma_idesc_tf32(128, 2 * HP, false);
+      const unsigned long long da0 = umma_desc(smem_addr(xs), G::A_LBO, 128);
+      const unsigned long long db0 = umma_desc(smem_addr(ws), G::B_LBO, 128);
+      constexpr unsigned long long a_op = (unsigned long long)(G::A_BYTES >> 4);
+      constexpr unsigned long long b_op = (unsigned long long)(G::B_BYTES >> 4);
+      constexpr unsigned long long ak = (unsigned long long)((2 * G::A_LBO) >> 4);
+      constexpr unsigned long long bk = (unsigned long long)((2 * G::B_LBO) >> 4);
       for (int t = 0; t < n_iter; ++t) {
-        const int s = t & 1;
-        const unsigned ph = (unsigned)((t >> 1) & 1);
-        if (!wait_or_abort(&xfull[s], ph, abort_flag)) break;
-        if (!wait_or_abort(&wfull[s], ph, abort_flag)) break;
+        const int sx = t % 3, sw = t & 1;
+        if (!wait_or_abort(&xfull[sx], (unsigned)((t / 3) & 1), abort_flag)) break;
+        if (!wait_or_abort(&wfull[sw], (unsigned)((t >> 1) & 1), abort_flag)) break;
         tc_fence_after();
-        // (x plane, w plane, accumulator region, negate A): Y1 = Wa X1 + Wb X2, Y2 = Wb X1 + Wa X2
-        constexpr int XP[16] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3};
-        constexpr int WP[16] = {0, 1, 2, 3, 1, 0, 3, 2, 2, 3, 0, 1, 3, 2, 1, 0};
-        constexpr int NG[16] = {0, 1, 0, 1, 0, 0, 0, 0, 0, 1, 0, 1, 0, 0, 0, 0};
+        const unsigned long long dx = da0 + (unsigned long long)sx * (unsigned long long)(G::X_STAGE >> 4);
+        const unsigned long long dw = db0 + (unsigned long long)sw * (unsigned long long)(G::W_STAGE >> 4);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const unsigned dcol = tmem + (unsigned)((q >> 2) * HP);
-          const unsigned long long da0 = dx0[XP[q]] + (unsigned long long)s * xs_step;
-          const unsigned long long db0 = dw0[WP[q]] + (unsigned long long)s * ws_step;
-#pragma unroll
-          for (int kk = 0; kk < KS; ++kk) {
-            const unsigned acc = (t == 0 && (q & 3) == 0 && kk == 0) ? 0u : 1u;
-            umma_tf32(dcol, da0 + kk * xk, db0 + kk * wk, NG[q] ? idesc_neg : idesc, acc);
-          }
+        for (int kk = 0; kk < KS; ++kk) {
+          const unsigned acc = (t == 0 && kk == 0) ? 0u : 1u;
+          umma_tf32(tmem, dx + kk * ak, dw + kk * bk, idesc, acc);                       // [S;Si] [P;Pi]
+          umma_tf32(tmem + 2 * HP, dx + a_op + kk * ak, dw + b_op + kk * bk, idesc, acc);  // [D;Di] [Q;Qi]
         }
-        umma_commit(&empty[s]);
+        umma_commit(&xempty[sx]);
+        umma_commit(&wempty[sw]);
       }
       umma_commit(accum);
     }
     __syncwarp();
+  } else if (warp == kLoadWarp) {
+    // ===================== source panels =====================
+    if (lane == 0) {
+      for (int t = 0; t < n_iter; ++t) {
+        const int sx = t % 3;
+        const int j = t < i ? t : t + 1;
+        if (*abort_flag) break;
+        if (t >= 3 && !wait_or_abort(&xempty[sx], (unsigned)(((t / 3) - 1) & 1), abort_flag)) break;
+        const unsigned char* src =
+            reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)grp * N + j) * G::X_STAGE;
+        issued[sx] = t;  // written before the copy: the next load into this stage waits for its MMAs
+        bulk_load(xs + sx * G::X_STAGE, src, G::X_STAGE, &xfull[sx]);
+      }
+    }
+    __syncwarp();
   } else {
-    // ===================== source panels + pair table =====================
+    // ===================== pair tables (two warps take alternate pairs) =====================
+    const int par = warp - kGeomWarp0;
     const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
-    for (int t = 0; t < n_iter; ++t) {
-      const int s = t & 1;
-      const unsigned k = (unsigned)(t >> 1);
+    const float kf = (float)a.k;
+    for (int t = par; t < n_iter; t += 2) {
+      const int sg = t & 3;
       const int j = t < i ? t : t + 1;
       int ok = 1;
-      if (lane == 0) {
-        ok = t < 2 || wait_or_abort(&empty[s], (k - 1) & 1, abort_flag);
-        if (ok) {
-          const unsigned char* src =
-              reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)grp * N + j) * G::X_STAGE;
-          bulk_load(xs + s * G::X_STAGE, src, G::X_STAGE, &xfull[s]);
-          *last_issued = t;
-          ok = t < 2 || wait_or_abort(&gempty[s], (k - 1) & 1, abort_flag);
-        }
-      }
+      if (lane == 0)
+        ok = t < 4 ? !*abort_flag
+                   : wait_or_abort(&gempty[sg], (unsigned)(((t >> 2) - 1) & 1), abort_flag);
+      __syncwarp();
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
-      float2* g = gt + s * (P * DW);
       if (lane < P) {
-        const int d = lane;
-        const double dx = xi - a.pos[3 * j], dy = yi - a.pos[3 * j + 1], dz = zi - a.pos[3 * j + 2];
-        const double r = sqrt(dx * dx + dy * dy + dz * dz);
-        double ctd = dz / r;
-        ctd = fmin(1.0, fmax(-1.0, ctd));
-        const float ct = (float)ctd;
-        const float st = (float)sqrt(1.0 - ctd * ctd);
-        const double rho = sqrt(dx * dx + dy * dy);
-        const double phi = (rho > 0.0) ? atan2(dy, dx) : 0.0;
-        float sdp, cdp;
-        sincosf((float)(d * phi), &sdp, &cdp);
-        const double xd = a.k * r;
-        double sxd, cxd;
-        sincos(xd, &sxd, &cxd);
-        const float x = (float)xd, sx = (float)sxd, cx = (float)cxd;
-        const float ix = 1.0f / x;
-        float hr0 = sx * ix, hi0 = -cx * ix;
-        float hr1 = (sx - x * cx) * ix * ix, hi1 = -(cx + x * sx) * ix * ix;
-        for (int q = 0; q < d; ++q) {
-          const float f = (float)(2 * q + 3) * ix;
-          const float nr = f * hr1 - hr0, ni = f * hi1 - hi0;
-          hr0 = hr1; hi0 = hi1; hr1 = nr; hi1 = ni;
+        const float dx = (float)(xi - a.pos[3 * j]);
+        const float dy = (float)(yi - a.pos[3 * j + 1]);
+        const float dz = (float)(zi - a.pos[3 * j + 2]);
+        const float rho2 = dx * dx + dy * dy;
+        const float r2 = rho2 + dz * dz;
+        const float rinv = rsqrtf(r2);
+        const float r = r2 * rinv;
+        const float ct = fminf(1.f, fmaxf(-1.f, dz * rinv));
+        float c1 = 1.f, s1 = 0.f, st = 0.f;  // e^{i phi}, sin theta
+        if (rho2 > 0.f) {
+          const float rhoinv = rsqrtf(rho2);
+          c1 = dx * rhoinv;
+          s1 = dy * rhoinv;
+          st = rho2 * rhoinv * rinv;
         }
-        float stp = 1.f;
-        for (int q = 0; q < d; ++q) stp *= st;
-        float Pp = 0.f, Pc = (float)a.leg->start[d] * stp;
-        for (int p = d; p < P; ++p) {
-          const float gr = Pc * hr0, gi = Pc * hi0;
-          g[p * DW + (2 * L + d)] = make_float2(gr * cdp - gi * sdp, gr * sdp + gi * cdp);
-          g[p * DW + (2 * L - d)] = make_float2(gr * cdp + gi * sdp, gi * cdp - gr * sdp);
-          if (p + 1 < P) {
-            const float Pn = (float)a.leg->alpha[p * kLegStride + d] * ct * Pc -
-                             (float)a.leg->beta[p * kLegStride + d] * Pp;
-            Pp = Pc;
-            Pc = Pn;
-            const float f = (float)(2 * p + 3) * ix;
-            const float nr = f * hr1 - hr0, ni = f * hi1 - hi0;
-            hr0 = hr1; hi0 = hi1; hr1 = nr; hi1 = ni;
+        float cdp = 1.f, sdp = 0.f;  // e^{i d phi} by powers of e^{i phi}
+#pragma unroll
+        for (int q = 0; q < P - 1; ++q) {
+          if (q < lane) {
+            const float cn = cdp * c1 - sdp * s1;
+            sdp = cdp * s1 + sdp * c1;
+            cdp = cn;
           }
         }
+        const float x = kf * r;
+        float sx, cx;
+        sincosf(x, &sx, &cx);
+        pair_table<L>(reinterpret_cast<float2*>(gt + sg * G::G_STAGE), lane, ct, st, cdp, sdp, x, sx,
+                      cx, legA, legB, legS);
       }
       __syncwarp();
-      if (lane == 0)
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&gfull[s])) : "memory");
+      if (lane == 0) mbar_arrive(&gfull[sg]);
     }
   }
+  __syncthreads();  // every role has left its loop: no further source copy will be issued
 
   // ===================== epilogue =====================
   if (warp < 4) {
-    // wait (bounded) for the MMAs and source copies in flight before reading or freeing TMEM
-    const bool ok = n_iter == 0 || mbar_wait(accum, 0);
-    if (tid == 0 && *last_issued >= 0) {
-      const int tl = *last_issued;
-      (void)mbar_wait(&xfull[tl & 1], (unsigned)((tl >> 1) & 1));
-      if (tl >= 1) (void)mbar_wait(&xfull[(tl - 1) & 1], (unsigned)(((tl - 1) >> 1) & 1));
-    }
+    // No copy may still be landing when the stages are reused or the block exits. A load into a
+    // stage is issued only after the MMAs consumed the previous one, so only the newest load of
+    // each stage can be in flight (bounded waits).
+    if (tid == 0)
+      for (int b = 0; b < 3; ++b)
+        if (issued[b] >= 0) (void)panel_wait(&xfull[b], (unsigned)((issued[b] / 3) & 1));
+    // wait (bounded) for the MMAs before reading tensor memory
+    const bool ok = n_iter == 0 || panel_wait(accum, 0);
     tc_fence_after();
+    named_sync(1, 128);  // the drain above precedes every write to the exchange buffer
     const bool aborted = *abort_flag != 0;
     if (aborted && tid == 0) atomicExch(a.err, 1);
-    const int row = (lane & 15) + 16 * warp;  // M = 64: row l + 16q sits in lane l + 32q
-    const int col = grp * M + row;
-    const bool live = lane < 16 && col < a.nrhs;
+    float* xch = reinterpret_cast<float*>(xs);  // [64][XCH_STRIDE]: imaginary-row accumulators
     const unsigned lane_base = tmem + ((unsigned)(32 * warp) << 16);
-    for (int n = 0; n < H; n += 8) {
-      float v[4][8];
+    if (warp >= 2) {
+      const int r = 32 * (warp - 2) + lane;
+#pragma unroll 1
+      for (int n = 0; n < 4 * HP; n += 8) {
+        float v[8];
+        tmem_ld32<8>(lane_base + n, v);
 #pragma unroll
-      for (int reg = 0; reg < 4; ++reg) tmem_ld32<8>(lane_base + reg * HP + n, v[reg]);
-      if (!live) continue;
+        for (int u = 0; u < 8; ++u) xch[r * G::XCH_STRIDE + n + u] = v[u];
+      }
+    }
+    named_sync(1, 128);
+    if (warp < 2) {
+      const int c = 32 * warp + lane;  // column within the group
+      const int col = grp * G::M + c;
+      const bool live = col < a.nrhs;
+      const float* im = xch + c * G::XCH_STRIDE;
+#pragma unroll 1
+      for (int n = 0; n < H; n += 8) {
+        float pr[8], pi[8], qr[8], qi[8];
+        tmem_ld32<8>(lane_base + n, pr);                // S_r P_r^T
+        tmem_ld32<8>(lane_base + HP + n, pi);           // S_r P_i^T
+        tmem_ld32<8>(lane_base + 2 * HP + n, qr);       // D_r Q_r^T
+        tmem_ld32<8>(lane_base + 3 * HP + n, qi);       // D_r Q_i^T
+        if (!live) continue;
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int q = n + u;
-        if (q >= H) break;
+        for (int u = 0; u < 8; ++u) {
+          const int q = n + u;
+          if (q >= H) break;
+          const float ur = pr[u] - im[HP + q], ui = pi[u] + im[q];
+          const float vr = qr[u] - im[3 * HP + q], vi = qi[u] + im[2 * HP + q];
+          double y1r = 0.5 * ((double)ur + (double)vr), y1i = 0.5 * ((double)ui + (double)vi);
+          double y2r = 0.5 * ((double)ur - (double)vr), y2i = 0.5 * ((double)ui - (double)vi);
+          if (n_iter == 0) { y1r = y1i = y2r = y2i = 0.0; }
+          if (aborted || !ok) { y1r = y1i = y2r = y2i = __longlong_as_double(0x7ff8000000000000LL); }
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          const int nn = half * H + q;
-          double yr = 0.0, yi = 0.0;
-          if (n_iter > 0) {
-            yr = (double)v[2 * half][u];
-            yi = (double)v[2 * half + 1][u];
+          for (int half = 0; half < 2; ++half) {
+            const int nn = half * H + q;
+            const double yr = half ? y2r : y1r, yi = half ? y2i : y1i;
+            const size_t gi = (size_t)col * a.ldy + (size_t)i * a.nmax + nn;
+            double2 out;
+            if (a.tmat) {
+              const double2 tv = a.tmat[(size_t)i * a.nmax + nn];
+              const double2 xv = a.x[(size_t)col * a.ld + (size_t)i * a.nmax + nn];
+              out = make_double2(xv.x - (tv.x * yr - tv.y * yi), xv.y - (tv.x * yi + tv.y * yr));
+            } else {
+              out = make_double2(yr, yi);
+            }
+            a.y[gi] = out;
           }
-          if (aborted || !ok) { yr = nan(""); yi = nan(""); }
-          const size_t gi = (size_t)col * a.ldy + (size_t)i * a.nmax + nn;
-          double2 out;
-          if (a.tmat) {
-            const double2 tv = a.tmat[(size_t)i * a.nmax + nn];
-            const double2 xv = a.x[(size_t)col * a.ld + (size_t)i * a.nmax + nn];
-            out = make_double2(xv.x - (tv.x * yr - tv.y * yi), xv.y - (tv.x * yi + tv.y * yr));
-          } else {
-            out = make_double2(yr, yi);
-          }
-          a.y[gi] = out;
         }
       }
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 8) {
+  if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(G::TMEM_COLS)
@@ -427,7 +599,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   }
 }
 
-// Source panels: columns [grp*64, grp*64+64) of x rounded to TF32 in the X-operand layout.
+// Source panels: columns [grp*64, grp*64+64) of x as the A operands [S_r; S_i] and [D_r; D_i]
+// (S = X1 + X2, D = X1 - X2 of every column, rounded to TF32).
 template <int L>
 __global__ void xpanel_kernel(int n_particles, int nmax, int nrhs, long long ld, const double2* x,
                               float* xp) {
@@ -435,20 +608,22 @@ __global__ void xpanel_kernel(int n_particles, int nmax, int nrhs, long long ld,
   constexpr int H = G::H, HP = G::HP, M = G::M;
   const int j = blockIdx.x, grp = blockIdx.y;
   unsigned char* dst = reinterpret_cast<unsigned char*>(xp) + ((size_t)grp * n_particles + j) * G::X_STAGE;
-  for (int e = threadIdx.x; e < M * HP * 2; e += blockDim.x) {
-    const int half = e / (M * HP);
-    const int rem = e - half * M * HP;
-    const int r = rem / HP, q = rem - (rem / HP) * HP;
+  for (int e = threadIdx.x; e < M * HP; e += blockDim.x) {
+    const int r = e / HP, q = e - (e / HP) * HP;
     const int col = grp * M + r;
-    float re = 0.f, im = 0.f;
+    float sr = 0.f, si = 0.f, dr = 0.f, di = 0.f;
     if (q < H && col < nrhs) {
-      const double2 v = x[(size_t)col * ld + (size_t)j * nmax + half * H + q];
-      re = to_tf32((float)v.x);
-      im = to_tf32((float)v.y);
+      const double2 v1 = x[(size_t)col * ld + (size_t)j * nmax + q];
+      const double2 v2 = x[(size_t)col * ld + (size_t)j * nmax + H + q];
+      sr = to_tf32((float)(v1.x + v2.x));
+      si = to_tf32((float)(v1.y + v2.y));
+      dr = to_tf32((float)(v1.x - v2.x));
+      di = to_tf32((float)(v1.y - v2.y));
     }
-    const int off = kmajor_offset(r, q, M);
-    *reinterpret_cast<float*>(dst + (2 * half) * G::X_PLANE + off) = re;
-    *reinterpret_cast<float*>(dst + (2 * half + 1) * G::X_PLANE + off) = im;
+    *reinterpret_cast<float*>(dst + kmajor_offset(r, q, 128)) = sr;
+    *reinterpret_cast<float*>(dst + kmajor_offset(64 + r, q, 128)) = si;
+    *reinterpret_cast<float*>(dst + G::A_BYTES + kmajor_offset(r, q, 128)) = dr;
+    *reinterpret_cast<float*>(dst + G::A_BYTES + kmajor_offset(64 + r, q, 128)) = di;
   }
 }
 
