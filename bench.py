@@ -657,7 +657,7 @@ def panel_probe(args) -> None:
 
 
 def matvec_probe(args) -> None:
-    """Four coupling matvecs (the first is warm-up) on the first N spheres of the workload."""
+    """Four coupling matvecs (the first is warm-up, the others timed) on the first N spheres."""
     import torch
 
     from yasf_b200.device import PRECISIONS, CouplingDevice
@@ -669,11 +669,16 @@ def matvec_probe(args) -> None:
                          torch.device("cuda", 0))
     g = torch.Generator(device="cuda").manual_seed(0)
     x = torch.randn(dev.n, dtype=torch.complex128, device=dev.device, generator=g)
-    for _ in range(4):
+    y = dev.coupling(x, PRECISIONS[args.precision])
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
         y = dev.coupling(x, PRECISIONS[args.precision])
-    torch.cuda.synchronize()
+    e1.record()
+    e1.synchronize()
     print(json.dumps({"probe": agg.name, "n": n, "precision": args.precision,
-                      "max_abs": float(y.abs().max())}))
+                      "ms": e0.elapsed_time(e1) / 3, "max_abs": float(y.abs().max())}))
 
 
 def main() -> None:

@@ -121,21 +121,36 @@ int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::v
   }
 }
 
+// Right-hand-side groups of 64 per panel block: two as soon as there are two (each W_ij is then
+// generated once for 128 columns), padded to an even count whose extra columns are zero.
+static int panel_groups_per_block(int groups) { return groups >= 2 ? 2 : 1; }
+static int panel_padded_groups(int groups) {
+  const int ng = panel_groups_per_block(groups);
+  return (groups + ng - 1) / ng * ng;
+}
+
+template <int L, int NG>
+static int launch_panel_ng(const PanelArgs& pa, int padded, cudaStream_t s) {
+  using G = PanelGeom<L>;
+  YASF_CUDA_TRY(cudaFuncSetAttribute(panel_kernel<L, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     G::SMEM));
+  const dim3 grid(pa.n_particles, padded / NG);
+  YASF_COUNTED(panel_kernel<L, NG><<<grid, kPanelThreads, G::SMEM, s>>>(pa));
+  YASF_CUDA_TRY(cudaGetLastError());
+  return YASF_OK;
+}
+
 template <int L>
 static int launch_panel(const PanelArgs& pa, int groups, cudaStream_t s) {
-  using G = PanelGeom<L>;
+  const int padded = panel_padded_groups(groups);
   {
-    const dim3 grid(pa.n_particles, groups);
+    const dim3 grid(pa.n_particles, padded);
     YASF_COUNTED(xpanel_kernel<L><<<grid, 256, 0, s>>>(pa.n_particles, pa.nmax, pa.nrhs, pa.ld, pa.x,
                                                      const_cast<float*>(pa.xp)));
     YASF_CUDA_TRY(cudaGetLastError());
   }
-  YASF_CUDA_TRY(cudaFuncSetAttribute(panel_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     G::SMEM));
-  const dim3 grid(pa.n_particles, groups);
-  YASF_COUNTED(panel_kernel<L><<<grid, kPanelThreads, G::SMEM, s>>>(pa));
-  YASF_CUDA_TRY(cudaGetLastError());
-  return YASF_OK;
+  return panel_groups_per_block(groups) == 2 ? launch_panel_ng<L, 2>(pa, padded, s)
+                                             : launch_panel_ng<L, 1>(pa, padded, s);
 }
 
 static size_t panel_xstage(int L) {
@@ -159,7 +174,7 @@ extern "C" int yasf_panel_workspace_size(const yasf_plan* plan, int n_particles,
   if (!plan || !bytes || n_particles <= 0 || nrhs <= 0) return YASF_ERR_INVALID_ARGUMENT;
   const size_t xs = panel_xstage(plan->lmax);
   if (!xs) return YASF_ERR_UNSUPPORTED;
-  const size_t groups = (size_t)(nrhs + 63) / 64;
+  const size_t groups = (size_t)panel_padded_groups((nrhs + 63) / 64);
   *bytes = ((groups * n_particles * xs + 255) & ~size_t(255)) + 256;
   return YASF_OK;
 }

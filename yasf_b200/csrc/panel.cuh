@@ -64,7 +64,6 @@ struct PanelGeom {
   static constexpr int G_STAGE = (P * P + 4 * L + 1) * 8;
   static constexpr int G_STAGES = 4;
   static constexpr int LEG_BYTES = ((2 * P * P + P) * 4 + 15) & ~15;
-  static constexpr int TMEM_COLS = tmem_cols(4 * HP);
   static constexpr int X_OFF = 0;
   static constexpr int W_OFF = X_OFF + X_STAGES * X_STAGE;
   static constexpr int G_OFF = W_OFF + W_STAGES * W_STAGE;
@@ -309,9 +308,13 @@ __device__ __forceinline__ void pair_table(float2* g, int d, float ct, float st,
 }
 
 // ---- the kernel ---------------------------------------------------------------------------
-template <int L>
+// NG right-hand-side groups of 64 per block (1 or 2): with two, every W_ij is generated once for
+// 128 columns; the source panels of the two groups pass through the stage ring one after the
+// other and the accumulators of group g sit at tensor-memory column g * 4 HP.
+template <int L, int NG>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   using G = PanelGeom<L>;
+  constexpr int TMEM_COLS = tmem_cols(4 * G::HP * NG);
   using Sched = PanelSched<L>;
   static_assert(Sched::kWarps == kGenWarps, "schedule built for another warp count");
   constexpr int H = G::H, HP = G::HP, P = G::P, KS = G::KS;
@@ -338,7 +341,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   const int i = blockIdx.x;    // receiving sphere
-  const int grp = blockIdx.y;  // right-hand-side group of 64
+  const int grp0 = blockIdx.y * NG;  // first right-hand-side group of 64 of this block
   const int N = a.n_particles;
   const int n_iter = N - 1;    // every source but the receiver itself
 
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(tmem_slot)),
-                 "r"(G::TMEM_COLS)
+                 "r"(TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -434,20 +437,31 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       constexpr unsigned long long b_op = (unsigned long long)(G::B_BYTES >> 4);
       constexpr unsigned long long ak = (unsigned long long)((2 * G::A_LBO) >> 4);
       constexpr unsigned long long bk = (unsigned long long)((2 * G::B_LBO) >> 4);
-      for (int t = 0; t < n_iter; ++t) {
-        const int sx = t % 3, sw = t & 1;
-        if (!wait_or_abort(&xfull[sx], (unsigned)((t / 3) & 1), abort_flag)) break;
+      bool stop = false;
+      for (int t = 0; t < n_iter && !stop; ++t) {
+        const int sw = t & 1;
         if (!wait_or_abort(&wfull[sw], (unsigned)((t >> 1) & 1), abort_flag)) break;
-        tc_fence_after();
-        const unsigned long long dx = da0 + (unsigned long long)sx * (unsigned long long)(G::X_STAGE >> 4);
         const unsigned long long dw = db0 + (unsigned long long)sw * (unsigned long long)(G::W_STAGE >> 4);
 #pragma unroll
-        for (int kk = 0; kk < KS; ++kk) {
-          const unsigned acc = (t == 0 && kk == 0) ? 0u : 1u;
-          umma_tf32(tmem, dx + kk * ak, dw + kk * bk, idesc, acc);                       // [S;Si] [P;Pi]
-          umma_tf32(tmem + 2 * HP, dx + a_op + kk * ak, dw + b_op + kk * bk, idesc, acc);  // [D;Di] [Q;Qi]
+        for (int g = 0; g < NG; ++g) {
+          const int u = t * NG + g;  // source-panel unit: pair t, group g
+          const int sx = u % 3;
+          if (!wait_or_abort(&xfull[sx], (unsigned)((u / 3) & 1), abort_flag)) {
+            stop = true;
+            break;
+          }
+          tc_fence_after();
+          const unsigned long long dx = da0 + (unsigned long long)sx * (unsigned long long)(G::X_STAGE >> 4);
+          const unsigned td = tmem + (unsigned)(g * 4 * HP);
+#pragma unroll
+          for (int kk = 0; kk < KS; ++kk) {
+            const unsigned acc = (t == 0 && kk == 0) ? 0u : 1u;
+            umma_tf32(td, dx + kk * ak, dw + kk * bk, idesc, acc);                         // [S;Si] [P;Pi]
+            umma_tf32(td + 2 * HP, dx + a_op + kk * ak, dw + b_op + kk * bk, idesc, acc);  // [D;Di] [Q;Qi]
+          }
+          umma_commit(&xempty[sx]);
         }
-        umma_commit(&xempty[sx]);
+        if (stop) break;
         umma_commit(&wempty[sw]);
       }
       umma_commit(accum);
@@ -456,14 +470,15 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   } else if (warp == kLoadWarp) {
     // ===================== source panels =====================
     if (lane == 0) {
-      for (int t = 0; t < n_iter; ++t) {
-        const int sx = t % 3;
+      for (int u = 0; u < n_iter * NG; ++u) {
+        const int t = u / NG, g = u - (u / NG) * NG;
+        const int sx = u % 3;
         const int j = t < i ? t : t + 1;
         if (*abort_flag) break;
-        if (t >= 3 && !wait_or_abort(&xempty[sx], (unsigned)(((t / 3) - 1) & 1), abort_flag)) break;
+        if (u >= 3 && !wait_or_abort(&xempty[sx], (unsigned)(((u / 3) - 1) & 1), abort_flag)) break;
         const unsigned char* src =
-            reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)grp * N + j) * G::X_STAGE;
-        issued[sx] = t;  // written before the copy: the next load into this stage waits for its MMAs
+            reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)(grp0 + g) * N + j) * G::X_STAGE;
+        issued[sx] = u;  // written before the copy: the next load into this stage waits for its MMAs
         bulk_load(xs + sx * G::X_STAGE, src, G::X_STAGE, &xfull[sx]);
       }
     }
@@ -535,55 +550,59 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     const bool aborted = *abort_flag != 0;
     if (aborted && tid == 0) atomicExch(a.err, 1);
     float* xch = reinterpret_cast<float*>(xs);  // [64][XCH_STRIDE]: imaginary-row accumulators
-    const unsigned lane_base = tmem + ((unsigned)(32 * warp) << 16);
-    if (warp >= 2) {
-      const int r = 32 * (warp - 2) + lane;
 #pragma unroll 1
-      for (int n = 0; n < 4 * HP; n += 8) {
-        float v[8];
-        tmem_ld32<8>(lane_base + n, v);
+    for (int g = 0; g < NG; ++g) {
+      const unsigned lane_base = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(g * 4 * HP);
+      if (g > 0) named_sync(1, 128);  // the previous group's exchange rows are consumed
+      if (warp >= 2) {
+        const int r = 32 * (warp - 2) + lane;
+#pragma unroll 1
+        for (int n = 0; n < 4 * HP; n += 8) {
+          float v[8];
+          tmem_ld32<8>(lane_base + n, v);
 #pragma unroll
-        for (int u = 0; u < 8; ++u) xch[r * G::XCH_STRIDE + n + u] = v[u];
+          for (int u = 0; u < 8; ++u) xch[r * G::XCH_STRIDE + n + u] = v[u];
+        }
       }
-    }
-    named_sync(1, 128);
-    if (warp < 2) {
-      const int c = 32 * warp + lane;  // column within the group
-      const int col = grp * G::M + c;
-      const bool live = col < a.nrhs;
-      const float* im = xch + c * G::XCH_STRIDE;
+      named_sync(1, 128);
+      if (warp < 2) {
+        const int c = 32 * warp + lane;  // column within the group
+        const int col = (grp0 + g) * G::M + c;
+        const bool live = col < a.nrhs;
+        const float* im = xch + c * G::XCH_STRIDE;
 #pragma unroll 1
-      for (int n = 0; n < H; n += 8) {
-        float pr[8], pi[8], qr[8], qi[8];
-        tmem_ld32<8>(lane_base + n, pr);                // S_r P_r^T
-        tmem_ld32<8>(lane_base + HP + n, pi);           // S_r P_i^T
-        tmem_ld32<8>(lane_base + 2 * HP + n, qr);       // D_r Q_r^T
-        tmem_ld32<8>(lane_base + 3 * HP + n, qi);       // D_r Q_i^T
-        if (!live) continue;
+        for (int n = 0; n < H; n += 8) {
+          float pr[8], pi[8], qr[8], qi[8];
+          tmem_ld32<8>(lane_base + n, pr);                // S_r P_r^T
+          tmem_ld32<8>(lane_base + HP + n, pi);           // S_r P_i^T
+          tmem_ld32<8>(lane_base + 2 * HP + n, qr);       // D_r Q_r^T
+          tmem_ld32<8>(lane_base + 3 * HP + n, qi);       // D_r Q_i^T
+          if (!live) continue;
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int q = n + u;
-          if (q >= H) break;
-          const float ur = pr[u] - im[HP + q], ui = pi[u] + im[q];
-          const float vr = qr[u] - im[3 * HP + q], vi = qi[u] + im[2 * HP + q];
-          double y1r = 0.5 * ((double)ur + (double)vr), y1i = 0.5 * ((double)ui + (double)vi);
-          double y2r = 0.5 * ((double)ur - (double)vr), y2i = 0.5 * ((double)ui - (double)vi);
-          if (n_iter == 0) { y1r = y1i = y2r = y2i = 0.0; }
-          if (aborted || !ok) { y1r = y1i = y2r = y2i = __longlong_as_double(0x7ff8000000000000LL); }
+          for (int u = 0; u < 8; ++u) {
+            const int q = n + u;
+            if (q >= H) break;
+            const float ur = pr[u] - im[HP + q], ui = pi[u] + im[q];
+            const float vr = qr[u] - im[3 * HP + q], vi = qi[u] + im[2 * HP + q];
+            double y1r = 0.5 * ((double)ur + (double)vr), y1i = 0.5 * ((double)ui + (double)vi);
+            double y2r = 0.5 * ((double)ur - (double)vr), y2i = 0.5 * ((double)ui - (double)vi);
+            if (n_iter == 0) { y1r = y1i = y2r = y2i = 0.0; }
+            if (aborted || !ok) { y1r = y1i = y2r = y2i = __longlong_as_double(0x7ff8000000000000LL); }
 #pragma unroll
-          for (int half = 0; half < 2; ++half) {
-            const int nn = half * H + q;
-            const double yr = half ? y2r : y1r, yi = half ? y2i : y1i;
-            const size_t gi = (size_t)col * a.ldy + (size_t)i * a.nmax + nn;
-            double2 out;
-            if (a.tmat) {
-              const double2 tv = a.tmat[(size_t)i * a.nmax + nn];
-              const double2 xv = a.x[(size_t)col * a.ld + (size_t)i * a.nmax + nn];
-              out = make_double2(xv.x - (tv.x * yr - tv.y * yi), xv.y - (tv.x * yi + tv.y * yr));
-            } else {
-              out = make_double2(yr, yi);
+            for (int half = 0; half < 2; ++half) {
+              const int nn = half * H + q;
+              const double yr = half ? y2r : y1r, yi = half ? y2i : y1i;
+              const size_t gi = (size_t)col * a.ldy + (size_t)i * a.nmax + nn;
+              double2 out;
+              if (a.tmat) {
+                const double2 tv = a.tmat[(size_t)i * a.nmax + nn];
+                const double2 xv = a.x[(size_t)col * a.ld + (size_t)i * a.nmax + nn];
+                out = make_double2(xv.x - (tv.x * yr - tv.y * yi), xv.y - (tv.x * yi + tv.y * yr));
+              } else {
+                out = make_double2(yr, yi);
+              }
+              a.y[gi] = out;
             }
-            a.y[gi] = out;
           }
         }
       }
@@ -594,7 +613,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(G::TMEM_COLS)
+                 "r"(TMEM_COLS)
                  : "memory");
   }
 }
