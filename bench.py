@@ -631,7 +631,8 @@ def run_serve(args, rank: int, world: int) -> None:
 
 
 def panel_probe(args) -> None:
-    """Four panel matvecs (the first is warm-up) on the first N spheres with --nrhs columns."""
+    """Four panel matvecs (the first is warm-up) on the first N spheres with --nrhs columns
+    (TF32 tensor-core panel, or the float64 dense multi-column kernel with --float64-panel)."""
     import torch
 
     from yasf_b200.device import CouplingDevice
@@ -646,14 +647,15 @@ def panel_probe(args) -> None:
     tmat = torch.randn(dev.n, dtype=torch.complex128, device=dev.device, generator=g) * 0.1
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    y = dev.panel(x, tmat)
+    apply = dev.dpanel if args.float64_panel else dev.panel
+    y = apply(x, tmat)
     e0.record()
     for _ in range(3):
-        y = dev.panel(x, tmat)
+        y = apply(x, tmat)
     e1.record()
     e1.synchronize()
-    print(json.dumps({"probe": "panel", "n": n, "nrhs": args.nrhs, "ms": e0.elapsed_time(e1) / 3,
-                      "max_abs": float(y.abs().max())}))
+    print(json.dumps({"probe": "dpanel" if args.float64_panel else "panel", "n": n, "nrhs": args.nrhs,
+                      "ms": e0.elapsed_time(e1) / 3, "max_abs": float(y.abs().max())}))
 
 
 def matvec_probe(args) -> None:
@@ -699,6 +701,8 @@ def main() -> None:
     ap.add_argument("--panel-probe", type=int, default=0, metavar="N",
                     help="profiling aid: run 4 TF32 panel matvecs on the first N spheres and exit")
     ap.add_argument("--nrhs", type=int, default=128, help="columns of --panel-probe")
+    ap.add_argument("--float64-panel", action="store_true",
+                    help="--panel-probe times the float64 dense multi-column coupling instead")
     ap.add_argument("--restart-batched", type=int, default=50, help="inner GMRES cycle length (c3)")
     ap.add_argument("--slots", type=int, default=4, help="serving slots (serve)")
     ap.add_argument("--serve-rtol", type=float, default=1e-6, help="serving refinement tolerance")

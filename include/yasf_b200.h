@@ -115,6 +115,19 @@ int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const double* posi
                       long long ldx, long long ldy, void* workspace, size_t workspace_bytes,
                       void* stream);
 
+/* ---- float64 dense multi-column coupling -------------------------------------------------------
+ * The multi-channel particle_interaction (yasfpy/functions/cpu_numba.py:99-181) in float64 for
+ * nrhs columns at once: every W_ij is formed once per pair (tau-symmetric P = Wa + Wb, Q = Wa - Wb)
+ * and applied to blocks of 32 columns. Same arguments and outputs as yasf_panel_matvec
+ * (y = x - T (.) W x when tmat is non-NULL, else y = W x), float64 throughout; agrees with
+ * yasf_coupling_matvec to rounding. lmax <= 6 (YASF_ERR_UNSUPPORTED otherwise). Used for the
+ * float64 residuals of yasf_batched_solve. */
+int yasf_dpanel_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, size_t* bytes);
+int yasf_dpanel_matvec(const yasf_plan* plan, int n_particles, const double* positions,
+                       double k_medium, const double* tmat, const double* x, double* y, int nrhs,
+                       long long ldx, long long ldy, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
 /* ---- batched right-hand sides: refined lockstep GMRES -----------------------------------------
  * (I - T W) X = B for nrhs columns (incidence directions x polarisations; the reference solves one
  * incidence per Simulation, yasfpy/scattered_field_coefficients.py:95-144 with
@@ -124,7 +137,8 @@ int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const double* posi
  * operator inner_kind: 0 tensor-core TF32 panel (lmax <= 6), 1 complex64 coupling kernel,
  * 2 complex128 coupling kernel. X0 = 0. Columns leave when ||B_c - A X_c|| <= rtol ||B_c||.
  * stats (host, may be NULL): [0] lockstep inner steps, [1] panel applications, [2] column
- * applications of kinds 1/2, [3] float64 residual matvecs, [4] worst relative residual,
+ * applications of kinds 1/2, [3] float64 residual column applications (float64 applications to
+ * two or more columns use yasf_dpanel_matvec when lmax <= 6), [4] worst relative residual,
  * [5] unconverged columns, [6] refinement steps. column_residuals (host, may be NULL): nrhs
  * final relative residuals. Synchronous. */
 int yasf_batched_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, int restart,

@@ -67,6 +67,8 @@ SIGNATURES = {
     "yasf_coupling_matvec_noalloc": [_vp, _i, _vp, _d, _vp, _vp, _i, _vp],
     "yasf_panel_workspace_size": [_vp, _i, _i, _c.POINTER(_sz)],
     "yasf_panel_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _ll, _vp, _sz, _vp],
+    "yasf_dpanel_workspace_size": [_vp, _i, _i, _c.POINTER(_sz)],
+    "yasf_dpanel_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _ll, _vp, _sz, _vp],
     "yasf_batched_workspace_size": [_vp, _i, _i, _i, _i, _c.POINTER(_sz)],
     "yasf_batched_solve": [_vp, _i, _vp, _d, _vp, _vp, _vp, _vp, _i, _d, _i, _i, _d, _i, _vp, _sz,
                            _dp, _dp, _vp],

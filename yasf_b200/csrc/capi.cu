@@ -334,8 +334,13 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
   // Generation terms for the tensor-core panel path (lmax <= 6).
   std::vector<float> gen_c1;
   std::vector<unsigned> gen_meta, gen_dst;
+  std::vector<int4> dgen_chunks;
+  std::vector<int2> dgen_items;
+  std::vector<int> dgen_idx;
+  std::vector<double> dgen_coef;
   {
-    const int bst = panel_build_terms(L, ab5, gen_c1, gen_meta, gen_dst);
+    int bst = panel_build_terms(L, ab5, gen_c1, gen_meta, gen_dst);
+    if (bst == YASF_OK) bst = dpanel_build_items(L, ab5, dgen_chunks, dgen_items, dgen_idx, dgen_coef);
     if (bst != YASF_OK) {
       delete plan;
       set_error_text("translation table does not follow the a5/b5 selection rules of the panel schedule");
@@ -375,6 +380,10 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     cudaFree(plan->d_gen_c1);
     cudaFree(plan->d_gen_meta);
     cudaFree(plan->d_gen_dst);
+    cudaFree(plan->d_dgen_chunks);
+    cudaFree(plan->d_dgen_items);
+    cudaFree(plan->d_dgen_idx);
+    cudaFree(plan->d_dgen_coef);
     delete plan;
     return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
   };
@@ -399,6 +408,13 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     YASF_UPLOAD(plan->d_gen_meta, gen_meta);
     YASF_UPLOAD(plan->d_gen_dst, gen_dst);
   }
+  if (!dgen_chunks.empty()) {
+    YASF_UPLOAD(plan->d_dgen_chunks, dgen_chunks);
+    YASF_UPLOAD(plan->d_dgen_items, dgen_items);
+    YASF_UPLOAD(plan->d_dgen_idx, dgen_idx);
+    YASF_UPLOAD(plan->d_dgen_coef, dgen_coef);
+    plan->dgen_chunks = (int)dgen_chunks.size();
+  }
 #undef YASF_UPLOAD
   if ((e = cudaMalloc(reinterpret_cast<void**>(&plan->d_leg), sizeof(LegendreTables))) != cudaSuccess)
     return fail(e);
@@ -420,6 +436,10 @@ extern "C" int yasf_plan_destroy(yasf_plan* plan) {
   cudaFree(plan->d_gen_c1);
   cudaFree(plan->d_gen_meta);
   cudaFree(plan->d_gen_dst);
+  cudaFree(plan->d_dgen_chunks);
+  cudaFree(plan->d_dgen_items);
+  cudaFree(plan->d_dgen_idx);
+  cudaFree(plan->d_dgen_coef);
   delete plan;
   return YASF_OK;
 }

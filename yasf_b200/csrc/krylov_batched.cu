@@ -254,7 +254,7 @@ __global__ void bbacksolve_kernel(int R, int m, const int* stop, const double2* 
 }
 
 struct BatchWs {
-  size_t o_cpl = 0, cpl = 0, o_pnl = 0, pnl = 0, o_Q = 0, o_W = 0, o_Z = 0, o_R = 0, o_D = 0,
+  size_t o_cpl = 0, cpl = 0, o_pnl = 0, pnl = 0, o_dpn = 0, dpn = 0, o_Q = 0, o_W = 0, o_Z = 0, o_R = 0, o_D = 0,
          o_H = 0, o_gc = 0, o_gs = 0, o_S = 0, o_y = 0, o_part = 0, o_vec = 0, o_int = 0, total = 0;
 };
 
@@ -267,9 +267,15 @@ static BatchWs batch_layout(const yasf_plan* plan, int N, int R, int m, int inne
     size_t b = 0;
     if (yasf_panel_workspace_size(plan, N, R, &b) == YASF_OK) L.pnl = b;
   }
+  // float64 dense multi-column coupling for the float64 applications (lmax <= 6, 2+ columns)
+  if (R >= 2 && plan->d_dgen_chunks) {
+    size_t b = 0;
+    if (yasf_dpanel_workspace_size(plan, N, R, &b) == YASF_OK) L.dpn = b;
+  }
   size_t o = 0;
   L.o_cpl = o; o += up(L.cpl);
   L.o_pnl = o; o += up(L.pnl);
+  L.o_dpn = o; o += up(L.dpn);
   L.o_Q = o; o += up((size_t)R * (m + 1) * n * sizeof(double2));
   L.o_W = o; o += up((size_t)R * n * sizeof(double2));
   L.o_Z = o; o += up((size_t)R * n * sizeof(double2));
@@ -342,6 +348,7 @@ extern "C" int yasf_batched_solve(const yasf_plan* plan, int n_particles, const 
   double2* X = reinterpret_cast<double2*>(x);
   void* cws = ws + L.o_cpl;
   void* pws = ws + L.o_pnl;
+  void* dws = ws + L.o_dpn;
   const double eps = 2.220446049250313e-16;
   const dim3 pgrid(256, R);
 
@@ -372,6 +379,12 @@ extern "C" int yasf_batched_solve(const yasf_plan* plan, int n_particles, const 
                                R, col_stride, n, pws, L.pnl, s);
     }
     const int prec = inner_kind == 1 ? YASF_C64 : YASF_C128;
+    if (prec == YASF_C128 && L.dpn) {  // all columns in one float64 dense pass
+      mv_col += R;
+      return yasf_dpanel_matvec(plan, n_particles, positions, k_medium, tmat,
+                                reinterpret_cast<const double*>(V), reinterpret_cast<double*>(out), R,
+                                col_stride, n, dws, L.dpn, s);
+    }
     for (int c = 0; c < R; ++c) {
       if (!h_live[c]) continue;
       mv_col++;
@@ -493,13 +506,22 @@ extern "C" int yasf_batched_solve(const yasf_plan* plan, int n_particles, const 
     YASF_COUNTED(bax_kernel<<<pgrid, 256, 0, s>>>(n, 1, D, nullptr, X, d_live));
     YASF_CUDA_TRY(cudaGetLastError());
     // ---- float64 residual of the active columns -------------------------------------------------
-    for (int c = 0; c < R; ++c) {
-      if (!h_active[c]) continue;
-      mv64++;
-      st = coupling_column(plan, n_particles, positions, k_medium, tmat,
-                           reinterpret_cast<const double*>(X + (size_t)c * n),
-                           reinterpret_cast<double*>(W + (size_t)c * n), YASF_C128, 1, cws, L.cpl, s);
+    int n_active = 0;
+    for (int c = 0; c < R; ++c) n_active += h_active[c] != 0;
+    if (L.dpn && n_active >= 2) {  // every column in one float64 dense pass
+      mv64 += R;
+      st = yasf_dpanel_matvec(plan, n_particles, positions, k_medium, tmat, reinterpret_cast<const double*>(X),
+                              reinterpret_cast<double*>(W), R, n, n, dws, L.dpn, s);
       if (st != YASF_OK) return st;
+    } else {
+      for (int c = 0; c < R; ++c) {
+        if (!h_active[c]) continue;
+        mv64++;
+        st = coupling_column(plan, n_particles, positions, k_medium, tmat,
+                             reinterpret_cast<const double*>(X + (size_t)c * n),
+                             reinterpret_cast<double*>(W + (size_t)c * n), YASF_C128, 1, cws, L.cpl, s);
+        if (st != YASF_OK) return st;
+      }
     }
     if ((st = to_dev_i(d_active, h_active.data())) != YASF_OK) return st;
     YASF_COUNTED(bax_kernel<<<pgrid, 256, 0, s>>>(n, 0, B, W, Rr, d_active));

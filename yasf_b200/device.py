@@ -164,6 +164,18 @@ class CouplingDevice:
              _ptr(cols), _ptr(y), R, self.n, self.n, _ptr(ws), nb.value, _stream_ptr())
         return y.reshape(x.shape)
 
+    def dpanel(self, x: torch.Tensor, tmat: torch.Tensor | None = None, out: torch.Tensor | None = None):
+        """Float64 dense multi-column coupling: (R, n) columns -> W x (or x - T W x)."""
+        cols = x.reshape(-1, self.n).contiguous()
+        R = cols.shape[0]
+        y = out if out is not None else torch.empty_like(cols)
+        nb = ctypes.c_size_t()
+        call("yasf_dpanel_workspace_size", self.plan.handle, self.n_particles, R, ctypes.byref(nb))
+        ws = self.ws.get(nb.value)
+        call("yasf_dpanel_matvec", self.plan.handle, self.n_particles, _ptr(self.pos), self.k, _ptr(tmat),
+             _ptr(cols), _ptr(y), R, self.n, self.n, _ptr(ws), nb.value, _stream_ptr())
+        return y.reshape(x.shape)
+
     INNER_KINDS = {"tf32": 0, "c64": 1, "c128": 2}
 
     def batched_solve(self, tmat: torch.Tensor, B: torch.Tensor, rtol: float, restart: int = 50,
