@@ -14,6 +14,8 @@ Reported:
   latency_ms       p50 / p99 of the timed solves
   mixed            complex64 inner solves in float64 refinement: solves/s and C_ext error
                    against the plain float64 solve
+  batched_r128     the mixed-precision batched form on the same aggregate: 128 incidences in one
+                   refined solve (TF32 tensor-core inner operator), solves/s and speed-up over value
   roofline         the coupling contraction (contract_kernel) against the float64 pipe
   cpu_baseline     the oracle (plain-C restatement of the reference CPU matvec) on host cores,
                    row-sampled, converted to solves/s with this solve's matvec count
@@ -359,6 +361,36 @@ def run_b200(args, rank: int, world: int) -> None:
                  "c_ext_rel_err_vs_fp64": abs(float(om.c_ext[0]) - c_ext64) / abs(c_ext64),
                  "stats": mst}
 
+    # ---- mixed-precision batched solve of the same aggregate (R incidences) ------------------
+    batched = None
+    if args.batched_rhs and agg.lmax <= 6 and not args.no_mixed:
+        from yasf_b200.incident import plane_wave_block
+        from yasf_b200.workloads import incidences
+
+        polar, azim, pol = incidences(args.batched_rhs // 2, rotation_seed=0)
+        a_blk = plane_wave_block(agg.lmax, agg.positions, agg.k, polar, azim, pol)
+        A_cols = np.ascontiguousarray(np.moveaxis(a_blk, 2, 0).reshape(len(pol), -1))
+        tm_host = tmat.cpu().numpy()
+        B_cols = torch.from_numpy(np.ascontiguousarray(A_cols * tm_host[None, :])).to(device)
+        kw = dict(rtol=rtol, restart=50, max_refine=8, inner_rtol=1e-3, inner="tf32")
+        dev.batched_solve(tmat, B_cols, **kw)  # warm-up (workspace, plan set-up)
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        Xb, bst = dev.batched_solve(tmat, B_cols, **kw)
+        e1.record()
+        e1.synchronize()
+        b_s = e0.elapsed_time(e1) / 1e3
+        colres = bst.pop("column_residuals")
+        batched = {"solves_per_s": len(pol) / b_s, "speedup_vs_plain_fp64": len(pol) / b_s / value,
+                   "nrhs": len(pol), "seconds": b_s, "max_fp64_relative_residual": max(colres),
+                   "stats": bst,
+                   "config": "same aggregate, 64 seeded Fibonacci directions x TE/TM, TF32 tensor-core "
+                             "panel inner GMRES (inner rtol 1e-3, restart 50) in float64 refinement to "
+                             f"rtol {rtol}, float64 residuals by the dense multi-column kernel"}
+        del B_cols, Xb
+
     # ---- CPU baseline (oracle port, row sample) -----------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -399,6 +431,7 @@ def run_b200(args, rank: int, world: int) -> None:
         "c_ext": c_ext64,
         "c_sca": c_sca64,
         "mixed": mixed,
+        "batched_r128": batched,
         "roofline": {"bound": "fp64", "kernel": "contract_kernel (pair side + contraction)",
                      "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
                      "frac": achieved / FP64_NOMINAL_TFLOPS, "traffic": traffic,
@@ -693,6 +726,8 @@ def main() -> None:
     ap.add_argument("--restart", type=int, default=100)
     ap.add_argument("--no-precond", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--batched-rhs", type=int, default=128,
+                    help="right-hand sides of the batched solve reported beside the plain line (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--matvec-probe", type=int, default=0, metavar="N",
