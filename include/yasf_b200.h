@@ -138,7 +138,7 @@ int yasf_dpanel_matvec(const yasf_plan* plan, int n_particles, const double* pos
  * 2 complex128 coupling kernel. X0 = 0. Columns leave when ||B_c - A X_c|| <= rtol ||B_c||.
  * stats (host, may be NULL): [0] lockstep inner steps, [1] panel applications, [2] column
  * applications of kinds 1/2, [3] float64 residual column applications (float64 applications to
- * two or more columns use yasf_dpanel_matvec when lmax <= 6), [4] worst relative residual,
+ * 12 or more columns use yasf_dpanel_matvec when lmax <= 6), [4] worst relative residual,
  * [5] unconverged columns, [6] refinement steps. column_residuals (host, may be NULL): nrhs
  * final relative residuals. Synchronous. */
 int yasf_batched_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, int restart,

@@ -1,6 +1,6 @@
 """GPU parity of the float64 dense multi-column coupling (yasf_dpanel_matvec) against the
 single-column float64 coupling kernel: equal to rounding (relative 1e-12), every lmax it supports,
-column counts that are and are not multiples of the 32-column block, the master form
+column counts that are and are not multiples of the 32- and 64-column tiles, the master form
 x - T (.) W x, and a single sphere (W = 0)."""
 
 from __future__ import annotations
@@ -27,7 +27,8 @@ def _setup(lmax, n, seed, device):
     return dev, rng
 
 
-@pytest.mark.parametrize("lmax,n,R", [(1, 6, 3), (2, 9, 1), (3, 17, 33), (4, 30, 64), (5, 12, 7), (6, 25, 40)])
+@pytest.mark.parametrize("lmax,n,R", [(1, 6, 3), (2, 9, 1), (3, 17, 33), (4, 30, 64), (5, 12, 7), (6, 25, 40),
+                                      (6, 21, 130), (3, 10, 64), (2, 7, 65)])
 def test_dpanel_matches_float64_coupling(cuda_device, lmax, n, R):
     dev, rng = _setup(lmax, n, 300 + lmax, cuda_device)
     X = torch.from_numpy(rng.normal(size=(R, dev.n)) + 1j * rng.normal(size=(R, dev.n))).to(cuda_device)

@@ -11,11 +11,12 @@
 // (l1 -m1, l2 -m2) have equal Wa and negated Wb coefficients on A[p][|m2 - m1|] and conjugate
 // phases e^{+-i (m2 - m1) phi}, so both come from one set of loads.
 //
-// Block = (receiving sphere i, tile of 32 columns), 288 threads. Warps 0-7 generate P and Q of
-// W_ij into shared memory, then apply them: warps 0-3 form U = P S and warps 4-7 V = Q D, each
-// warp RPW receiving rows times 32 columns (one column per lane, W entries broadcast). Warp 8 runs
-// one pair ahead: it copies the source tile [S; D] (cp.async.bulk, two stages) and computes the
-// float64 pair table (A[p][d] = Pn_p^d(cos theta) h_p(k r), e^{i delta phi}; two stages). All waits
+// Block = (receiving sphere i, tile of 32 or 64 columns). Worker warps generate P and Q of W_ij
+// into shared memory, then apply them: per 32 columns, 4 warps form U = P S and 4 warps V = Q D,
+// each warp RPW receiving rows times 32 columns (one column per lane, W entries broadcast). A
+// helper warp runs ahead: it computes the float64 pair table (A[p][d] = Pn_p^d(cos theta)
+// h_p(k r), e^{i delta phi}; two stages) and copies the source tile [S; D] (cp.async.bulk; two
+// stages at 32 columns, one at 64). All waits
 // are bounded in time; on a timeout every role stops, the error word is set and the result is NaN.
 #include <algorithm>
 #include <cmath>
@@ -25,28 +26,30 @@
 
 namespace yasf {
 
-constexpr int kDpCols = 32;        // columns per block
-constexpr int kDpWorkers = 256;    // warps 0-7
-constexpr int kDpThreads = 288;    // + helper warp 8
-
-template <int L>
+// Column tile of a block: 32 columns with 8 worker warps and two source-tile stages, or 64 columns
+// with 16 worker warps and one stage (each W_ij then serves 64 columns; the copy of the next tile
+// overlaps the generation of the next W).
+template <int L, int CT>
 struct DpGeom {
   static constexpr int H = L * (L + 2);
   static constexpr int P = 2 * L + 1;
   static constexpr int RPW = (H + 3) / 4;            // receiving rows per worker warp
   static constexpr int HR = 4 * RPW;                 // padded row count
+  static constexpr int WORKERS = 8 * (CT / 32);      // worker warps: (column half, block, row group)
+  static constexpr int THREADS = 32 * (WORKERS + 1); // + helper warp
+  static constexpr int XS = CT == 32 ? 2 : 1;        // source-tile stages
   static constexpr int W_BYTES = 2 * H * HR * 16;    // P, Q as [blk][q2][q1] complex float64
-  static constexpr int X_STAGE = 2 * H * kDpCols * 16;  // [S; D] as [blk][q2][c]
+  static constexpr int X_STAGE = 2 * H * CT * 16;    // [S; D] as [blk][q2][c]
   static constexpr int T_ENTRIES = P * P + 4 * L + 1;
   static constexpr int T_STAGE = T_ENTRIES * 16;
   static constexpr int W_OFF = 0;
   static constexpr int X_OFF = W_BYTES;
-  static constexpr int T_OFF = X_OFF + 2 * X_STAGE;
+  static constexpr int T_OFF = X_OFF + XS * X_STAGE;
   static constexpr int BAR_OFF = T_OFF + 2 * T_STAGE;
   static constexpr int SMEM = BAR_OFF + 128;
   static_assert(SMEM <= 232448, "dpanel shared memory exceeds the per-block limit");
   static_assert(W_BYTES % 16 == 0 && X_STAGE % 16 == 0 && T_STAGE % 16 == 0, "alignment");
-  static_assert(2 * HR * kDpCols * 16 <= 2 * X_STAGE, "exchange buffer does not fit");
+  static_assert(HR * CT * 16 <= XS * X_STAGE, "exchange buffer does not fit");
 };
 
 struct DpArgs {
@@ -123,21 +126,23 @@ __device__ __forceinline__ void dp_pair_table(double2* T, const LegendreTables* 
   }
 }
 
-template <int L>
-__global__ void __launch_bounds__(kDpThreads, 1) dpanel_kernel(DpArgs a) {
-  using G = DpGeom<L>;
-  constexpr int H = G::H, P = G::P, RPW = G::RPW, HR = G::HR;
+template <int L, int CT>
+__global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArgs a) {
+  using G = DpGeom<L, CT>;
+  constexpr int H = G::H, P = G::P, RPW = G::RPW, HR = G::HR, NW = G::WORKERS, XS = G::XS;
+  constexpr int NWT = 32 * NW;  // worker threads
   extern __shared__ __align__(128) unsigned char dp_smem[];
   double2* W = reinterpret_cast<double2*>(dp_smem + G::W_OFF);    // [2][H][HR]
-  unsigned char* xs = dp_smem + G::X_OFF;                         // [2][X_STAGE]
+  unsigned char* xs = dp_smem + G::X_OFF;                         // [XS][X_STAGE]
   unsigned char* ts = dp_smem + G::T_OFF;                         // [2][T_STAGE]
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(dp_smem + G::BAR_OFF);
-  unsigned long long* xfull = bars;      // [2]
-  unsigned long long* tfull = bars + 2;  // [2]
-  unsigned long long* sfree = bars + 4;  // [2] stage consumed by the workers
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 6);
-  volatile int* issued = reinterpret_cast<volatile int*>(bars + 7);  // [2]
-  volatile int* go = reinterpret_cast<volatile int*>(bars + 8);      // [2] workers' uniform decisions
+  unsigned long long* xfull = bars;      // [XS] source tile landed
+  unsigned long long* xfree = bars + 2;  // [XS] source tile consumed (apply done)
+  unsigned long long* tfull = bars + 4;  // [2] pair table ready
+  unsigned long long* tfree = bars + 6;  // [2] pair table consumed (generation done)
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 8);
+  volatile int* issued = reinterpret_cast<volatile int*>(bars + 9);  // [2] newest pair per stage
+  volatile int* go = reinterpret_cast<volatile int*>(bars + 10);     // [2] workers' uniform decisions
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int i = blockIdx.x, tile = blockIdx.y;
@@ -148,8 +153,9 @@ __global__ void __launch_bounds__(kDpThreads, 1) dpanel_kernel(DpArgs a) {
   if (tid == 0) {
     for (int b = 0; b < 2; ++b) {
       mbar_init(&xfull[b], 1);
+      mbar_init(&xfree[b], 1);
       mbar_init(&tfull[b], 1);
-      mbar_init(&sfree[b], 1);
+      mbar_init(&tfree[b], 1);
     }
     *abort_flag = 0;
     issued[0] = issued[1] = -1;
@@ -157,26 +163,30 @@ __global__ void __launch_bounds__(kDpThreads, 1) dpanel_kernel(DpArgs a) {
   }
   __syncthreads();
 
-  if (warp < 8) {
+  if (warp < NW) {
     // ===================== generation + dense application =====================
-    const int blk = warp >> 2;                 // 0: U = P S, 1: V = Q D
+    const int ch = warp >> 3;                  // column half (64-column tiles)
+    const int blk = (warp >> 2) & 1;           // 0: U = P S, 1: V = Q D
     const int r0 = (warp & 3) * RPW;
-    // complex accumulators as two independent partial sums each (re: w.x x.x | -w.y x.y,
-    // im: w.x x.y | w.y x.x), so consecutive FMAs of a row do not wait on each other
-    double2 acc[RPW], acc2[RPW];
+    const int c = ch * 32 + lane;              // column within the tile
+    // 32-column tiles: complex accumulators as two independent partial sums each (re: w.x x.x |
+    // -w.y x.y, im: w.x x.y | w.y x.x), so consecutive FMAs of a row do not wait on each other
+    double2 acc[RPW], acc2[CT == 32 ? RPW : 1];
 #pragma unroll
-    for (int r = 0; r < RPW; ++r) acc[r] = acc2[r] = make_double2(0.0, 0.0);
+    for (int r = 0; r < RPW; ++r) acc[r] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < (CT == 32 ? RPW : 1); ++r) acc2[r] = make_double2(0.0, 0.0);
     // One thread waits (bounded) and publishes the outcome across a workers' barrier, so every
     // worker warp takes the same branch and no warp is left waiting at a barrier.
     for (int t = 0; t < n_iter; ++t) {
-      const int s = t & 1;
-      if (tid == 0) go[0] = wait_or_abort(&tfull[s], (unsigned)((t >> 1) & 1), abort_flag) ? 1 : 0;
-      named_sync(1, kDpWorkers);
+      const int st = t & 1, sx = t % XS;
+      if (tid == 0) go[0] = wait_or_abort(&tfull[st], (unsigned)((t >> 1) & 1), abort_flag) ? 1 : 0;
+      named_sync(1, NWT);
       if (!go[0]) break;
-      const double2* T = reinterpret_cast<const double2*>(ts + s * G::T_STAGE);
-      for (int c = warp; c < a.n_chunks; c += 8) {
-        const int4 cm = __ldg(a.chunks + c);
-        const int2 m = __ldg(a.items + 32 * c + lane);
+      const double2* T = reinterpret_cast<const double2*>(ts + st * G::T_STAGE);
+      for (int cc = warp; cc < a.n_chunks; cc += NW) {
+        const int4 cm = __ldg(a.chunks + cc);
+        const int2 m = __ldg(a.items + 32 * cc + lane);
         const int* ti = a.term_idx + (size_t)cm.z * 32 + lane;
         const double* tc = a.term_coef + (size_t)cm.z * 32 + lane;
         double2 sa = make_double2(0.0, 0.0), sb = make_double2(0.0, 0.0);
@@ -211,49 +221,73 @@ __global__ void __launch_bounds__(kDpThreads, 1) dpanel_kernel(DpArgs a) {
         W[mq2 * HR + mq1] = make_double2(ma.x + mb.y, ma.y - mb.x);
         W[(H + mq2) * HR + mq1] = make_double2(ma.x - mb.y, ma.y + mb.x);
       }
-      if (tid == 0) go[1] = wait_or_abort(&xfull[s], (unsigned)((t >> 1) & 1), abort_flag) ? 1 : 0;
-      named_sync(1, kDpWorkers);  // W complete, source tile decision published
+      if (tid == 0) go[1] = wait_or_abort(&xfull[sx], (unsigned)((t / XS) & 1), abort_flag) ? 1 : 0;
+      named_sync(1, NWT);  // W complete, source tile decision published
+      if (tid == 0) mbar_arrive(&tfree[st]);
       if (!go[1]) break;
-      const double2* X = reinterpret_cast<const double2*>(xs + s * G::X_STAGE) + blk * H * kDpCols;
+      const double2* X = reinterpret_cast<const double2*>(xs + sx * G::X_STAGE) + blk * H * CT + c;
       const double2* Wb = W + blk * H * HR + r0;
+      if constexpr (CT == 32) {
 #pragma unroll 2
-      for (int q2 = 0; q2 < H; ++q2) {
-        const double2 xv = X[q2 * kDpCols + lane];
+        for (int q2 = 0; q2 < H; ++q2) {
+          const double2 xv = X[q2 * CT];
 #pragma unroll
-        for (int r = 0; r < RPW; ++r) {
-          const double2 w = Wb[q2 * HR + r];
-          acc[r].x = fma(w.x, xv.x, acc[r].x);
-          acc2[r].x = fma(-w.y, xv.y, acc2[r].x);
-          acc[r].y = fma(w.x, xv.y, acc[r].y);
-          acc2[r].y = fma(w.y, xv.x, acc2[r].y);
+          for (int r = 0; r < RPW; ++r) {
+            const double2 w = Wb[q2 * HR + r];
+            acc[r].x = fma(w.x, xv.x, acc[r].x);
+            acc2[r].x = fma(-w.y, xv.y, acc2[r].x);
+            acc[r].y = fma(w.x, xv.y, acc[r].y);
+            acc2[r].y = fma(w.y, xv.x, acc2[r].y);
+          }
+        }
+      } else {
+        // fewer registers per thread at 544 threads: one accumulator per row, the two FMAs of
+        // each component issued in separate passes over the rows (RPW instructions apart)
+#pragma unroll 1
+        for (int q2 = 0; q2 < H; ++q2) {
+          const double2 xv = X[q2 * CT];
+#pragma unroll
+          for (int r = 0; r < RPW; ++r) {
+            const double wx = Wb[q2 * HR + r].x;
+            acc[r].x = fma(wx, xv.x, acc[r].x);
+            acc[r].y = fma(wx, xv.y, acc[r].y);
+          }
+#pragma unroll
+          for (int r = 0; r < RPW; ++r) {
+            const double wy = Wb[q2 * HR + r].y;
+            acc[r].x = fma(-wy, xv.y, acc[r].x);
+            acc[r].y = fma(wy, xv.x, acc[r].y);
+          }
         }
       }
-      named_sync(1, kDpWorkers);  // W and the stage are consumed
-      if (tid == 0) mbar_arrive(&sfree[s]);
+      named_sync(1, NWT);  // W and the source tile are consumed
+      if (tid == 0) mbar_arrive(&xfree[sx]);
     }
+    if constexpr (CT == 32) {
 #pragma unroll
-    for (int r = 0; r < RPW; ++r) acc[r] = make_double2(acc[r].x + acc2[r].x, acc[r].y + acc2[r].y);
+      for (int r = 0; r < RPW; ++r) acc[r] = make_double2(acc[r].x + acc2[r].x, acc[r].y + acc2[r].y);
+    }
     // park V in shared memory after every role has finished (below), then combine
     __syncthreads();
     if (tid == 0)
-      for (int b = 0; b < 2; ++b)
-        if (issued[b] >= 0) (void)panel_wait(&xfull[b], (unsigned)((issued[b] >> 1) & 1));
-    named_sync(1, kDpWorkers);
-    double2* xch = reinterpret_cast<double2*>(xs);  // [HR][32] V
+      for (int b = 0; b < XS; ++b)
+        if (issued[b] >= 0) (void)panel_wait(&xfull[b], (unsigned)((issued[b] / XS) & 1));
+    named_sync(1, NWT);
+    double2* xch = reinterpret_cast<double2*>(xs);  // [HR][CT] V
     if (blk == 1) {
 #pragma unroll
-      for (int r = 0; r < RPW; ++r) xch[(r0 + r) * kDpCols + lane] = acc[r];
+      for (int r = 0; r < RPW; ++r) xch[(r0 + r) * CT + c] = acc[r];
     }
-    named_sync(1, kDpWorkers);
+    named_sync(1, NWT);
     const bool aborted = *abort_flag != 0;
     if (aborted && tid == 0) atomicExch(a.err, 1);
-    const int col = tile * kDpCols + lane;
+    const int col = tile * CT + c;
     if (blk == 0 && col < a.nrhs) {
 #pragma unroll
       for (int r = 0; r < RPW; ++r) {
         const int q = r0 + r;
         if (q >= H) break;
-        const double2 v = xch[q * kDpCols + lane];
+        const double2 v = xch[q * CT + c];
         double y1r = 0.5 * (acc[r].x + v.x), y1i = 0.5 * (acc[r].y + v.y);
         double y2r = 0.5 * (acc[r].x - v.x), y2i = 0.5 * (acc[r].y - v.y);
         if (aborted) y1r = y1i = y2r = y2i = __longlong_as_double(0x7ff8000000000000LL);
@@ -274,62 +308,73 @@ __global__ void __launch_bounds__(kDpThreads, 1) dpanel_kernel(DpArgs a) {
       }
     }
   } else {
-    // ===================== helper: source tiles and pair tables, one pair ahead =====================
+    // ===================== helper: pair tables (two stages) and source tiles (XS stages) =====
+    // Pair t's table is written once generation of pair t - 2 has released its stage; pair t's
+    // tile is copied once the apply of pair t - XS has released its stage. With one tile stage the
+    // table of pair t + 1 is computed while the workers generate and apply pair t.
     const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
     for (int t = 0; t < n_iter; ++t) {
-      const int s = t & 1;
+      const int st = t & 1, sx = t % XS;
       const int j = t < i ? t : t + 1;
       int ok = 1;
+      if (lane == 0)
+        ok = t < 2 ? !*abort_flag : wait_or_abort(&tfree[st], (unsigned)(((t >> 1) - 1) & 1), abort_flag);
+      __syncwarp();
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      if (lane < P)
+        dp_pair_table<L>(reinterpret_cast<double2*>(ts + st * G::T_STAGE), a.leg, lane, xi - a.pos[3 * j],
+                         yi - a.pos[3 * j + 1], zi - a.pos[3 * j + 2], a.k);
+      __syncwarp();
       if (lane == 0) {
-        ok = t < 2 ? !*abort_flag
-                   : wait_or_abort(&sfree[s], (unsigned)(((t >> 1) - 1) & 1), abort_flag);
+        mbar_arrive(&tfull[st]);
+        ok = t < XS ? !*abort_flag
+                    : wait_or_abort(&xfree[sx], (unsigned)(((t / XS) - 1) & 1), abort_flag);
         if (ok) {
-          issued[s] = t;
-          bulk_load(xs + s * G::X_STAGE,
+          issued[sx] = t;
+          bulk_load(xs + sx * G::X_STAGE,
                     reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)tile * N + j) * G::X_STAGE,
-                    G::X_STAGE, &xfull[s]);
+                    G::X_STAGE, &xfull[sx]);
         }
       }
       __syncwarp();
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
-      if (lane < P)
-        dp_pair_table<L>(reinterpret_cast<double2*>(ts + s * G::T_STAGE), a.leg, lane, xi - a.pos[3 * j],
-                         yi - a.pos[3 * j + 1], zi - a.pos[3 * j + 2], a.k);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tfull[s]);
     }
     __syncthreads();  // pairs with the workers' barrier before the drain
   }
 }
 
-// Source tiles: for columns [tile*32, tile*32 + 32), [S; D] = [X1 + X2; X1 - X2] as [blk][q2][c]
+// Source tiles: for columns [tile*CT, tile*CT + CT), [S; D] = [X1 + X2; X1 - X2] as [blk][q2][c]
 // (zero beyond nrhs); blockIdx.z selects S or D. Read column-contiguous, written row-contiguous
-// through shared memory.
-template <int L>
+// through shared memory, 32 columns at a time.
+template <int L, int CT>
 __global__ void __launch_bounds__(256) dpanel_tiles_kernel(int n_particles, int nmax, int nrhs, long long ld,
                                                            const double2* x, double2* xp) {
-  using G = DpGeom<L>;
+  using G = DpGeom<L, CT>;
   constexpr int H = G::H;
-  __shared__ double2 buf[H][kDpCols + 1];
+  __shared__ double2 buf[H][33];
   const int j = blockIdx.x, tile = blockIdx.y, blk = blockIdx.z;
   const double sg = blk ? -1.0 : 1.0;
-  for (int e = threadIdx.x; e < kDpCols * H; e += blockDim.x) {
-    const int c = e / H, q = e - (e / H) * H;
-    const int col = tile * kDpCols + c;
-    double2 v = make_double2(0.0, 0.0);
-    if (col < nrhs) {
-      const double2 v1 = x[(size_t)col * ld + (size_t)j * nmax + q];
-      const double2 v2 = x[(size_t)col * ld + (size_t)j * nmax + H + q];
-      v = make_double2(v1.x + sg * v2.x, v1.y + sg * v2.y);
+  double2* dst = xp + ((size_t)tile * n_particles + j) * (G::X_STAGE / 16) + (size_t)blk * H * CT;
+  for (int c0 = 0; c0 < CT; c0 += 32) {
+    for (int e = threadIdx.x; e < 32 * H; e += blockDim.x) {
+      const int c = e / H, q = e - (e / H) * H;
+      const int col = tile * CT + c0 + c;
+      double2 v = make_double2(0.0, 0.0);
+      if (col < nrhs) {
+        const double2 v1 = x[(size_t)col * ld + (size_t)j * nmax + q];
+        const double2 v2 = x[(size_t)col * ld + (size_t)j * nmax + H + q];
+        v = make_double2(v1.x + sg * v2.x, v1.y + sg * v2.y);
+      }
+      buf[q][c] = v;
     }
-    buf[q][c] = v;
-  }
-  __syncthreads();
-  double2* dst = xp + ((size_t)tile * n_particles + j) * (G::X_STAGE / 16) + (size_t)blk * H * kDpCols;
-  for (int e = threadIdx.x; e < H * kDpCols; e += blockDim.x) {
-    const int row = e / kDpCols, c = e - (e / kDpCols) * kDpCols;
-    dst[e] = buf[row][c];
+    __syncthreads();
+    for (int e = threadIdx.x; e < H * 32; e += blockDim.x) {
+      const int row = e / 32, c = e - (e / 32) * 32;
+      dst[row * CT + c0 + c] = buf[row][c];
+    }
+    __syncthreads();
   }
 }
 
@@ -423,26 +468,37 @@ int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std:
   return YASF_OK;
 }
 
-template <int L>
-static int launch_dpanel(const DpArgs& da, int tiles, cudaStream_t s) {
-  using G = DpGeom<L>;
-  YASF_COUNTED(dpanel_tiles_kernel<L><<<dim3(da.n_particles, tiles, 2), 256, 0, s>>>(
+// Column tile width for nrhs columns: 64 once there are 64 or more.
+static int dpanel_cols(int nrhs) { return nrhs >= 64 ? 64 : 32; }
+
+template <int L, int CT>
+static int launch_dpanel_ct(const DpArgs& da, cudaStream_t s) {
+  using G = DpGeom<L, CT>;
+  const int tiles = (da.nrhs + CT - 1) / CT;
+  YASF_COUNTED(dpanel_tiles_kernel<L, CT><<<dim3(da.n_particles, tiles, 2), 256, 0, s>>>(
       da.n_particles, da.nmax, da.nrhs, da.ld, da.x, const_cast<double2*>(da.xp)));
   YASF_CUDA_TRY(cudaGetLastError());
-  YASF_CUDA_TRY(cudaFuncSetAttribute(dpanel_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
-  YASF_COUNTED(dpanel_kernel<L><<<dim3(da.n_particles, tiles), kDpThreads, G::SMEM, s>>>(da));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(dpanel_kernel<L, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     G::SMEM));
+  YASF_COUNTED(dpanel_kernel<L, CT><<<dim3(da.n_particles, tiles), G::THREADS, G::SMEM, s>>>(da));
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
 }
 
+template <int L>
+static int launch_dpanel(const DpArgs& da, cudaStream_t s) {
+  return dpanel_cols(da.nrhs) == 64 ? launch_dpanel_ct<L, 64>(da, s) : launch_dpanel_ct<L, 32>(da, s);
+}
+
+// Bytes of one source's [S; D] for 32 columns.
 static size_t dpanel_tile_bytes(int L) {
   switch (L) {
-    case 1: return DpGeom<1>::X_STAGE;
-    case 2: return DpGeom<2>::X_STAGE;
-    case 3: return DpGeom<3>::X_STAGE;
-    case 4: return DpGeom<4>::X_STAGE;
-    case 5: return DpGeom<5>::X_STAGE;
-    case 6: return DpGeom<6>::X_STAGE;
+    case 1: return DpGeom<1, 32>::X_STAGE;
+    case 2: return DpGeom<2, 32>::X_STAGE;
+    case 3: return DpGeom<3, 32>::X_STAGE;
+    case 4: return DpGeom<4, 32>::X_STAGE;
+    case 5: return DpGeom<5, 32>::X_STAGE;
+    case 6: return DpGeom<6, 32>::X_STAGE;
     default: return 0;
   }
 }
@@ -455,8 +511,9 @@ extern "C" int yasf_dpanel_workspace_size(const yasf_plan* plan, int n_particles
   if (!plan || !bytes || n_particles <= 0 || nrhs <= 0) return YASF_ERR_INVALID_ARGUMENT;
   const size_t tb = dpanel_tile_bytes(plan->lmax);
   if (!tb) return YASF_ERR_UNSUPPORTED;
-  const size_t tiles = (size_t)(nrhs + kDpCols - 1) / kDpCols;
-  *bytes = ((tiles * n_particles * tb + 255) & ~size_t(255)) + 256;
+  const int ct = dpanel_cols(nrhs);
+  const size_t tiles = (size_t)(nrhs + ct - 1) / ct;
+  *bytes = ((tiles * (ct / 32) * n_particles * tb + 255) & ~size_t(255)) + 256;
   return YASF_OK;
 }
 
@@ -499,14 +556,13 @@ extern "C" int yasf_dpanel_matvec(const yasf_plan* plan, int n_particles, const 
   da.tmat = reinterpret_cast<const double2*>(tmat);
   da.y = reinterpret_cast<double2*>(y);
   da.err = err;
-  const int tiles = (nrhs + kDpCols - 1) / kDpCols;
   switch (plan->lmax) {
-    case 1: return launch_dpanel<1>(da, tiles, s);
-    case 2: return launch_dpanel<2>(da, tiles, s);
-    case 3: return launch_dpanel<3>(da, tiles, s);
-    case 4: return launch_dpanel<4>(da, tiles, s);
-    case 5: return launch_dpanel<5>(da, tiles, s);
-    case 6: return launch_dpanel<6>(da, tiles, s);
+    case 1: return launch_dpanel<1>(da, s);
+    case 2: return launch_dpanel<2>(da, s);
+    case 3: return launch_dpanel<3>(da, s);
+    case 4: return launch_dpanel<4>(da, s);
+    case 5: return launch_dpanel<5>(da, s);
+    case 6: return launch_dpanel<6>(da, s);
     default: return YASF_ERR_UNSUPPORTED;
   }
 }

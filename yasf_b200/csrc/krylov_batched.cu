@@ -253,6 +253,8 @@ __global__ void bbacksolve_kernel(int R, int m, const int* stop, const double2* 
   }
 }
 
+constexpr int kDenseMin = 12;  // columns from which the float64 dense kernel replaces column matvecs
+
 struct BatchWs {
   size_t o_cpl = 0, cpl = 0, o_pnl = 0, pnl = 0, o_dpn = 0, dpn = 0, o_Q = 0, o_W = 0, o_Z = 0, o_R = 0, o_D = 0,
          o_H = 0, o_gc = 0, o_gs = 0, o_S = 0, o_y = 0, o_part = 0, o_vec = 0, o_int = 0, total = 0;
@@ -267,8 +269,9 @@ static BatchWs batch_layout(const yasf_plan* plan, int N, int R, int m, int inne
     size_t b = 0;
     if (yasf_panel_workspace_size(plan, N, R, &b) == YASF_OK) L.pnl = b;
   }
-  // float64 dense multi-column coupling for the float64 applications (lmax <= 6, 2+ columns)
-  if (R >= 2 && plan->d_dgen_chunks) {
+  // float64 dense multi-column coupling for the float64 applications (lmax <= 6): one pass costs
+  // about as much as 10 single-column matvecs at 32 columns, so it is used from kDenseMin columns
+  if (R >= kDenseMin && plan->d_dgen_chunks) {
     size_t b = 0;
     if (yasf_dpanel_workspace_size(plan, N, R, &b) == YASF_OK) L.dpn = b;
   }
@@ -379,7 +382,7 @@ extern "C" int yasf_batched_solve(const yasf_plan* plan, int n_particles, const 
                                R, col_stride, n, pws, L.pnl, s);
     }
     const int prec = inner_kind == 1 ? YASF_C64 : YASF_C128;
-    if (prec == YASF_C128 && L.dpn) {  // all columns in one float64 dense pass
+    if (prec == YASF_C128 && L.dpn) {  // all columns in one float64 dense pass (R >= kDenseMin)
       mv_col += R;
       return yasf_dpanel_matvec(plan, n_particles, positions, k_medium, tmat,
                                 reinterpret_cast<const double*>(V), reinterpret_cast<double*>(out), R,
@@ -508,7 +511,7 @@ extern "C" int yasf_batched_solve(const yasf_plan* plan, int n_particles, const 
     // ---- float64 residual of the active columns -------------------------------------------------
     int n_active = 0;
     for (int c = 0; c < R; ++c) n_active += h_active[c] != 0;
-    if (L.dpn && n_active >= 2) {  // every column in one float64 dense pass
+    if (L.dpn && n_active >= kDenseMin) {  // every column in one float64 dense pass
       mv64 += R;
       st = yasf_dpanel_matvec(plan, n_particles, positions, k_medium, tmat, reinterpret_cast<const double*>(X),
                               reinterpret_cast<double*>(W), R, n, n, dws, L.dpn, s);
