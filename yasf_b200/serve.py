@@ -9,7 +9,8 @@ incidences (directions x polarisations = R right-hand sides). The loop:
 - runs every admitted request on its own CUDA stream, so the kernels of in-flight solves
   interleave on the device while their GMRES state stays resident there;
 - solves in mixed precision: the batched refined solve (yasf_batched_solve) with the tensor-core
-  TF32 panel as the inner operator (complex64 coupling kernel beyond lmax 6), float64 residuals,
+  TF32 panel as the inner operator (complex64 coupling kernel for one or two columns and beyond
+  lmax 6), float64 residuals,
   stopping at rtol (1e-6 by default, which keeps the extinction cross section well inside 1e-6 of
   the float64 solution);
 - reports per-request latency (completion - arrival, queueing included), p50/p99 and solves/s.
@@ -68,8 +69,13 @@ class RequestResult:
         return self.finished - self.arrival
 
 
-def inner_kind(lmax: int) -> str:
-    return "tf32" if lmax <= 6 else "c64"
+def inner_kind(lmax: int, nrhs: int) -> str:
+    """Inner operator of a request's refined solve.
+
+    The TF32 tensor-core panel costs the same for 1 to 64 columns (about twice one complex64 column
+    application), so requests with one or two columns, and every lmax above the panel's 6, use the
+    complex64 coupling kernel column by column."""
+    return "tf32" if lmax <= 6 and nrhs >= 3 else "c64"
 
 
 def footprint_bytes(req: Request, cfg: ServeConfig, dev_plan_handle=None) -> int:
@@ -100,7 +106,7 @@ def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> Reque
     tmat = torch.from_numpy(tm).to(device)
     Bt = torch.from_numpy(B).to(device)
     X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
-                              inner_rtol=cfg.inner_rtol, inner=inner_kind(agg.lmax))
+                              inner_rtol=cfg.inner_rtol, inner=inner_kind(agg.lmax, R))
     Xh = X.cpu().numpy()
     res.c_ext = -np.real(np.einsum("rn,rn->r", A.conj(), Xh)) / agg.k**2 * np.pi
     st.pop("column_residuals", None)
