@@ -313,8 +313,13 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
           ha_r = hb_r; ha_i = hb_i; hb_r = nr; hb_i = ni;
         }
       }
-#pragma unroll 1
-      for (int p = d; p <= PMAX; ++p) {
+      // The orders p of the contraction for this source. With float64 the p loop is unrolled (d is
+      // a warp-uniform runtime value): the valid row counts of every (m1, p) become compile-time
+      // and the row loops carry no predicates. With float32 the rolled loop from p = d is faster.
+      constexpr int kPUnroll = sizeof(Real) == 8 ? PMAX + 1 : 1;
+#pragma unroll kPUnroll
+      for (int p = (sizeof(Real) == 8 ? 0 : d); p <= PMAX; ++p) {
+        if (p < d) continue;
         Real g0r, g0i;
         if constexpr (!REGULAR) {
           g0r = P_cur * ha_r;
