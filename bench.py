@@ -603,7 +603,10 @@ def run_serve(args, rank: int, world: int) -> None:
     for i in range(max(args.warmup, len(lmaxes))):
         lm = (lmaxes[i % len(lmaxes)],) if lmaxes else (3,)
         warm += serving_requests(1, seed=7 + i, n_range=(50, 300), lmax_choices=lm, param_seed=100_000 + i)
-    cfg = ServeConfig(max_slots=args.slots, rtol=args.serve_rtol)
+    from yasf_b200.autotune import Autotuner
+
+    tuner = Autotuner() if args.autotune else None
+    cfg = ServeConfig(max_slots=args.slots, rtol=args.serve_rtol, tuner=tuner)
     server = Server(cfg, device=device)
     server.run(warm, realtime=False)
     torch.cuda.synchronize()
@@ -653,6 +656,9 @@ def run_serve(args, rank: int, world: int) -> None:
         "rhs_solves": tot["rhs_solves"], "makespan_s": tot["makespan_s"], "rank0_summary": summ,
         "c_ext_error_vs_fp64": {"max": max((e["c_ext_rel_err"] for e in errs), default=None),
                                 "samples": errs},
+        "autotune": None if tuner is None else {
+            "decisions": len(tuner.decisions()),
+            "inner_chosen": {k: sum(1 for d in tuner.decisions() if d.inner == k) for k in ("tf32", "c64")}},
         "e2e": {"value": tot["solves_per_s"], "unit": UNIT,
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "note": "each request enters as host arrays (geometry, incidences) and returns C_ext "
@@ -740,6 +746,9 @@ def main() -> None:
                     help="--panel-probe times the float64 dense multi-column coupling instead")
     ap.add_argument("--restart-batched", type=int, default=50, help="inner GMRES cycle length (c3)")
     ap.add_argument("--slots", type=int, default=4, help="serving slots (serve)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="serve: choose each request's inner operator with the (lmax, N, R) autotuner "
+                         "(timed inside the run) instead of the fixed rule")
     ap.add_argument("--serve-rtol", type=float, default=1e-6, help="serving refinement tolerance")
     ap.add_argument("--error-samples", type=int, default=3, help="float64 check solves (c3, serve)")
     args = ap.parse_args()

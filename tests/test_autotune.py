@@ -1,0 +1,55 @@
+"""The (lmax, N, R) autotuner's host logic: keys and buckets, the cheapest-candidate rule, caching
+(no second measurement for a key, thread-safe), and JSON persistence. The measurement itself is
+replaced by a stand-in; tests/test_gpu_autotune.py times real operators."""
+
+from __future__ import annotations
+
+import threading
+
+from yasf_b200.autotune import Autotuner, choose, n_bucket
+
+
+class FakeDev:
+    def __init__(self, lmax, n):
+        self.lmax, self.n_particles = lmax, n
+
+
+def test_choose_and_buckets():
+    assert choose({"c64": 30.0, "tf32": 12.0}) == "tf32"
+    assert choose({"c64": 3.0, "tf32": 12.0}) == "c64"
+    assert n_bucket(2000) == n_bucket(2050)
+    assert n_bucket(2000) != n_bucket(2600)
+
+
+def test_cache_and_persistence(tmp_path):
+    calls = []
+
+    def measure(dev, tmat, nrhs):
+        calls.append((dev.lmax, dev.n_particles, nrhs))
+        return {"c64": 5.0 * nrhs, "tf32": 40.0} if dev.lmax <= 6 else {"c64": 5.0 * nrhs}
+
+    path = tmp_path / "tune.json"
+    t = Autotuner(path=path, measure=measure)
+    assert t.decide(FakeDev(6, 2000), None, 1).inner == "c64"
+    assert t.decide(FakeDev(6, 2000), None, 64).inner == "tf32"
+    assert t.decide(FakeDev(6, 2030), None, 64).inner == "tf32"   # same bucket: cached
+    assert t.decide(FakeDev(8, 2000), None, 64).inner == "c64"    # no panel above lmax 6
+    assert len(calls) == 3
+    t2 = Autotuner(path=path, measure=measure)
+    assert t2.decide(FakeDev(6, 2000), None, 64).inner == "tf32"
+    assert len(calls) == 3                                          # loaded, not re-measured
+    assert {tuple(d.key) for d in t2.decisions()} == {tuple(d.key) for d in t.decisions()}
+
+
+def test_concurrent_decisions_agree():
+    def measure(dev, tmat, nrhs):
+        return {"c64": 1.0, "tf32": 2.0}
+
+    t = Autotuner(measure=measure)
+    out = []
+    th = [threading.Thread(target=lambda: out.append(t.decide(FakeDev(5, 900), None, 16).inner)) for _ in range(8)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    assert out == ["c64"] * 8 and len(t.decisions()) == 1

@@ -10,7 +10,8 @@ incidences (directions x polarisations = R right-hand sides). The loop:
   interleave on the device while their GMRES state stays resident there;
 - solves in mixed precision: the batched refined solve (yasf_batched_solve) with the tensor-core
   TF32 panel as the inner operator (complex64 coupling kernel for one or two columns and beyond
-  lmax 6), float64 residuals,
+  lmax 6; with ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for
+  the request's (lmax, N, R)), float64 residuals,
   stopping at rtol (1e-6 by default, which keeps the extinction cross section well inside 1e-6 of
   the float64 solution);
 - reports per-request latency (completion - arrival, queueing included), p50/p99 and solves/s.
@@ -48,6 +49,7 @@ class ServeConfig:
     max_refine: int = 8
     inner_rtol: float = 1e-3
     keep_solutions: bool = False
+    tuner: object | None = None           # an autotune.Autotuner: inner operator by measurement
 
 
 @dataclass
@@ -105,11 +107,13 @@ def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> Reque
     dev = CouplingDevice(agg.lmax, table, agg.positions, agg.k, device)
     tmat = torch.from_numpy(tm).to(device)
     Bt = torch.from_numpy(B).to(device)
+    inner = cfg.tuner.decide(dev, tmat, R).inner if cfg.tuner is not None else inner_kind(agg.lmax, R)
     X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
-                              inner_rtol=cfg.inner_rtol, inner=inner_kind(agg.lmax, R))
+                              inner_rtol=cfg.inner_rtol, inner=inner)
     Xh = X.cpu().numpy()
     res.c_ext = -np.real(np.einsum("rn,rn->r", A.conj(), Xh)) / agg.k**2 * np.pi
     st.pop("column_residuals", None)
+    st["inner"] = inner
     res.stats = st
     if cfg.keep_solutions:
         res.x = Xh
