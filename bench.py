@@ -14,8 +14,9 @@ Reported:
   latency_ms       p50 / p99 of the timed solves
   mixed            complex64 inner solves in float64 refinement: solves/s and C_ext error
                    against the plain float64 solve
-  batched_r128     the mixed-precision batched form on the same aggregate: 128 incidences in one
-                   refined solve (TF32 tensor-core inner operator), solves/s and speed-up over value
+  batched          the mixed-precision batched form on the same aggregate: --batched-rhs incidences
+                   (128 by default) in one refined solve (TF32 tensor-core inner operator), solves/s
+                   and speed-up over value
   roofline         the coupling contraction (contract_kernel) against the float64 pipe
   cpu_baseline     the oracle (plain-C restatement of the reference CPU matvec) on host cores,
                    row-sampled, converted to solves/s with this solve's matvec count
@@ -386,9 +387,10 @@ def run_b200(args, rank: int, world: int) -> None:
         batched = {"solves_per_s": len(pol) / b_s, "speedup_vs_plain_fp64": len(pol) / b_s / value,
                    "nrhs": len(pol), "seconds": b_s, "max_fp64_relative_residual": max(colres),
                    "stats": bst,
-                   "config": "same aggregate, 64 seeded Fibonacci directions x TE/TM, TF32 tensor-core "
-                             "panel inner GMRES (inner rtol 1e-3, restart 50) in float64 refinement to "
-                             f"rtol {rtol}, float64 residuals by the dense multi-column kernel"}
+                   "config": f"same aggregate, {len(pol) // 2} seeded Fibonacci directions x TE/TM, TF32 "
+                             "tensor-core panel inner GMRES (inner rtol 1e-3, restart 50) in float64 "
+                             f"refinement to rtol {rtol}, float64 residuals by the dense multi-column "
+                             "kernel from 12 columns"}
         del B_cols, Xb
 
     # ---- CPU baseline (oracle port, row sample) -----------------------------------------------
@@ -431,7 +433,7 @@ def run_b200(args, rank: int, world: int) -> None:
         "c_ext": c_ext64,
         "c_sca": c_sca64,
         "mixed": mixed,
-        "batched_r128": batched,
+        "batched": batched,
         "roofline": {"bound": "fp64", "kernel": "contract_kernel (pair side + contraction)",
                      "achieved": achieved, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
                      "frac": achieved / FP64_NOMINAL_TFLOPS, "traffic": traffic,
