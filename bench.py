@@ -373,7 +373,7 @@ def run_b200(args, rank: int, world: int) -> None:
         A_cols = np.ascontiguousarray(np.moveaxis(a_blk, 2, 0).reshape(len(pol), -1))
         tm_host = tmat.cpu().numpy()
         B_cols = torch.from_numpy(np.ascontiguousarray(A_cols * tm_host[None, :])).to(device)
-        kw = dict(rtol=rtol, restart=50, max_refine=8, inner_rtol=1e-3, inner="tf32")
+        kw = dict(rtol=rtol, restart=50, max_refine=8, inner_rtol=args.inner_rtol, inner="tf32")
         dev.batched_solve(tmat, B_cols, **kw)  # warm-up (workspace, plan set-up)
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -388,7 +388,7 @@ def run_b200(args, rank: int, world: int) -> None:
                    "nrhs": len(pol), "seconds": b_s, "max_fp64_relative_residual": max(colres),
                    "stats": bst,
                    "config": f"same aggregate, {len(pol) // 2} seeded Fibonacci directions x TE/TM, TF32 "
-                             "tensor-core panel inner GMRES (inner rtol 1e-3, restart 50) in float64 "
+                             f"tensor-core panel inner GMRES (inner rtol {args.inner_rtol:g}, restart 50) in float64 "
                              f"refinement to rtol {rtol}, float64 residuals by the dense multi-column "
                              "kernel from 12 columns"}
         del B_cols, Xb
@@ -494,7 +494,7 @@ def run_batched(args, rank: int, world: int) -> None:
     tmat = torch.from_numpy(tm).to(device)
     B = B_host.to(device)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
-    kw = dict(rtol=rtol, restart=args.restart_batched, max_refine=8, inner_rtol=1e-3, inner="tf32")
+    kw = dict(rtol=rtol, restart=args.restart_batched, max_refine=8, inner_rtol=args.inner_rtol, inner="tf32")
 
     for _ in range(args.warmup):
         dev.batched_solve(tmat, B, **kw)
@@ -562,7 +562,7 @@ def run_batched(args, rank: int, world: int) -> None:
         "data": "synthetic (seeded RSA aggregate, seeded Fibonacci incidences, no dataset)",
         "config": {"workload": agg.name + "-R128", "n_spheres": agg.n, "lmax": agg.lmax,
                    "unknowns": dev.n, "nrhs": R, "rtol": rtol, "restart": args.restart_batched,
-                   "inner": "TF32 tensor-core panel, inner_rtol 1e-3", "preconditioner": None,
+                   "inner": f"TF32 tensor-core panel, inner_rtol {args.inner_rtol:g}", "preconditioner": None,
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "flushed (256 MB write) before every timed solve"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -747,6 +747,8 @@ def main() -> None:
     ap.add_argument("--float64-panel", action="store_true",
                     help="--panel-probe times the float64 dense multi-column coupling instead")
     ap.add_argument("--restart-batched", type=int, default=50, help="inner GMRES cycle length (c3)")
+    ap.add_argument("--inner-rtol", type=float, default=2e-3,
+                    help="batched solves: inner GMRES tolerance per float64 refinement step")
     ap.add_argument("--slots", type=int, default=4, help="serving slots (serve)")
     ap.add_argument("--autotune", action="store_true",
                     help="serve: choose each request's inner operator with the (lmax, N, R) autotuner "
