@@ -105,10 +105,11 @@ int yasf_master_matvec(const yasf_plan* plan, int n_particles, const double* pos
  * The batched form of the coupling matvec for R right-hand sides (incidence directions x
  * polarisations), replacing the multi-channel particle_interaction loop
  * (yasfpy/functions/cpu_numba.py:99-181) for the inner solves of the refined, batched GMRES:
- * every pair block W_ij is generated once in complex64 and applied to the nmax x R panel of the
- * source on tcgen05 tensor cores (TF32 inputs, FP32 accumulation). y = x - T (.) (W x) when tmat
- * is non-NULL, else y = W x; x and y columns have leading dimensions ldx and ldy. lmax <= 6
- * (YASF_ERR_UNSUPPORTED otherwise). */
+ * every pair block W_ij is generated once in FP32 (as the tau-symmetric P = Wa + Wb, Q = Wa - Wb)
+ * and applied to the source's columns, 64 or 128 per block, on tcgen05 tensor cores (TF32 inputs,
+ * FP32 accumulation; relative accuracy ~1e-3). y = x - T (.) (W x) when tmat is non-NULL, else
+ * y = W x; x and y columns have leading dimensions ldx and ldy. lmax <= 6 (YASF_ERR_UNSUPPORTED
+ * otherwise). */
 int yasf_panel_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, size_t* bytes);
 int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const double* positions,
                       double k_medium, const double* tmat, const double* x, double* y, int nrhs,

@@ -44,7 +44,7 @@ template <int L>
 struct PanelGeom {
   static constexpr int H = half_modes(L);        // modes per tau half
   static constexpr int HP = pad8(H);             // padded to the MMA granularity
-  static constexpr int M = 64;                   // right-hand sides per block
+  static constexpr int M = 64;                   // right-hand sides per group (1 or 2 per block)
   static constexpr int P = 2 * L + 1;            // orders p
   static constexpr int KS = HP / 8;              // K steps of 8 TF32 columns
   // A operands [S_r; S_i], [D_r; D_i]: 128 rows x HP columns
