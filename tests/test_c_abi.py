@@ -58,6 +58,13 @@ def test_argument_validation_without_device(lib):
                                 None, None) == 1
     assert lib.yasf_precond_apply(None, None, None, 1, 0, 0, None) == 1
     assert lib.yasf_dotc(0, None, None, None, None, 0, None) == 1
+    n = ctypes.c_size_t()
+    for fn in ("yasf_panel_workspace_size", "yasf_dpanel_workspace_size"):
+        assert getattr(lib, fn)(None, 10, 4, ctypes.byref(n)) == 1      # no plan
+    for fn in ("yasf_panel_matvec", "yasf_dpanel_matvec"):
+        assert getattr(lib, fn)(None, 10, None, 1.0, None, None, None, 4, 0, 0, None, 0, None) == 1
+    assert lib.yasf_batched_workspace_size(None, 10, 4, 30, 0, ctypes.byref(n)) == 1
+    assert lib.yasf_batched_workspace_size(None, 10, 4, 30, 3, ctypes.byref(n)) == 1
 
 
 def test_no_cpu_fallback_in_product():
