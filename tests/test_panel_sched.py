@@ -18,7 +18,7 @@ from yasf_b200.panel_sched import WARPS, _lm, mirror, schedule
 from yasf_b200.wigner import translation_table_ab5
 
 
-@pytest.mark.parametrize("L", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("L", [1, 2, 3, 4, 5, 6, 7])
 def test_schedule_structure(L):
     steps, table = schedule(L)
     H = L * (L + 2)
@@ -80,7 +80,7 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj):
     return np.concatenate([(U + V) / 2, (U - V) / 2])
 
 
-@pytest.mark.parametrize("L", [2, 4, 6])
+@pytest.mark.parametrize("L", [2, 4, 6, 7])
 def test_generation_algebra_matches_oracle(L):
     rng = np.random.default_rng(L)
     tab = translation_table_ab5(L)

@@ -1,11 +1,31 @@
 // C-ABI entry points of the multi-right-hand-side tensor-core coupling (see panel.cuh).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "capi_internal.h"
 #include "panel.cuh"
 
 namespace yasf {
+
+// IEEE half-precision bits of a float (round to nearest even; normal range, tiny values flush to 0).
+static unsigned short half_bits(float f) {
+  unsigned u;
+  std::memcpy(&u, &f, sizeof(u));
+  const unsigned sign = (u >> 16) & 0x8000u;
+  int exp = (int)((u >> 23) & 0xFFu) - 127 + 15;
+  unsigned m = (u & 0x7FFFFFu) >> 13;
+  const unsigned rem = u & 0x1FFFu;
+  if (exp <= 0) return (unsigned short)sign;
+  if (exp >= 31) return (unsigned short)(sign | 0x7BFFu);
+  if (rem > 0x1000u || (rem == 0x1000u && (m & 1u))) {
+    if (++m == 0x400u) {
+      m = 0;
+      if (++exp >= 31) return (unsigned short)(sign | 0x7BFFu);
+    }
+  }
+  return (unsigned short)(sign | ((unsigned)exp << 10) | m);
+}
 
 // Generation data of the panel kernel from the build-time schedule (panel_sched.h). For every
 // generator thread and slot: the real coefficient and the byte offset of A[p][|d|] of one term of
@@ -94,8 +114,11 @@ static int build_terms_for(const double* ab5, const unsigned short* entry, const
           coefficient(which, q1, q2, p, cr, ci);
           const int slot = which == 0 ? base + na++ : base + wa[k] + nb++;
           if (na > wa[k] || nb > wb[k]) return YASF_ERR_INVALID_ARGUMENT;
-          coef[(size_t)slot * kGenThreads + th] = (float)(which == 0 ? cr : ci);
-          goff[(size_t)slot * kGenThreads + th] = (unsigned)((p * P + std::abs(m2 - m1)) * 8);
+          const float cf = (float)(which == 0 ? cr : ci);
+          const unsigned idx = (unsigned)(p * P + std::abs(m2 - m1));
+          coef[(size_t)slot * kGenThreads + th] = cf;
+          goff[(size_t)slot * kGenThreads + th] =
+              PanelGeom<L>::PACKED ? ((unsigned)half_bits(cf) << 16) | idx : idx * 8;
         }
       }
       base += wa[k] + wb[k];
@@ -117,7 +140,8 @@ int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::v
     case 4: return build_terms_for<4>(ab5, kPanelEntry4, kPanelStepWa4, kPanelStepWb4, coef, goff, dst);
     case 5: return build_terms_for<5>(ab5, kPanelEntry5, kPanelStepWa5, kPanelStepWb5, coef, goff, dst);
     case 6: return build_terms_for<6>(ab5, kPanelEntry6, kPanelStepWa6, kPanelStepWb6, coef, goff, dst);
-    default: return YASF_OK;  // no tensor-core panel beyond lmax 6
+    case 7: return build_terms_for<7>(ab5, kPanelEntry7, kPanelStepWa7, kPanelStepWb7, coef, goff, dst);
+    default: return YASF_OK;  // no tensor-core panel beyond lmax 7
   }
 }
 
@@ -161,6 +185,7 @@ static size_t panel_xstage(int L) {
     case 4: return PanelGeom<4>::X_STAGE;
     case 5: return PanelGeom<5>::X_STAGE;
     case 6: return PanelGeom<6>::X_STAGE;
+    case 7: return PanelGeom<7>::X_STAGE;
     default: return 0;
   }
 }
@@ -224,6 +249,7 @@ extern "C" int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const d
     case 4: return launch_panel<4>(pa, groups, s);
     case 5: return launch_panel<5>(pa, groups, s);
     case 6: return launch_panel<6>(pa, groups, s);
+    case 7: return launch_panel<7>(pa, groups, s);
     default: return YASF_ERR_UNSUPPORTED;
   }
 }

@@ -26,6 +26,7 @@
 // the error word, every role stops, the result is written as NaN and tensor memory is freed.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "coupling.cuh"
@@ -52,13 +53,17 @@ struct PanelGeom {
   static constexpr int A_LBO = (A_ROWS / 8) * 128;   // bytes between 4-column K chunks
   static constexpr int A_BYTES = A_ROWS * HP * 4;
   static constexpr int X_STAGE = 2 * A_BYTES;        // one source panel (S and D operands)
-  static constexpr int X_STAGES = 3;
+  static constexpr int X_STAGES = L <= 6 ? 3 : 2;    // lmax 7: shared memory allows two
   // B operands [P_r; P_i], [Q_r; Q_i]: 2 HP rows x HP columns
   static constexpr int B_ROWS = 2 * HP;
   static constexpr int B_LBO = (B_ROWS / 8) * 128;
   static constexpr int B_BYTES = B_ROWS * HP * 4;
   static constexpr int W_STAGE = 2 * B_BYTES;
-  static constexpr int W_STAGES = 2;
+  static constexpr int W_STAGES = L <= 6 ? 2 : 1;    // lmax 7: generation waits for the MMAs
+  // lmax 7: a thread's 40 generation slots are packed (FP16 coefficient << 16 | table index) to fit
+  // the register budget; up to lmax 6 coefficient and byte offset are separate registers
+  static constexpr bool PACKED = L >= 7;
+  static_assert(!PACKED || W_STAGE <= 65536, "packed store offsets need W stages of at most 64 KB");
   static constexpr int IM_OFF = (HP / 8) * 128;      // row HP + q of a B operand vs row q
   // pair table: A[p][d] at p*P + d, e^{i delta phi} at P*P + 2L + delta (float2)
   static constexpr int G_STAGE = (P * P + 4 * L + 1) * 8;
@@ -239,21 +244,39 @@ __device__ __forceinline__ unsigned after_wait(unsigned v) {
 //   entry:  Wa = E Sa,       Wb = i E Sb
 //   mirror: Wa' = conj(E) Sa, Wb' = -i conj(E) Sb
 // and P = Wa + Wb, Q = Wa - Wb of both to their four operand rows each.
-template <int BASE, int TA, int TB, int S, int IM_OFF, int B_BYTES>
-__device__ __forceinline__ void gen_step(const float (&gc)[S], const unsigned (&go)[S], unsigned gbase,
+template <bool PACKED, int SC, int S>
+__device__ __forceinline__ void slot(const float (&gc)[SC], const unsigned (&go)[S], int q, float& c,
+                                     unsigned& off) {
+  if constexpr (PACKED) {
+    c = __half2float(__ushort_as_half((unsigned short)(go[q] >> 16)));
+    off = (go[q] & 0xFFFFu) << 3;
+  } else {
+    c = gc[q];
+    off = go[q];
+  }
+}
+
+template <int BASE, int TA, int TB, bool PACKED, int SC, int S, int IM_OFF, int B_BYTES>
+__device__ __forceinline__ void gen_step(const float (&gc)[SC], const unsigned (&go)[S], unsigned gbase,
                                          unsigned eoff, unsigned dst, unsigned dstm) {
   float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
 #pragma unroll
   for (int q = 0; q < TA; ++q) {
-    const float2 g = lds_f2(gbase + go[BASE + q]);
-    ar = fmaf(gc[BASE + q], g.x, ar);
-    ai = fmaf(gc[BASE + q], g.y, ai);
+    float c;
+    unsigned off;
+    slot<PACKED>(gc, go, BASE + q, c, off);
+    const float2 g = lds_f2(gbase + off);
+    ar = fmaf(c, g.x, ar);
+    ai = fmaf(c, g.y, ai);
   }
 #pragma unroll
   for (int q = 0; q < TB; ++q) {
-    const float2 g = lds_f2(gbase + go[BASE + TA + q]);
-    br = fmaf(gc[BASE + TA + q], g.x, br);
-    bi = fmaf(gc[BASE + TA + q], g.y, bi);
+    float c;
+    unsigned off;
+    slot<PACKED>(gc, go, BASE + TA + q, c, off);
+    const float2 g = lds_f2(gbase + off);
+    br = fmaf(c, g.x, br);
+    bi = fmaf(c, g.y, bi);
   }
   const float2 e = lds_f2(gbase + eoff);
   {
@@ -319,24 +342,27 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   static_assert(Sched::kWarps == kGenWarps, "schedule built for another warp count");
   constexpr int H = G::H, HP = G::HP, P = G::P, KS = G::KS;
   constexpr int S = Sched::kSlots, NS = Sched::kSteps;
+  constexpr int XS = G::X_STAGES, WS = G::W_STAGES;
+  constexpr bool PK = G::PACKED;
+  constexpr int SC = PK ? 1 : S;
   extern __shared__ __align__(1024) unsigned char panel_smem[];
-  unsigned char* xs = panel_smem + G::X_OFF;                                  // [3][X_STAGE]
-  unsigned char* ws = panel_smem + G::W_OFF;                                  // [2][W_STAGE]
+  unsigned char* xs = panel_smem + G::X_OFF;                                  // [XS][X_STAGE]
+  unsigned char* ws = panel_smem + G::W_OFF;                                  // [WS][W_STAGE]
   unsigned char* gt = panel_smem + G::G_OFF;                                  // [4][G_STAGE]
   float* legA = reinterpret_cast<float*>(panel_smem + G::LEG_OFF);            // [P][P]
   float* legB = legA + P * P;
   float* legS = legB + P * P;
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(panel_smem + G::BAR_OFF);
-  unsigned long long* xfull = bars;        // [3] source panel landed
-  unsigned long long* xempty = bars + 3;   // [3] MMAs of the panel done
-  unsigned long long* wfull = bars + 6;    // [2] W generated (one arrival per generator warp)
-  unsigned long long* wempty = bars + 8;   // [2] MMAs of the W stage done
+  unsigned long long* xfull = bars;        // [XS] source panel landed
+  unsigned long long* xempty = bars + 3;   // [XS] MMAs of the panel done
+  unsigned long long* wfull = bars + 6;    // [WS] W generated (one arrival per generator warp)
+  unsigned long long* wempty = bars + 8;   // [WS] MMAs of the W stage done
   unsigned long long* gfull = bars + 10;   // [4] pair table ready
   unsigned long long* gempty = bars + 14;  // [4] pair table consumed (one arrival per generator warp)
   unsigned long long* accum = bars + 18;   // accumulators final
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 19);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 20);
-  volatile int* issued = reinterpret_cast<volatile int*>(bars + 21);  // [3] newest pair loaded per stage
+  volatile int* issued = reinterpret_cast<volatile int*>(bars + 21);  // [XS] newest unit loaded per stage
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -346,19 +372,27 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   const int n_iter = N - 1;    // every source but the receiver itself
 
   // generation data of this thread (registers)
-  float gc[S];
+  float gc[SC];
   unsigned go[S];
-  unsigned gd[NS], gm[NS], ge[NS];
+  // store offsets of the entry and mirror rows: absolute shared addresses, or (packed variant)
+  // both W-stage offsets (< 64 KB) in one register, entry in the low half
+  unsigned gd[NS], gm[PK ? 1 : NS], ge[NS];
   if (tid < kGenThreads) {
 #pragma unroll
     for (int q = 0; q < S; ++q) {
-      gc[q] = __ldg(a.gen_coef + q * kGenThreads + tid);
+      if constexpr (!PK) gc[q] = __ldg(a.gen_coef + q * kGenThreads + tid);
       go[q] = __ldg(a.gen_goff + q * kGenThreads + tid);
     }
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-      gd[k] = smem_addr(ws) + __ldg(a.gen_dst + k * kGenThreads + tid);
-      gm[k] = smem_addr(ws) + __ldg(a.gen_dst + (NS + k) * kGenThreads + tid);
+      const unsigned od = __ldg(a.gen_dst + k * kGenThreads + tid);
+      const unsigned om = __ldg(a.gen_dst + (NS + k) * kGenThreads + tid);
+      if constexpr (PK) {
+        gd[k] = od | (om << 16);
+      } else {
+        gd[k] = smem_addr(ws) + od;
+        gm[k] = smem_addr(ws) + om;
+      }
       ge[k] = __ldg(a.gen_dst + (2 * NS + k) * kGenThreads + tid);
     }
   }
@@ -380,7 +414,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     for (int b = 0; b < 4; ++b) mbar_init(&gempty[b], kGenWarps);
     mbar_init(accum, 1);
     *abort_flag = 0;
-    for (int b = 0; b < 3; ++b) issued[b] = -1;
+    for (int b = 0; b < 3; ++b) issued[b] = -1;  // stages beyond XS stay unused
     mbar_fence_init();
   }
   if (warp == kMmaWarp) {
@@ -400,10 +434,10 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     // ===================== W generation =====================
     const unsigned gt0 = smem_addr(gt);
     for (int t = 0; t < n_iter; ++t) {
-      const int sw = t & 1, sg = t & 3;
+      const int sw = t % WS, sg = t & 3;
       int ok = 1;
       if (lane == 0) {
-        ok = (t < 2 || wait_or_abort(&wempty[sw], (unsigned)(((t >> 1) - 1) & 1), abort_flag)) &&
+        ok = (t < WS || wait_or_abort(&wempty[sw], (unsigned)(((t / WS) - 1) & 1), abort_flag)) &&
              wait_or_abort(&gfull[sg], (unsigned)((t >> 2) & 1), abort_flag);
       }
       __syncwarp();  // orders the other lanes' reads after lane 0's acquire
@@ -411,14 +445,18 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       if (!ok) break;
       const unsigned gbase = after_wait(gt0 + (unsigned)(sg * G::G_STAGE));
       const unsigned woff = (unsigned)(sw * G::W_STAGE);
-#define YASF_GEN_STEP(k, base, ta, tb) \
-  gen_step<base, ta, tb, S, G::IM_OFF, G::B_BYTES>(gc, go, gbase, ge[k], gd[k] + woff, gm[k] + woff);
+      const unsigned wsb = smem_addr(ws) + woff;
+#define YASF_GEN_STEP(k, base, ta, tb)                                                         \
+  gen_step<base, ta, tb, PK, SC, S, G::IM_OFF, G::B_BYTES>(                                     \
+      gc, go, gbase, ge[k], PK ? wsb + (gd[k] & 0xFFFFu) : gd[k] + woff,                         \
+      PK ? wsb + (gd[k] >> 16) : gm[PK ? 0 : k] + woff);
       if constexpr (L == 1) { YASF_PANEL_STEPS_1(YASF_GEN_STEP) }
       if constexpr (L == 2) { YASF_PANEL_STEPS_2(YASF_GEN_STEP) }
       if constexpr (L == 3) { YASF_PANEL_STEPS_3(YASF_GEN_STEP) }
       if constexpr (L == 4) { YASF_PANEL_STEPS_4(YASF_GEN_STEP) }
       if constexpr (L == 5) { YASF_PANEL_STEPS_5(YASF_GEN_STEP) }
       if constexpr (L == 6) { YASF_PANEL_STEPS_6(YASF_GEN_STEP) }
+      if constexpr (L == 7) { YASF_PANEL_STEPS_7(YASF_GEN_STEP) }
 #undef YASF_GEN_STEP
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
@@ -439,14 +477,14 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       constexpr unsigned long long bk = (unsigned long long)((2 * G::B_LBO) >> 4);
       bool stop = false;
       for (int t = 0; t < n_iter && !stop; ++t) {
-        const int sw = t & 1;
-        if (!wait_or_abort(&wfull[sw], (unsigned)((t >> 1) & 1), abort_flag)) break;
+        const int sw = t % WS;
+        if (!wait_or_abort(&wfull[sw], (unsigned)((t / WS) & 1), abort_flag)) break;
         const unsigned long long dw = db0 + (unsigned long long)sw * (unsigned long long)(G::W_STAGE >> 4);
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           const int u = t * NG + g;  // source-panel unit: pair t, group g
-          const int sx = u % 3;
-          if (!wait_or_abort(&xfull[sx], (unsigned)((u / 3) & 1), abort_flag)) {
+          const int sx = u % XS;
+          if (!wait_or_abort(&xfull[sx], (unsigned)((u / XS) & 1), abort_flag)) {
             stop = true;
             break;
           }
@@ -472,10 +510,10 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     if (lane == 0) {
       for (int u = 0; u < n_iter * NG; ++u) {
         const int t = u / NG, g = u - (u / NG) * NG;
-        const int sx = u % 3;
+        const int sx = u % XS;
         const int j = t < i ? t : t + 1;
         if (*abort_flag) break;
-        if (u >= 3 && !wait_or_abort(&xempty[sx], (unsigned)(((u / 3) - 1) & 1), abort_flag)) break;
+        if (u >= XS && !wait_or_abort(&xempty[sx], (unsigned)(((u / XS) - 1) & 1), abort_flag)) break;
         const unsigned char* src =
             reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)(grp0 + g) * N + j) * G::X_STAGE;
         issued[sx] = u;  // written before the copy: the next load into this stage waits for its MMAs
@@ -541,8 +579,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     // stage is issued only after the MMAs consumed the previous one, so only the newest load of
     // each stage can be in flight (bounded waits).
     if (tid == 0)
-      for (int b = 0; b < 3; ++b)
-        if (issued[b] >= 0) (void)panel_wait(&xfull[b], (unsigned)((issued[b] / 3) & 1));
+      for (int b = 0; b < XS; ++b)
+        if (issued[b] >= 0) (void)panel_wait(&xfull[b], (unsigned)((issued[b] / XS) & 1));
     // wait (bounded) for the MMAs before reading tensor memory
     const bool ok = n_iter == 0 || panel_wait(accum, 0);
     tc_fence_after();

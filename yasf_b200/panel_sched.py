@@ -1,4 +1,4 @@
-"""Build step: the W-generation schedule of the tensor-core panel kernel (lmax 1..6).
+"""Build step: the W-generation schedule of the tensor-core panel kernel (lmax 1..7).
 
 The panel kernel forms, for every ordered sphere pair (i, j), the two translation blocks of the
 tau-symmetric coupling, Wa (tau1 = tau2) and Wb (tau1 != tau2), and stores P = Wa + Wb and
@@ -152,7 +152,7 @@ def schedule(L: int):
     return steps, table
 
 
-def header_text(lmax_values=range(1, 7)) -> str:
+def header_text(lmax_values=range(1, 8)) -> str:
     out = [
         "// Generated by yasf_b200/panel_sched.py at build time: the W-generation schedule of the",
         "// tensor-core panel kernel. Do not edit.",

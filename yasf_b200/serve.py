@@ -10,7 +10,7 @@ incidences (directions x polarisations = R right-hand sides). The loop:
   interleave on the device while their GMRES state stays resident there;
 - solves in mixed precision: the batched refined solve (yasf_batched_solve) with the tensor-core
   TF32 panel as the inner operator (complex64 coupling kernel for one or two columns and beyond
-  lmax 6; with ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for
+  lmax 7; with ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for
   the request's (lmax, N, R)), float64 residuals,
   stopping at rtol (1e-6 by default, which keeps the extinction cross section well inside 1e-6 of
   the float64 solution);
@@ -75,9 +75,9 @@ def inner_kind(lmax: int, nrhs: int) -> str:
     """Inner operator of a request's refined solve.
 
     The TF32 tensor-core panel costs the same for 1 to 64 columns (about twice one complex64 column
-    application), so requests with one or two columns, and every lmax above the panel's 6, use the
+    application), so requests with one or two columns, and every lmax above the panel's 7, use the
     complex64 coupling kernel column by column."""
-    return "tf32" if lmax <= 6 and nrhs >= 3 else "c64"
+    return "tf32" if lmax <= 7 and nrhs >= 3 else "c64"
 
 
 def footprint_bytes(req: Request, cfg: ServeConfig, dev_plan_handle=None) -> int:
