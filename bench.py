@@ -647,7 +647,7 @@ def run_serve(args, rank: int, world: int) -> None:
         "metric": METRIC_SERVE, "value": tot["solves_per_s"], "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot["makespan_s"] * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "tf32 inner (lmax<=6) / c64 inner (lmax 7-8), c128 refinement",
+        "dtype": "tf32 inner (enough columns) / c64 inner (few columns), c128 refinement",
         "data": "synthetic (seeded request stream, no dataset)",
         "config": {"workload": f"serving stream, first {args.steps} of 512 requests (Poisson 20 req/s)",
                    "requests": args.steps, "slots": args.slots, "rtol": args.serve_rtol,

@@ -108,8 +108,8 @@ int yasf_master_matvec(const yasf_plan* plan, int n_particles, const double* pos
  * every pair block W_ij is generated once in FP32 (as the tau-symmetric P = Wa + Wb, Q = Wa - Wb)
  * and applied to the source's columns, 64 or 128 per block, on tcgen05 tensor cores (TF32 inputs,
  * FP32 accumulation; relative accuracy ~1e-3). y = x - T (.) (W x) when tmat is non-NULL, else
- * y = W x; x and y columns have leading dimensions ldx and ldy. lmax <= 7 (YASF_ERR_UNSUPPORTED
- * otherwise). */
+ * y = W x; x and y columns have leading dimensions ldx and ldy. Every lmax of
+ * a plan (1..8). */
 int yasf_panel_workspace_size(const yasf_plan* plan, int n_particles, int nrhs, size_t* bytes);
 int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const double* positions,
                       double k_medium, const double* tmat, const double* x, double* y, int nrhs,
@@ -135,7 +135,7 @@ int yasf_dpanel_matvec(const yasf_plan* plan, int n_particles, const double* pos
  * yasfpy/solver.py:108-121). Float64 iterative refinement: residuals B - A X in float64, inner
  * left-preconditioned GMRES cycles (restart steps, each column its own float64 Krylov basis, all
  * live columns sharing one operator application per step) to inner_rtol on the reduced-precision
- * operator inner_kind: 0 tensor-core TF32 panel (lmax <= 7), 1 complex64 coupling kernel,
+ * operator inner_kind: 0 tensor-core TF32 panel, 1 complex64 coupling kernel,
  * 2 complex128 coupling kernel. X0 = 0. Columns leave when ||B_c - A X_c|| <= rtol ||B_c||.
  * stats (host, may be NULL): [0] lockstep inner steps, [1] panel applications, [2] column
  * applications of kinds 1/2, [3] float64 residual column applications (float64 applications to

@@ -26,14 +26,15 @@ def test_cache_and_persistence(tmp_path):
 
     def measure(dev, tmat, nrhs):
         calls.append((dev.lmax, dev.n_particles, nrhs))
-        return {"c64": 5.0 * nrhs, "tf32": 40.0} if dev.lmax <= 6 else {"c64": 5.0 * nrhs}
+        # a shape without a panel candidate (fake: lmax 9) decides among what was measured
+        return {"c64": 5.0 * nrhs, "tf32": 40.0} if dev.lmax <= 8 else {"c64": 5.0 * nrhs}
 
     path = tmp_path / "tune.json"
     t = Autotuner(path=path, measure=measure)
     assert t.decide(FakeDev(6, 2000), None, 1).inner == "c64"
     assert t.decide(FakeDev(6, 2000), None, 64).inner == "tf32"
     assert t.decide(FakeDev(6, 2030), None, 64).inner == "tf32"   # same bucket: cached
-    assert t.decide(FakeDev(8, 2000), None, 64).inner == "c64"    # no panel above lmax 6
+    assert t.decide(FakeDev(9, 2000), None, 64).inner == "c64"    # no panel candidate
     assert len(calls) == 3
     t2 = Autotuner(path=path, measure=measure)
     assert t2.decide(FakeDev(6, 2000), None, 64).inner == "tf32"

@@ -14,13 +14,13 @@ from yasf_b200.incident import plane_wave_block
 from yasf_b200.mie import compute_mie_coefficients
 from yasf_b200.preconditioner import make_particle_partition
 from yasf_b200.wigner import translation_table_ab5
-from yasf_b200.workloads import aggregate_c1, incidences
+from yasf_b200.workloads import aggregate_c1, aggregate_c2, incidences
 
 pytestmark = pytest.mark.gpu
 
 
-def _problem(device, n=30, ndir=3):
-    agg = aggregate_c1(seed=4, n=n)
+def _problem(device, n=30, ndir=3, agg=None):
+    agg = aggregate_c1(seed=4, n=n) if agg is None else agg
     dev = CouplingDevice(agg.lmax, translation_table_ab5(agg.lmax), agg.positions, agg.k, device)
     pairs = np.array([[r, agg.refractive_index] for r in agg.radii])
     mie, _ = compute_mie_coefficients(agg.lmax, np.array([agg.k]), np.array([agg.k]), pairs)
@@ -79,3 +79,18 @@ def test_batched_zero_column(cuda_device):
     X, st = dev.batched_solve(tmat, B2, rtol=1e-9, restart=20, inner="tf32")
     assert st["unconverged"] == 0
     assert torch.count_nonzero(X[1]) == 0
+
+
+@pytest.mark.parametrize("lmax", [7, 8])
+def test_batched_tf32_high_lmax(cuda_device, lmax):
+    # the packed panel variant (FP16 coefficients, implicit pair-table addresses) as inner operator
+    agg, dev, tmat, B, A = _problem(cuda_device, ndir=2, agg=aggregate_c2(seed=5, n=10, lmax=lmax))
+    Xref = _reference(dev, tmat, B)
+    X, st = dev.batched_solve(tmat, B, rtol=1e-10, restart=40, inner="tf32", inner_rtol=1e-3)
+    assert st["unconverged"] == 0 and st["panel_matvecs"] > 0, st
+    Xn = X.cpu().numpy()
+    for c in range(B.shape[0]):
+        assert rel_err(Xn[c], Xref[c]) < 1e-8, c
+        ce = -np.real(np.vdot(A[c], Xn[c]))
+        cr = -np.real(np.vdot(A[c], Xref[c]))
+        assert abs(ce - cr) <= 1e-9 * abs(cr)

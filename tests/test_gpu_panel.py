@@ -28,7 +28,7 @@ def _setup(lmax, n, seed, device):
 
 @pytest.mark.parametrize("lmax,n,R", [(1, 5, 3), (2, 9, 1), (3, 17, 7), (4, 33, 64), (5, 12, 65), (6, 20, 16),
                                       (6, 41, 128), (3, 2, 2), (4, 23, 130), (5, 9, 200), (7, 19, 5),
-                                      (7, 27, 100)])
+                                      (7, 27, 100), (8, 7, 3), (8, 16, 70)])
 def test_panel_matches_float64_matvec(cuda_device, lmax, n, R):
     dev, rng = _setup(lmax, n, 100 + lmax, cuda_device)
     X = torch.from_numpy(rng.normal(size=(R, dev.n)) + 1j * rng.normal(size=(R, dev.n))).to(cuda_device)

@@ -5,7 +5,10 @@
 - arithmetic: emulating the kernel's generation in float64 from the schedule (items of an entry
   and its mirror, the A[p][|d|] table, phases e^{i d phi}, P = Wa + Wb, Q = Wa - Wb) and its
   tau-symmetric product (S = X1 + X2, D = X1 - X2, Y1 = (U + V) / 2, Y2 = (U - V) / 2) reproduces
-  the oracle's two-sphere coupling W_ij x_j to rounding.
+  the oracle's two-sphere coupling W_ij x_j to rounding; for lmax 7 and 8 the emulation reads the
+  pair table the way the packed kernel variant does (slot q of a step at row p0 + 2q of the lane's
+  term window, zero coefficients outside the item's terms) and checks every read stays inside the
+  written, finite part of the table.
 """
 
 from __future__ import annotations
@@ -14,11 +17,11 @@ import numpy as np
 import pytest
 
 from oracle import restate as R
-from yasf_b200.panel_sched import WARPS, _lm, mirror, schedule
+from yasf_b200.panel_sched import WARPS, _lm, mirror, schedule, window_starts
 from yasf_b200.wigner import translation_table_ab5
 
 
-@pytest.mark.parametrize("L", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("L", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_schedule_structure(L):
     steps, table = schedule(L)
     H = L * (L + 2)
@@ -39,7 +42,7 @@ def test_schedule_structure(L):
     assert collisions <= 4 * WARPS * len(steps)  # a few lanes per step, padding recomputation only
 
 
-def _emulate_wx(L, table_ab5, ri, rj, k, xj):
+def _emulate_wx(L, table_ab5, ri, rj, k, xj, packed=False):
     H = L * (L + 2)
     P = 2 * L + 1
     d = np.asarray(ri) - np.asarray(rj)
@@ -50,7 +53,12 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj):
     h = j + 1j * y
     leg = R.legendre(P - 1, ct, st)
     A = np.array([[leg[p, dd] * h[p] if dd <= p else 0 for dd in range(P)] for p in range(P)])
+    # the kernel's pair table: A[p][d] at p P + d (zero for p < d), phases at P P + 2L + delta
+    g = np.zeros(P * P + 4 * L + 1, dtype=complex)
+    g[:P * P] = A.reshape(-1)
+    g[P * P:] = np.exp(1j * np.arange(-2 * L, 2 * L + 1) * phi)
     steps, sched = schedule(L)
+    win = window_starts(L, steps, sched)
     Pm = np.full((H, H), np.nan, dtype=complex)
     Qm = np.full((H, H), np.nan, dtype=complex)
     tab = np.asarray(table_ab5)
@@ -64,11 +72,24 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj):
                 dl = m2 - m1
                 pmin = max(abs(l1 - l2), abs(dl))
                 Sa = Sb = 0j
-                for p in range(pmin, l1 + l2 + 1):
-                    if (l1 + l2 + p) % 2 == 0:
-                        Sa += tab[q2, q1, p].real * A[p, abs(dl)]
-                    else:
-                        Sb += tab[H + q2, q1, p].imag * A[p, abs(dl)]
+                if packed:
+                    pa0, pb0 = win[w][kk][sched[w][kk].index((q1, q2))]
+                    for which, (p0, T) in enumerate(((pa0, steps[kk][0]), (pb0, steps[kk][1]))):
+                        for q in range(T):
+                            p = p0 + 2 * q
+                            idx = p * P + abs(dl)
+                            assert 0 <= idx < g.size and np.isfinite(g[idx])
+                            real = pmin <= p <= l1 + l2 and ((l1 + l2 + p) % 2 == 0) == (which == 0)
+                            if which == 0:
+                                Sa += (tab[q2, q1, p].real if real else 0.0) * g[idx]
+                            else:
+                                Sb += (tab[H + q2, q1, p].imag if real else 0.0) * g[idx]
+                else:
+                    for p in range(pmin, l1 + l2 + 1):
+                        if (l1 + l2 + p) % 2 == 0:
+                            Sa += tab[q2, q1, p].real * A[p, abs(dl)]
+                        else:
+                            Sb += tab[H + q2, q1, p].imag * A[p, abs(dl)]
                 E = np.exp(1j * dl * phi)
                 Wa, Wb = E * Sa, 1j * E * Sb
                 Pm[q1, q2], Qm[q1, q2] = Wa + Wb, Wa - Wb
@@ -80,8 +101,8 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj):
     return np.concatenate([(U + V) / 2, (U - V) / 2])
 
 
-@pytest.mark.parametrize("L", [2, 4, 6, 7])
-def test_generation_algebra_matches_oracle(L):
+@pytest.mark.parametrize("L, packed", [(2, False), (4, False), (6, False), (7, True), (8, True)])
+def test_generation_algebra_matches_oracle(L, packed):
     rng = np.random.default_rng(L)
     tab = translation_table_ab5(L)
     k = 2 * np.pi / 0.55
@@ -90,5 +111,5 @@ def test_generation_algebra_matches_oracle(L):
     x = np.zeros(2 * nmax, dtype=complex)
     x[nmax:] = rng.normal(size=nmax) + 1j * rng.normal(size=nmax)
     ref = R.coupling_matvec_rows(L, pos, k, tab, x, 0, 1)
-    got = _emulate_wx(L, tab, pos[0], pos[1], k, x[nmax:])
+    got = _emulate_wx(L, tab, pos[0], pos[1], k, x[nmax:], packed=packed)
     assert np.max(np.abs(got - ref)) <= 1e-11 * np.max(np.abs(ref))

@@ -9,7 +9,7 @@ import time
 
 import numpy as np
 
-from yasf_b200.serve import RequestResult, ServeConfig, Server, summarize
+from yasf_b200.serve import RequestResult, ServeConfig, Server, inner_kind, summarize
 from yasf_b200.workloads import Aggregate, Request
 
 
@@ -84,3 +84,9 @@ def test_failed_request_does_not_stop_the_loop():
     res = srv.run([_req(i, 0.0) for i in range(3)], realtime=False)
     assert res[1].error.startswith("FloatingPointError")
     assert res[0].error is None and res[2].error is None
+
+
+def test_inner_kind_rule():
+    assert [inner_kind(6, r) for r in (1, 2, 3, 64)] == ["c64", "c64", "tf32", "tf32"]
+    assert [inner_kind(7, r) for r in (4, 5)] == ["c64", "tf32"]
+    assert [inner_kind(8, r) for r in (3, 4, 64)] == ["c64", "tf32", "tf32"]

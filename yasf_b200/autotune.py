@@ -2,7 +2,7 @@
 
 A refined batched solve spends almost all of its time in inner-operator applications, and which
 operator is cheapest depends on the shape of the problem: the TF32 tensor-core panel costs about the
-same for 1 to 64 columns (and is available up to lmax 7), the complex64 coupling kernel costs one
+same for 1 to 64 columns (and is available up to lmax 8), the complex64 coupling kernel costs one
 application per column, and both scale differently with the number of spheres. The tuner times
 one application of each candidate on the problem's own operator (random columns, CUDA events on the
 current stream), picks the cheapest per inner step, and caches the decision under
@@ -60,7 +60,7 @@ def measure_step_costs(dev: CouplingDevice, tmat: torch.Tensor, nrhs: int) -> di
     g = torch.Generator(device=dev.device).manual_seed(0)
     x1 = torch.randn(dev.n, dtype=torch.complex128, device=dev.device, generator=g)
     costs = {"c64": nrhs * _time_ms(lambda: dev.coupling(x1, YASF_C64))}
-    if dev.lmax <= 7 and nrhs >= 1:
+    if dev.lmax <= 8 and nrhs >= 1:
         X = torch.randn(nrhs, dev.n, dtype=torch.complex128, device=dev.device, generator=g)
         costs["tf32"] = _time_ms(lambda: dev.panel(X, tmat))
     return costs

@@ -305,7 +305,7 @@ extern "C" int yasf_batched_workspace_size(const yasf_plan* plan, int n_particle
   if (!plan || !bytes || n_particles <= 0 || nrhs <= 0 || restart <= 0 || restart > 512)
     return YASF_ERR_INVALID_ARGUMENT;
   if (inner_kind < 0 || inner_kind > 2) return YASF_ERR_INVALID_ARGUMENT;
-  if (inner_kind == 0 && plan->lmax > 7) return YASF_ERR_UNSUPPORTED;
+  if (inner_kind == 0 && plan->lmax > 8) return YASF_ERR_UNSUPPORTED;
   *bytes = batch_layout(plan, n_particles, nrhs, restart, inner_kind).total;
   return YASF_OK;
 }
@@ -321,7 +321,7 @@ extern "C" int yasf_batched_solve(const yasf_plan* plan, int n_particles, const 
   if (!tmat || !b || !x || nrhs <= 0 || restart <= 0 || restart > 512 || max_refine < 1 ||
       !(rtol >= 0.0) || !(inner_rtol > 0.0) || inner_kind < 0 || inner_kind > 2)
     return YASF_ERR_INVALID_ARGUMENT;
-  if (inner_kind == 0 && plan->lmax > 7) return YASF_ERR_UNSUPPORTED;
+  if (inner_kind == 0 && plan->lmax > 8) return YASF_ERR_UNSUPPORTED;
   if (!aligned16(tmat) || !aligned16(b) || !aligned16(x) || !aligned16(workspace))
     return YASF_ERR_ALIGNMENT;
   const int R = nrhs;

@@ -30,14 +30,19 @@ static unsigned short half_bits(float f) {
 // Generation data of the panel kernel from the build-time schedule (panel_sched.h). For every
 // generator thread and slot: the real coefficient and the byte offset of A[p][|d|] of one term of
 // the thread's item; for every step: the W-stage byte offsets of the P_r rows of the item's entry
-// and of its mirror, and the byte offset of the entry's phase e^{i d phi}. Wa coefficients are
-// real and Wb coefficients purely imaginary (a5 / b5 of the plan); the Wb value stored is b / i.
+// and of its mirror, and the byte offset of the entry's phase e^{i d phi}. Packed variant
+// (lmax 7-8): goff holds the FP16 coefficients two per word and the third dst row the step's
+// pair-table bases (Wa | Wb << 10 | phase << 20, entry units); slot q of a step's Wa (Wb) terms is
+// the term at p = p0 + 2q, with the window starts p0 from the schedule (kPanelWindow; they keep
+// every window inside table rows 0 .. 2L + 1 and are checked here against the item's terms). Wa
+// coefficients are real and Wb coefficients purely imaginary (a5 / b5 of the plan); the Wb value
+// stored is b / i.
 // The mirror entry's coefficients are not stored: they equal the entry's (Wa) or their negatives
 // (Wb), which the kernel applies. Terms below 1e-12 of the largest coefficient cannot change a
 // TF32 entry and are dropped.
 template <int L>
-static int build_terms_for(const double* ab5, const unsigned short* entry, const unsigned char* wa,
-                           const unsigned char* wb, std::vector<float>& coef,
+static int build_terms_for(const double* ab5, const unsigned short* entry, const unsigned short* window,
+                           const unsigned char* wa, const unsigned char* wb, std::vector<float>& coef,
                            std::vector<unsigned>& goff, std::vector<unsigned>& dst) {
   using Sched = PanelSched<L>;
   constexpr int S = Sched::kSlots, NS = Sched::kSteps;
@@ -86,8 +91,9 @@ static int build_terms_for(const double* ab5, const unsigned short* entry, const
             return YASF_ERR_INVALID_ARGUMENT;
         }
       }
+  constexpr bool PK = PanelGeom<L>::PACKED;
   coef.assign((size_t)S * kGenThreads, 0.f);
-  goff.assign((size_t)S * kGenThreads, 0u);
+  goff.assign((size_t)(PK ? (S + 1) / 2 : S) * kGenThreads, 0u);
   dst.assign((size_t)3 * NS * kGenThreads, 0u);
   for (int th = 0; th < kGenThreads; ++th) {
     const int w = th >> 5, lane = th & 31;
@@ -104,21 +110,36 @@ static int build_terms_for(const double* ab5, const unsigned short* entry, const
       }
       dst[(size_t)k * kGenThreads + th] = (unsigned)kmajor_offset(q1, q2, 2 * HP);
       dst[(size_t)(NS + k) * kGenThreads + th] = (unsigned)kmajor_offset(mq1, mq2, 2 * HP);
-      dst[(size_t)(2 * NS + k) * kGenThreads + th] = (unsigned)((P * P + 2 * L + (m2 - m1)) * 8);
+      const int ad = std::abs(m2 - m1);
+      const int pmin = std::max(std::abs(l1 - l2), ad);
+      // packed variant: window starts p0 of the Wa and Wb terms (inside rows 0 .. 2L + 1)
+      const unsigned wv = window[((size_t)w * NS + k) * 32 + lane];
+      const int p0[2] = {(int)(wv & 255u), (int)(wv >> 8)};
+      if (PK && (p0[0] + 2 * (wa[k] - 1) > 2 * L + 1 || p0[1] + 2 * (wb[k] - 1) > 2 * L + 1))
+        return YASF_ERR_INVALID_ARGUMENT;
+      dst[(size_t)(2 * NS + k) * kGenThreads + th] =
+          PK ? (unsigned)(p0[0] * P + ad) | ((unsigned)(p0[1] * P + ad) << 10) |
+                   ((unsigned)(P * P + 2 * L + (m2 - m1)) << 20)
+             : (unsigned)((P * P + 2 * L + (m2 - m1)) * 8);
       if (real) {
-        const int pmin = std::max(std::abs(l1 - l2), std::abs(m2 - m1));
         int na = 0, nb = 0;
         for (int p = pmin; p <= l1 + l2; ++p) {
           const int which = ((l1 + l2 + p) % 2 == 0) ? 0 : 1;
           double cr, ci;
           coefficient(which, q1, q2, p, cr, ci);
-          const int slot = which == 0 ? base + na++ : base + wa[k] + nb++;
-          if (na > wa[k] || nb > wb[k]) return YASF_ERR_INVALID_ARGUMENT;
+          const int j = PK ? (p - p0[which]) / 2 : (which == 0 ? na : nb);
+          which == 0 ? ++na : ++nb;
+          if (na > wa[k] || nb > wb[k] || j < 0 || j >= (which == 0 ? wa[k] : wb[k]) ||
+              (PK && (p - p0[which]) % 2 != 0))
+            return YASF_ERR_INVALID_ARGUMENT;
+          const int slot = which == 0 ? base + j : base + wa[k] + j;
           const float cf = (float)(which == 0 ? cr : ci);
-          const unsigned idx = (unsigned)(p * P + std::abs(m2 - m1));
           coef[(size_t)slot * kGenThreads + th] = cf;
-          goff[(size_t)slot * kGenThreads + th] =
-              PanelGeom<L>::PACKED ? ((unsigned)half_bits(cf) << 16) | idx : idx * 8;
+          if constexpr (PK) {
+            goff[(size_t)(slot >> 1) * kGenThreads + th] |= (unsigned)half_bits(cf) << (16 * (slot & 1));
+          } else {
+            goff[(size_t)slot * kGenThreads + th] = (unsigned)(p * P + ad) * 8;
+          }
         }
       }
       base += wa[k] + wb[k];
@@ -133,23 +154,30 @@ int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::v
   coef.clear();
   goff.clear();
   dst.clear();
+#define YASF_TERMS(n)                                                                             \
+  case n:                                                                                         \
+    return build_terms_for<n>(ab5, kPanelEntry##n, kPanelWindow##n, kPanelStepWa##n, kPanelStepWb##n, \
+                              coef, goff, dst);
   switch (L) {
-    case 1: return build_terms_for<1>(ab5, kPanelEntry1, kPanelStepWa1, kPanelStepWb1, coef, goff, dst);
-    case 2: return build_terms_for<2>(ab5, kPanelEntry2, kPanelStepWa2, kPanelStepWb2, coef, goff, dst);
-    case 3: return build_terms_for<3>(ab5, kPanelEntry3, kPanelStepWa3, kPanelStepWb3, coef, goff, dst);
-    case 4: return build_terms_for<4>(ab5, kPanelEntry4, kPanelStepWa4, kPanelStepWb4, coef, goff, dst);
-    case 5: return build_terms_for<5>(ab5, kPanelEntry5, kPanelStepWa5, kPanelStepWb5, coef, goff, dst);
-    case 6: return build_terms_for<6>(ab5, kPanelEntry6, kPanelStepWa6, kPanelStepWb6, coef, goff, dst);
-    case 7: return build_terms_for<7>(ab5, kPanelEntry7, kPanelStepWa7, kPanelStepWb7, coef, goff, dst);
-    default: return YASF_OK;  // no tensor-core panel beyond lmax 7
+    YASF_TERMS(1)
+    YASF_TERMS(2)
+    YASF_TERMS(3)
+    YASF_TERMS(4)
+    YASF_TERMS(5)
+    YASF_TERMS(6)
+    YASF_TERMS(7)
+    YASF_TERMS(8)
+    default: return YASF_OK;
   }
+#undef YASF_TERMS
 }
 
 // Right-hand-side groups of 64 per panel block: two as soon as there are two (each W_ij is then
 // generated once for 128 columns), padded to an even count whose extra columns are zero.
-static int panel_groups_per_block(int groups) { return groups >= 2 ? 2 : 1; }
-static int panel_padded_groups(int groups) {
-  const int ng = panel_groups_per_block(groups);
+// lmax 8 keeps one group per block: two groups' accumulators would exceed tensor memory.
+static int panel_groups_per_block(int groups, int lmax) { return groups >= 2 && lmax <= 7 ? 2 : 1; }
+static int panel_padded_groups(int groups, int lmax) {
+  const int ng = panel_groups_per_block(groups, lmax);
   return (groups + ng - 1) / ng * ng;
 }
 
@@ -166,15 +194,17 @@ static int launch_panel_ng(const PanelArgs& pa, int padded, cudaStream_t s) {
 
 template <int L>
 static int launch_panel(const PanelArgs& pa, int groups, cudaStream_t s) {
-  const int padded = panel_padded_groups(groups);
+  const int padded = panel_padded_groups(groups, L);
   {
     const dim3 grid(pa.n_particles, padded);
     YASF_COUNTED(xpanel_kernel<L><<<grid, 256, 0, s>>>(pa.n_particles, pa.nmax, pa.nrhs, pa.ld, pa.x,
                                                      const_cast<float*>(pa.xp)));
     YASF_CUDA_TRY(cudaGetLastError());
   }
-  return panel_groups_per_block(groups) == 2 ? launch_panel_ng<L, 2>(pa, padded, s)
-                                             : launch_panel_ng<L, 1>(pa, padded, s);
+  if constexpr (4 * PanelGeom<L>::HP * 2 <= 512) {
+    if (panel_groups_per_block(groups, L) == 2) return launch_panel_ng<L, 2>(pa, padded, s);
+  }
+  return launch_panel_ng<L, 1>(pa, padded, s);
 }
 
 static size_t panel_xstage(int L) {
@@ -186,6 +216,7 @@ static size_t panel_xstage(int L) {
     case 5: return PanelGeom<5>::X_STAGE;
     case 6: return PanelGeom<6>::X_STAGE;
     case 7: return PanelGeom<7>::X_STAGE;
+    case 8: return PanelGeom<8>::X_STAGE;
     default: return 0;
   }
 }
@@ -199,7 +230,7 @@ extern "C" int yasf_panel_workspace_size(const yasf_plan* plan, int n_particles,
   if (!plan || !bytes || n_particles <= 0 || nrhs <= 0) return YASF_ERR_INVALID_ARGUMENT;
   const size_t xs = panel_xstage(plan->lmax);
   if (!xs) return YASF_ERR_UNSUPPORTED;
-  const size_t groups = (size_t)panel_padded_groups((nrhs + 63) / 64);
+  const size_t groups = (size_t)panel_padded_groups((nrhs + 63) / 64, plan->lmax);
   *bytes = ((groups * n_particles * xs + 255) & ~size_t(255)) + 256;
   return YASF_OK;
 }
@@ -250,6 +281,7 @@ extern "C" int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const d
     case 5: return launch_panel<5>(pa, groups, s);
     case 6: return launch_panel<6>(pa, groups, s);
     case 7: return launch_panel<7>(pa, groups, s);
+    case 8: return launch_panel<8>(pa, groups, s);
     default: return YASF_ERR_UNSUPPORTED;
   }
 }

@@ -22,7 +22,7 @@
 // banks; warps 0-3 also read the accumulators at the end. Warp 16 owns tensor memory and its
 // elected thread issues the MMAs. Warps 17 and 18 compute the pair tables of alternate pairs;
 // warp 19 issues the cp.async.bulk copies of the source panels. Three source-panel stages, two W
-// stages and four pair-table stages are in flight. Every wait is bounded in time: a timeout sets
+// stages and four pair-table stages are in flight (lmax 7: two and one; lmax 8: one and one). Every wait is bounded in time: a timeout sets
 // the error word, every role stops, the result is written as NaN and tensor memory is freed.
 #pragma once
 
@@ -53,17 +53,19 @@ struct PanelGeom {
   static constexpr int A_LBO = (A_ROWS / 8) * 128;   // bytes between 4-column K chunks
   static constexpr int A_BYTES = A_ROWS * HP * 4;
   static constexpr int X_STAGE = 2 * A_BYTES;        // one source panel (S and D operands)
-  static constexpr int X_STAGES = L <= 6 ? 3 : 2;    // lmax 7: shared memory allows two
+  static constexpr int X_STAGES = L <= 6 ? 3 : (L == 7 ? 2 : 1);  // what shared memory allows
   // B operands [P_r; P_i], [Q_r; Q_i]: 2 HP rows x HP columns
   static constexpr int B_ROWS = 2 * HP;
   static constexpr int B_LBO = (B_ROWS / 8) * 128;
   static constexpr int B_BYTES = B_ROWS * HP * 4;
   static constexpr int W_STAGE = 2 * B_BYTES;
-  static constexpr int W_STAGES = L <= 6 ? 2 : 1;    // lmax 7: generation waits for the MMAs
-  // lmax 7: a thread's 40 generation slots are packed (FP16 coefficient << 16 | table index) to fit
-  // the register budget; up to lmax 6 coefficient and byte offset are separate registers
+  static constexpr int W_STAGES = L <= 6 ? 2 : 1;    // lmax 7-8: generation waits for the MMAs
+  // lmax 7-8 (40 / 62 generation slots per thread): coefficients are held as FP16 pairs and the
+  // pair-table addresses of a step's terms are implicit (see gen_step_packed), so the generation
+  // state fits the register budget; up to lmax 6 every slot holds an FP32 coefficient and a byte
+  // offset
   static constexpr bool PACKED = L >= 7;
-  static_assert(!PACKED || W_STAGE <= 65536, "packed store offsets need W stages of at most 64 KB");
+  static_assert(!PACKED || W_STAGE / 4 <= 65536, "packed store offsets (4-byte units) exceed 16 bits");
   static constexpr int IM_OFF = (HP / 8) * 128;      // row HP + q of a B operand vs row q
   // pair table: A[p][d] at p*P + d, e^{i delta phi} at P*P + 2L + delta (float2)
   static constexpr int G_STAGE = (P * P + 4 * L + 1) * 8;
@@ -79,7 +81,9 @@ struct PanelGeom {
   static_assert(X_STAGE % 1024 == 0 && W_STAGE % 1024 == 0, "operand stages must stay aligned");
   // epilogue exchange of the imaginary-row accumulators (reuses the source-panel stages)
   static constexpr int XCH_STRIDE = 4 * HP + 1;  // floats per row (odd: conflict-free)
-  static_assert(64 * XCH_STRIDE * 4 <= X_STAGES * X_STAGE, "exchange buffer does not fit");
+  // (the source-panel and W stages are contiguous and both idle when the exchange runs)
+  static_assert(64 * XCH_STRIDE * 4 <= X_STAGES * X_STAGE + W_STAGES * W_STAGE,
+                "exchange buffer does not fit");
 };
 
 // Byte offset of element (row, k) in a canonical K-major no-swizzle operand with `rows` rows.
@@ -239,46 +243,13 @@ __device__ __forceinline__ unsigned after_wait(unsigned v) {
   return r;
 }
 
-// One schedule step of W generation for this thread: the item's TA Wa terms and TB Wb terms
-// (real coefficients on A[p][|d|]) into Sa, Sb; then, with E = e^{i d phi},
+// P = Wa + Wb and Q = Wa - Wb of an item to their four operand rows each, from the term sums
+// Sa = (ar, ai), Sb = (br, bi) and E = e^{i d phi}:
 //   entry:  Wa = E Sa,       Wb = i E Sb
 //   mirror: Wa' = conj(E) Sa, Wb' = -i conj(E) Sb
-// and P = Wa + Wb, Q = Wa - Wb of both to their four operand rows each.
-template <bool PACKED, int SC, int S>
-__device__ __forceinline__ void slot(const float (&gc)[SC], const unsigned (&go)[S], int q, float& c,
-                                     unsigned& off) {
-  if constexpr (PACKED) {
-    c = __half2float(__ushort_as_half((unsigned short)(go[q] >> 16)));
-    off = (go[q] & 0xFFFFu) << 3;
-  } else {
-    c = gc[q];
-    off = go[q];
-  }
-}
-
-template <int BASE, int TA, int TB, bool PACKED, int SC, int S, int IM_OFF, int B_BYTES>
-__device__ __forceinline__ void gen_step(const float (&gc)[SC], const unsigned (&go)[S], unsigned gbase,
-                                         unsigned eoff, unsigned dst, unsigned dstm) {
-  float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
-#pragma unroll
-  for (int q = 0; q < TA; ++q) {
-    float c;
-    unsigned off;
-    slot<PACKED>(gc, go, BASE + q, c, off);
-    const float2 g = lds_f2(gbase + off);
-    ar = fmaf(c, g.x, ar);
-    ai = fmaf(c, g.y, ai);
-  }
-#pragma unroll
-  for (int q = 0; q < TB; ++q) {
-    float c;
-    unsigned off;
-    slot<PACKED>(gc, go, BASE + TA + q, c, off);
-    const float2 g = lds_f2(gbase + off);
-    br = fmaf(c, g.x, br);
-    bi = fmaf(c, g.y, bi);
-  }
-  const float2 e = lds_f2(gbase + eoff);
+template <int IM_OFF, int B_BYTES>
+__device__ __forceinline__ void store_item(float2 e, float ar, float ai, float br, float bi, unsigned dst,
+                                           unsigned dstm) {
   {
     const float ur = e.x * ar - e.y * ai, ui = e.x * ai + e.y * ar;
     const float vr = e.x * br - e.y * bi, vi = e.x * bi + e.y * br;
@@ -295,6 +266,63 @@ __device__ __forceinline__ void gen_step(const float (&gc)[SC], const unsigned (
     sts_f32(dstm + B_BYTES, to_tf32(ur - vi));
     sts_f32(dstm + B_BYTES + IM_OFF, to_tf32(ui + vr));
   }
+}
+
+// One schedule step of W generation for this thread (lmax <= 6): the item's TA Wa terms and TB Wb
+// terms, each an FP32 coefficient gc[q] on the pair-table entry at byte offset go[q].
+template <int BASE, int TA, int TB, int S, int IM_OFF, int B_BYTES>
+__device__ __forceinline__ void gen_step(const float (&gc)[S], const unsigned (&go)[S], unsigned gbase,
+                                         unsigned eoff, unsigned dst, unsigned dstm) {
+  float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
+#pragma unroll
+  for (int q = 0; q < TA; ++q) {
+    const float2 g = lds_f2(gbase + go[BASE + q]);
+    ar = fmaf(gc[BASE + q], g.x, ar);
+    ai = fmaf(gc[BASE + q], g.y, ai);
+  }
+#pragma unroll
+  for (int q = 0; q < TB; ++q) {
+    const float2 g = lds_f2(gbase + go[BASE + TA + q]);
+    br = fmaf(gc[BASE + TA + q], g.x, br);
+    bi = fmaf(gc[BASE + TA + q], g.y, bi);
+  }
+  store_item<IM_OFF, B_BYTES>(lds_f2(gbase + eoff), ar, ai, br, bi, dst, dstm);
+}
+
+// FP16 coefficient of slot q from the packed pairs (slot 2w in the low half of word w).
+template <int NW>
+__device__ __forceinline__ float packed_coef(const unsigned (&gh)[NW], int q) {
+  const unsigned w = gh[q >> 1];
+  return __half2float(__ushort_as_half((unsigned short)((q & 1) ? (w >> 16) : (w & 0xFFFFu))));
+}
+
+// One schedule step of W generation for this thread (lmax 7-8). The Wa terms of an item run over
+// p = p0, p0 + 2, ... at one |d|, so slot q of the step reads A[p0a + 2q][|d|]: table entry
+// ia + 2 P q, with the step's bases ia, ib (Wb) and the phase entry ie packed in `bases` (10 bits
+// each, entry units). The plan places each lane's window [p0, p0 + 2 (T - 1)] inside rows
+// 0 .. 2L + 1 of the table (row 2L + 1 is the phase row) with zero coefficients on the slots
+// outside the item's own terms; rows p < d are never written and stay zero.
+template <int BASE, int TA, int TB, int P, int NW, int IM_OFF, int B_BYTES>
+__device__ __forceinline__ void gen_step_packed(const unsigned (&gh)[NW], unsigned gbase, unsigned bases,
+                                                unsigned dst, unsigned dstm) {
+  const unsigned ga = gbase + ((bases & 1023u) << 3);
+  const unsigned gb = gbase + (((bases >> 10) & 1023u) << 3);
+  float ar = 0.f, ai = 0.f, br = 0.f, bi = 0.f;
+#pragma unroll
+  for (int q = 0; q < TA; ++q) {
+    const float c = packed_coef(gh, BASE + q);
+    const float2 g = lds_f2(ga + (unsigned)(q * 16 * P));
+    ar = fmaf(c, g.x, ar);
+    ai = fmaf(c, g.y, ai);
+  }
+#pragma unroll
+  for (int q = 0; q < TB; ++q) {
+    const float c = packed_coef(gh, BASE + TA + q);
+    const float2 g = lds_f2(gb + (unsigned)(q * 16 * P));
+    br = fmaf(c, g.x, br);
+    bi = fmaf(c, g.y, bi);
+  }
+  store_item<IM_OFF, B_BYTES>(lds_f2(gbase + ((bases >> 20) << 3)), ar, ai, br, bi, dst, dstm);
 }
 
 // The pair table of one pair, lane d (< P): A[p][d] = Pn_p^d(cos theta) h_p(x) for p >= d at
@@ -338,13 +366,14 @@ template <int L, int NG>
 __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   using G = PanelGeom<L>;
   constexpr int TMEM_COLS = tmem_cols(4 * G::HP * NG);
+  static_assert(4 * G::HP * NG <= 512, "accumulators exceed tensor memory");
   using Sched = PanelSched<L>;
   static_assert(Sched::kWarps == kGenWarps, "schedule built for another warp count");
   constexpr int H = G::H, HP = G::HP, P = G::P, KS = G::KS;
   constexpr int S = Sched::kSlots, NS = Sched::kSteps;
   constexpr int XS = G::X_STAGES, WS = G::W_STAGES;
   constexpr bool PK = G::PACKED;
-  constexpr int SC = PK ? 1 : S;
+  constexpr int NW = (S + 1) / 2;  // packed coefficient words
   extern __shared__ __align__(1024) unsigned char panel_smem[];
   unsigned char* xs = panel_smem + G::X_OFF;                                  // [XS][X_STAGE]
   unsigned char* ws = panel_smem + G::W_OFF;                                  // [WS][W_STAGE]
@@ -371,24 +400,31 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   const int N = a.n_particles;
   const int n_iter = N - 1;    // every source but the receiver itself
 
-  // generation data of this thread (registers)
-  float gc[SC];
-  unsigned go[S];
+  // generation data of this thread (registers): per slot an FP32 coefficient and a pair-table
+  // offset, or (packed variant) two FP16 coefficients per word
+  float gc[PK ? 1 : S];
+  unsigned go[PK ? 1 : S], gh[PK ? NW : 1];
   // store offsets of the entry and mirror rows: absolute shared addresses, or (packed variant)
-  // both W-stage offsets (< 64 KB) in one register, entry in the low half
+  // both W-stage offsets in 4-byte units in one register, entry in the low half; ge: the phase
+  // offset, or (packed variant) the step's table bases
   unsigned gd[NS], gm[PK ? 1 : NS], ge[NS];
   if (tid < kGenThreads) {
+    if constexpr (PK) {
 #pragma unroll
-    for (int q = 0; q < S; ++q) {
-      if constexpr (!PK) gc[q] = __ldg(a.gen_coef + q * kGenThreads + tid);
-      go[q] = __ldg(a.gen_goff + q * kGenThreads + tid);
+      for (int w = 0; w < NW; ++w) gh[w] = __ldg(a.gen_goff + w * kGenThreads + tid);
+    } else {
+#pragma unroll
+      for (int q = 0; q < S; ++q) {
+        gc[q] = __ldg(a.gen_coef + q * kGenThreads + tid);
+        go[q] = __ldg(a.gen_goff + q * kGenThreads + tid);
+      }
     }
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
       const unsigned od = __ldg(a.gen_dst + k * kGenThreads + tid);
       const unsigned om = __ldg(a.gen_dst + (NS + k) * kGenThreads + tid);
       if constexpr (PK) {
-        gd[k] = od | (om << 16);
+        gd[k] = (od >> 2) | ((om >> 2) << 16);  // 4-byte units
       } else {
         gd[k] = smem_addr(ws) + od;
         gm[k] = smem_addr(ws) + om;
@@ -396,8 +432,10 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       ge[k] = __ldg(a.gen_dst + (2 * NS + k) * kGenThreads + tid);
     }
   }
-  // zero both W stages (padding rows and columns stay zero), Legendre tables to shared memory
-  for (int o = tid; o < (G::W_STAGES * G::W_STAGE) / 16; o += blockDim.x)
+  // zero the W stages (padding rows and columns stay zero) and the pair-table stages (entries
+  // p < d are never written), Legendre tables to shared memory
+  static_assert(G::G_STAGE % 16 == 0 && G::G_OFF == G::W_OFF + G::W_STAGES * G::W_STAGE, "layout");
+  for (int o = tid; o < (G::W_STAGES * G::W_STAGE + G::G_STAGES * G::G_STAGE) / 16; o += blockDim.x)
     reinterpret_cast<float4*>(ws)[o] = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int o = tid; o < P * P; o += blockDim.x) {
     const int p = o / P, d = o - (o / P) * P;
@@ -447,9 +485,13 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       const unsigned woff = (unsigned)(sw * G::W_STAGE);
       const unsigned wsb = smem_addr(ws) + woff;
 #define YASF_GEN_STEP(k, base, ta, tb)                                                         \
-  gen_step<base, ta, tb, PK, SC, S, G::IM_OFF, G::B_BYTES>(                                     \
-      gc, go, gbase, ge[k], PK ? wsb + (gd[k] & 0xFFFFu) : gd[k] + woff,                         \
-      PK ? wsb + (gd[k] >> 16) : gm[PK ? 0 : k] + woff);
+  if constexpr (PK) {                                                                           \
+    gen_step_packed<base, ta, tb, P, NW, G::IM_OFF, G::B_BYTES>(                                \
+        gh, gbase, ge[k], wsb + ((gd[k] & 0xFFFFu) << 2), wsb + ((gd[k] >> 16) << 2));           \
+  } else {                                                                                      \
+    gen_step<base, ta, tb, (PK ? 1 : S), G::IM_OFF, G::B_BYTES>(gc, go, gbase, ge[k],           \
+                                                                 gd[k] + woff, gm[PK ? 0 : k] + woff); \
+  }
       if constexpr (L == 1) { YASF_PANEL_STEPS_1(YASF_GEN_STEP) }
       if constexpr (L == 2) { YASF_PANEL_STEPS_2(YASF_GEN_STEP) }
       if constexpr (L == 3) { YASF_PANEL_STEPS_3(YASF_GEN_STEP) }
@@ -457,6 +499,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       if constexpr (L == 5) { YASF_PANEL_STEPS_5(YASF_GEN_STEP) }
       if constexpr (L == 6) { YASF_PANEL_STEPS_6(YASF_GEN_STEP) }
       if constexpr (L == 7) { YASF_PANEL_STEPS_7(YASF_GEN_STEP) }
+      if constexpr (L == 8) { YASF_PANEL_STEPS_8(YASF_GEN_STEP) }
 #undef YASF_GEN_STEP
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();

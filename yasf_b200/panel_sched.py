@@ -1,4 +1,4 @@
-"""Build step: the W-generation schedule of the tensor-core panel kernel (lmax 1..7).
+"""Build step: the W-generation schedule of the tensor-core panel kernel (lmax 1..8).
 
 The panel kernel forms, for every ordered sphere pair (i, j), the two translation blocks of the
 tau-symmetric coupling, Wa (tau1 = tau2) and Wb (tau1 != tau2), and stores P = Wa + Wb and
@@ -26,8 +26,8 @@ generator threads computes in which step so that
 Lanes without an item of their class in a step write zeros to a padding entry (row or column
 beyond the lmax(lmax+2) modes) of that class, or recompute an item that another lane also
 computes (same values, same addresses). The output header holds, per lmax, the step table as a
-macro list and the (warp, step, lane) -> primary entry table used by the plan to lay out
-coefficients.
+macro list, the (warp, step, lane) -> primary entry table used by the plan to lay out
+coefficients, and the term windows of the packed variant (``window_starts``).
 """
 
 from __future__ import annotations
@@ -152,7 +152,39 @@ def schedule(L: int):
     return steps, table
 
 
-def header_text(lmax_values=range(1, 8)) -> str:
+def window_start(L: int, q1: int, q2: int, which: int, T: int) -> int:
+    """First order p0 of a lane's window of T slots for the Wa (which=0) or Wb terms of (q1, q2).
+
+    The packed generation reads slot q at table row p0 + 2q (column |d|), so the window must cover
+    the item's own terms (same parity, stride 2) and stay inside rows 0 .. 2L + 1: rows p < |d|
+    hold zeros and row 2L + 1 is the phase row of the pair table, both finite. The window starts
+    at the item's first term and moves down by 2 until it fits. Padding entries (q1 or q2 beyond
+    the modes) start at 0.
+    """
+    H = L * (L + 2)
+    first = last = -1
+    if q1 < H and q2 < H:
+        l1, m1 = _lm(q1)
+        l2, m2 = _lm(q2)
+        pmin = max(abs(l1 - l2), abs(m2 - m1))
+        ps = [p for p in range(pmin, l1 + l2 + 1) if ((l1 + l2 + p) % 2 == 0) == (which == 0)]
+        if ps:
+            first, last = ps[0], ps[-1]
+    p0 = max(first, 0)
+    while p0 >= 0 and p0 + 2 * (T - 1) > 2 * L + 1:
+        p0 -= 2
+    if p0 < 0 or (first >= 0 and p0 + 2 * (T - 1) < last):
+        raise RuntimeError(f"lmax {L}: no term window for entry ({q1}, {q2})")
+    return p0
+
+
+def window_starts(L: int, steps, table):
+    """[warp][step][lane] -> (p0 of the Wa window, p0 of the Wb window)."""
+    return [[[(window_start(L, q1, q2, 0, steps[k][0]), window_start(L, q1, q2, 1, steps[k][1]))
+              for (q1, q2) in table[w][k]] for k in range(len(steps))] for w in range(WARPS)]
+
+
+def header_text(lmax_values=range(1, 9)) -> str:
     out = [
         "// Generated by yasf_b200/panel_sched.py at build time: the W-generation schedule of the",
         "// tensor-core panel kernel. Do not edit.",
@@ -185,6 +217,13 @@ def header_text(lmax_values=range(1, 8)) -> str:
         flat = [(q1 << 8) | q2 for w in range(WARPS) for k in range(len(steps)) for (q1, q2) in table[w][k]]
         out.append("// primary entry (q1 << 8 | q2) of [warp][step][lane]")
         out.append(f"static const unsigned short kPanelEntry{L}[{len(flat)}] = {{")
+        for i in range(0, len(flat), 16):
+            out.append("    " + ", ".join(str(v) for v in flat[i:i + 16]) + ",")
+        out.append("};")
+        win = window_starts(L, steps, table)
+        flat = [a | (b << 8) for w in range(WARPS) for k in range(len(steps)) for (a, b) in win[w][k]]
+        out.append("// term windows of the packed variant: p0 of Wa | p0 of Wb << 8, [warp][step][lane]")
+        out.append(f"static const unsigned short kPanelWindow{L}[{len(flat)}] = {{")
         for i in range(0, len(flat), 16):
             out.append("    " + ", ".join(str(v) for v in flat[i:i + 16]) + ",")
         out.append("};")

@@ -9,8 +9,7 @@ incidences (directions x polarisations = R right-hand sides). The loop:
 - runs every admitted request on its own CUDA stream, so the kernels of in-flight solves
   interleave on the device while their GMRES state stays resident there;
 - solves in mixed precision: the batched refined solve (yasf_batched_solve) with the tensor-core
-  TF32 panel as the inner operator (complex64 coupling kernel for one or two columns and beyond
-  lmax 7; with ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for
+  TF32 panel as the inner operator (complex64 coupling kernel for one or two columns; with ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for
   the request's (lmax, N, R)), float64 residuals,
   stopping at rtol (1e-6 by default, which keeps the extinction cross section well inside 1e-6 of
   the float64 solution);
@@ -71,13 +70,17 @@ class RequestResult:
         return self.finished - self.arrival
 
 
-def inner_kind(lmax: int, nrhs: int) -> str:
-    """Inner operator of a request's refined solve.
+# Columns from which one TF32 panel step is cheaper than complex64 column applications: one panel
+# step at 1000 spheres costs 1.7 (lmax 6), 4.9 (lmax 7) and 3.1 (lmax 8) complex64 columns (both
+# grow like N^2, so the ratio holds across sizes).
+_PANEL_MIN_COLUMNS = {7: 5, 8: 4}
 
-    The TF32 tensor-core panel costs the same for 1 to 64 columns (about twice one complex64 column
-    application), so requests with one or two columns, and every lmax above the panel's 7, use the
+
+def inner_kind(lmax: int, nrhs: int) -> str:
+    """Inner operator of a request's refined solve: the TF32 tensor-core panel once the request has
+    enough columns to amortise one panel step (3 up to lmax 6, 5 at lmax 7, 4 at lmax 8), else the
     complex64 coupling kernel column by column."""
-    return "tf32" if lmax <= 7 and nrhs >= 3 else "c64"
+    return "tf32" if lmax <= 8 and nrhs >= _PANEL_MIN_COLUMNS.get(lmax, 3) else "c64"
 
 
 def footprint_bytes(req: Request, cfg: ServeConfig, dev_plan_handle=None) -> int:
