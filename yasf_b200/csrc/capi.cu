@@ -336,11 +336,10 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
   std::vector<unsigned> gen_meta, gen_dst;
   std::vector<int4> dgen_chunks;
   std::vector<int2> dgen_items;
-  std::vector<int> dgen_idx;
   std::vector<double> dgen_coef;
   {
     int bst = panel_build_terms(L, ab5, gen_c1, gen_meta, gen_dst);
-    if (bst == YASF_OK) bst = dpanel_build_items(L, ab5, dgen_chunks, dgen_items, dgen_idx, dgen_coef);
+    if (bst == YASF_OK) bst = dpanel_build_items(L, ab5, dgen_chunks, dgen_items, dgen_coef);
     if (bst != YASF_OK) {
       delete plan;
       set_error_text("translation table does not follow the a5/b5 selection rules of the panel schedule");
@@ -382,7 +381,6 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     cudaFree(plan->d_gen_dst);
     cudaFree(plan->d_dgen_chunks);
     cudaFree(plan->d_dgen_items);
-    cudaFree(plan->d_dgen_idx);
     cudaFree(plan->d_dgen_coef);
     delete plan;
     return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
@@ -411,7 +409,6 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
   if (!dgen_chunks.empty()) {
     YASF_UPLOAD(plan->d_dgen_chunks, dgen_chunks);
     YASF_UPLOAD(plan->d_dgen_items, dgen_items);
-    YASF_UPLOAD(plan->d_dgen_idx, dgen_idx);
     YASF_UPLOAD(plan->d_dgen_coef, dgen_coef);
     plan->dgen_chunks = (int)dgen_chunks.size();
   }
@@ -438,7 +435,6 @@ extern "C" int yasf_plan_destroy(yasf_plan* plan) {
   cudaFree(plan->d_gen_dst);
   cudaFree(plan->d_dgen_chunks);
   cudaFree(plan->d_dgen_items);
-  cudaFree(plan->d_dgen_idx);
   cudaFree(plan->d_dgen_coef);
   delete plan;
   return YASF_OK;

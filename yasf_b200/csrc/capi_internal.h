@@ -35,7 +35,6 @@ struct yasf_plan {
   // float64 dense multi-column path (lmax <= 6): chunks of 32 entry/mirror items and their terms
   int4* d_dgen_chunks = nullptr;
   int2* d_dgen_items = nullptr;
-  int* d_dgen_idx = nullptr;
   double* d_dgen_coef = nullptr;
   int dgen_chunks = 0;
 };
@@ -86,6 +85,6 @@ int validate_coupling(const yasf_plan* plan, int n_particles, const double* posi
 int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::vector<unsigned>& goff,
                       std::vector<unsigned>& dst);
 int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std::vector<int2>& items,
-                       std::vector<int>& term_idx, std::vector<double>& term_coef);
+                       std::vector<double>& term_coef);
 
 }  // namespace yasf

@@ -64,8 +64,8 @@ struct DpArgs {
   const double2* xp;         // source tiles [tile][source][X_STAGE bytes]
   int n_chunks;              // chunks of 32 items
   const int4* chunks;        // Wa slots, Wb slots, first term slot, 0
-  const int2* items;         // [32 * n_chunks]: entry | mirror packed (-1: none), delta + 2L
-  const int* term_idx;       // [slot][lane] A-table index p*P + |delta| of chunk terms
+  const int2* items;         // [32 * n_chunks]: entry | mirror packed (-1: none),
+                             // delta + 2L | Wa table base << 8 | Wb table base << 18
   const double* term_coef;   // [slot][lane] Wa: real coefficient; Wb: coefficient / i; 0 padding
   const double2* x;          // input columns (master epilogue)
   const double2* tmat;       // T, master epilogue when non-null
@@ -150,6 +150,9 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
   const int n_iter = N - 1;
 
   for (int o = tid; o < G::W_BYTES / 16; o += blockDim.x) W[o] = make_double2(0.0, 0.0);
+  // pair-table entries p < d are never written: zero, as the term windows may read them
+  for (int o = tid; o < 2 * G::T_ENTRIES; o += blockDim.x)
+    reinterpret_cast<double2*>(ts)[o] = make_double2(0.0, 0.0);
   if (tid == 0) {
     for (int b = 0; b < 2; ++b) {
       mbar_init(&xfull[b], 1);
@@ -187,8 +190,10 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
       for (int cc = warp; cc < a.n_chunks; cc += NW) {
         const int4 cm = __ldg(a.chunks + cc);
         const int2 m = __ldg(a.items + 32 * cc + lane);
-        const int* ti = a.term_idx + (size_t)cm.z * 32 + lane;
         const double* tc = a.term_coef + (size_t)cm.z * 32 + lane;
+        // slot q of the Wa (Wb) terms is A[p0 + 2q][|delta|]: table entry base + 2 P q
+        const double2* Ta = T + ((m.y >> 8) & 1023);
+        const double2* Tb = T + ((m.y >> 18) & 1023);
         double2 sa = make_double2(0.0, 0.0), sb = make_double2(0.0, 0.0);
         // at most lmax + 1 Wa and lmax Wb terms per entry: fully unrolled, predicated, so that all
         // coefficient loads of the chunk are in flight together
@@ -196,23 +201,23 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
         for (int q = 0; q < L + 1; ++q) {
           if (q < cm.x) {
             const double cf = __ldg(tc + q * 32);
-            const double2 g = T[__ldg(ti + q * 32)];
+            const double2 g = Ta[2 * P * q];
             sa.x = fma(cf, g.x, sa.x);
             sa.y = fma(cf, g.y, sa.y);
           }
         }
 #pragma unroll
-        for (int q = 0; q < L + 1; ++q) {
+        for (int q = 0; q < L; ++q) {
           if (q < cm.y) {
             const double cf = __ldg(tc + (cm.x + q) * 32);
-            const double2 g = T[__ldg(ti + (cm.x + q) * 32)];
+            const double2 g = Tb[2 * P * q];
             sb.x = fma(cf, g.x, sb.x);
             sb.y = fma(cf, g.y, sb.y);
           }
         }
         if (m.x == -1) continue;
         const int q1 = m.x & 255, q2 = (m.x >> 8) & 255, mq1 = (m.x >> 16) & 255, mq2 = (m.x >> 24) & 255;
-        const double2 e = T[P * P + m.y];
+        const double2 e = T[P * P + (m.y & 255)];
         // entry: Wa = E Sa, Wb = i E Sb ; mirror: Wa' = conj(E) Sa, Wb' = -i conj(E) Sb
         const double2 ua = cmul(e, sa), vb = cmul(e, sb);
         W[q2 * HR + q1] = make_double2(ua.x - vb.y, ua.y + vb.x);            // P = Wa + Wb
@@ -380,14 +385,17 @@ __global__ void __launch_bounds__(256) dpanel_tiles_kernel(int n_particles, int 
 
 // Items (an entry and its mirror) of the float64 dense panel and their terms, from the plan's
 // a5/b5 table. Items run over q2 then q1, so the 32 items of a chunk (one warp) store to
-// consecutive entries of a row (no bank conflicts); the chunk's terms are laid out slot-major
-// ([slot][lane], coalesced loads) and padded with zero terms to the chunk's largest Wa and Wb
-// counts, so a warp's term loops have uniform bounds.
+// consecutive entries of a row (no bank conflicts); the chunk's coefficients are laid out
+// slot-major ([slot][lane], coalesced loads). The Wa (Wb) terms of an item sit at orders
+// p = p0, p0 + 2, ... of one table column |delta|, so slot q holds the coefficient of
+// p = p0 + 2q (zero where the item has no term) and the kernel reads table entry
+// p0 P + |delta| + 2 P q: no index loads. The chunk's slot counts are its items' largest spans;
+// each item's p0 is its first term, moved down by 2 until the window ends at row 2L + 1 at most
+// (row 2L + 1 is the phase row; rows p < |delta| hold zeros).
 int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std::vector<int2>& items,
-                       std::vector<int>& term_idx, std::vector<double>& term_coef) {
+                       std::vector<double>& term_coef) {
   chunks.clear();
   items.clear();
-  term_idx.clear();
   term_coef.clear();
   if (L < 1 || L > 6) return YASF_OK;
   const int nmax = 2 * L * (L + 2), P = 2 * L + 1, H = L * (L + 2);
@@ -401,7 +409,7 @@ int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std:
     lm(q, l, m);
     return l * l + l - 1 - m;
   };
-  struct Item { int packed, delta; std::vector<int> ia, ib; std::vector<double> ca, cb; };
+  struct Item { int packed, delta, ad; std::vector<int> pa, pb; std::vector<double> ca, cb; };
   std::vector<Item> list;
   std::vector<char> seen((size_t)H * H, 0);
   for (int q2 = 0; q2 < H; ++q2)
@@ -416,6 +424,7 @@ int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std:
       Item it;
       it.packed = q1 | (q2 << 8) | (mq1 << 16) | (mq2 << 24);
       it.delta = delta + 2 * L;
+      it.ad = ad;
       for (int which = 0; which < 2; ++which)
         for (int p = 0; p < P; ++p) {
           const size_t idx = ((size_t)(which * H + q2) * nmax + q1) * P + p;
@@ -427,11 +436,12 @@ int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std:
           if (std::fabs(mr - sgn * cr) > tol || std::fabs(mi - sgn * ci) > tol) return YASF_ERR_INVALID_ARGUMENT;
           if (cr == 0.0 && ci == 0.0) continue;
           if ((which == 0 && ci != 0.0) || (which == 1 && cr != 0.0) || p < ad) return YASF_ERR_INVALID_ARGUMENT;
-          (which == 0 ? it.ia : it.ib).push_back(p * P + ad);
+          (which == 0 ? it.pa : it.pb).push_back(p);
           (which == 0 ? it.ca : it.cb).push_back(which == 0 ? cr : ci);
         }
       list.push_back(std::move(it));
     }
+  auto span = [](const std::vector<int>& ps) { return ps.empty() ? 0 : (ps.back() - ps.front()) / 2 + 1; };
   const int n_chunks = ((int)list.size() + 31) / 32;
   int slot = 0;
   for (int c = 0; c < n_chunks; ++c) {
@@ -439,12 +449,12 @@ int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std:
     for (int l = 0; l < 32; ++l) {
       const size_t k = (size_t)c * 32 + l;
       if (k < list.size()) {
-        na = std::max(na, (int)list[k].ia.size());
-        nb = std::max(nb, (int)list[k].ib.size());
+        na = std::max(na, span(list[k].pa));
+        nb = std::max(nb, span(list[k].pb));
       }
     }
+    if (na > L + 1 || nb > L) return YASF_ERR_INVALID_ARGUMENT;
     chunks.push_back(make_int4(na, nb, slot, 0));
-    term_idx.resize((size_t)(slot + na + nb) * 32, 0);
     term_coef.resize((size_t)(slot + na + nb) * 32, 0.0);
     for (int l = 0; l < 32; ++l) {
       const size_t k = (size_t)c * 32 + l;
@@ -453,15 +463,22 @@ int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std:
         continue;
       }
       const Item& it = list[k];
-      items.push_back(make_int2(it.packed, it.delta));
-      for (size_t q = 0; q < it.ia.size(); ++q) {
-        term_idx[(size_t)(slot + q) * 32 + l] = it.ia[q];
-        term_coef[(size_t)(slot + q) * 32 + l] = it.ca[q];
+      int base[2];
+      for (int which = 0; which < 2; ++which) {
+        const std::vector<int>& ps = which == 0 ? it.pa : it.pb;
+        const std::vector<double>& cs = which == 0 ? it.ca : it.cb;
+        const int n = which == 0 ? na : nb, s0 = which == 0 ? slot : slot + na;
+        int p0 = ps.empty() ? 0 : ps.front();
+        while (p0 > 1 && p0 + 2 * (n - 1) > 2 * L + 1) p0 -= 2;
+        if (p0 + 2 * (n - 1) > 2 * L + 1) return YASF_ERR_INVALID_ARGUMENT;
+        for (size_t q = 0; q < ps.size(); ++q) {
+          const int j = (ps[q] - p0) / 2;
+          if ((ps[q] - p0) % 2 != 0 || j < 0 || j >= n) return YASF_ERR_INVALID_ARGUMENT;
+          term_coef[(size_t)(s0 + j) * 32 + l] = cs[q];
+        }
+        base[which] = p0 * P + it.ad;
       }
-      for (size_t q = 0; q < it.ib.size(); ++q) {
-        term_idx[(size_t)(slot + na + q) * 32 + l] = it.ib[q];
-        term_coef[(size_t)(slot + na + q) * 32 + l] = it.cb[q];
-      }
+      items.push_back(make_int2(it.packed, it.delta | (base[0] << 8) | (base[1] << 18)));
     }
     slot += na + nb;
   }
@@ -550,7 +567,6 @@ extern "C" int yasf_dpanel_matvec(const yasf_plan* plan, int n_particles, const 
   da.leg = plan->d_leg;
   da.xp = reinterpret_cast<const double2*>(ws);
   da.items = plan->d_dgen_items;
-  da.term_idx = plan->d_dgen_idx;
   da.term_coef = plan->d_dgen_coef;
   da.x = reinterpret_cast<const double2*>(x);
   da.tmat = reinterpret_cast<const double2*>(tmat);
