@@ -28,7 +28,7 @@ def _setup(lmax, n, seed, device):
 
 
 @pytest.mark.parametrize("lmax,n,R", [(1, 6, 3), (2, 9, 1), (3, 17, 33), (4, 30, 64), (5, 12, 7), (6, 25, 40),
-                                      (6, 21, 130), (3, 10, 64), (2, 7, 65)])
+                                      (6, 21, 130), (3, 10, 64), (2, 7, 65), (1, 5, 64), (5, 14, 70)])
 def test_dpanel_matches_float64_coupling(cuda_device, lmax, n, R):
     dev, rng = _setup(lmax, n, 300 + lmax, cuda_device)
     X = torch.from_numpy(rng.normal(size=(R, dev.n)) + 1j * rng.normal(size=(R, dev.n))).to(cuda_device)

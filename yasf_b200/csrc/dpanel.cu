@@ -12,8 +12,9 @@
 // phases e^{+-i (m2 - m1) phi}, so both come from one set of loads.
 //
 // Block = (receiving sphere i, tile of 32 or 64 columns). Worker warps generate P and Q of W_ij
-// into shared memory, then apply them: per 32 columns, 4 warps form U = P S and 4 warps V = Q D,
-// each warp RPW receiving rows times 32 columns (one column per lane, W entries broadcast). A
+// into shared memory, then apply them: half the warps form U = P S and half V = Q D, each warp
+// RPW receiving rows times the tile's columns (one column per lane and 32 columns, W entries
+// broadcast: 4 row groups of H/4 rows at 32 columns, 8 row groups of H/8 rows at 64). A
 // helper warp runs ahead: it computes the float64 pair table (A[p][d] = Pn_p^d(cos theta)
 // h_p(k r), e^{i delta phi}; two stages) and copies the source tile [S; D] (cp.async.bulk; two
 // stages at 32 columns, one at 64). All waits
@@ -33,9 +34,11 @@ template <int L, int CT>
 struct DpGeom {
   static constexpr int H = L * (L + 2);
   static constexpr int P = 2 * L + 1;
-  static constexpr int RPW = (H + 3) / 4;            // receiving rows per worker warp
-  static constexpr int HR = 4 * RPW;                 // padded row count
-  static constexpr int WORKERS = 8 * (CT / 32);      // worker warps: (column half, block, row group)
+  static constexpr int CPT = CT / 32;                // columns per thread
+  static constexpr int RG = 4 * CPT;                 // row groups per block (U or V)
+  static constexpr int RPW = (H + RG - 1) / RG;      // receiving rows per worker warp
+  static constexpr int HR = RG * RPW;                // padded row count
+  static constexpr int WORKERS = 2 * RG;             // worker warps: (block, row group)
   static constexpr int THREADS = 32 * (WORKERS + 1); // + helper warp
   static constexpr int XS = CT == 32 ? 2 : 1;        // source-tile stages
   static constexpr int W_BYTES = 2 * H * HR * 16;    // P, Q as [blk][q2][q1] complex float64
@@ -49,7 +52,7 @@ struct DpGeom {
   static constexpr int SMEM = BAR_OFF + 128;
   static_assert(SMEM <= 232448, "dpanel shared memory exceeds the per-block limit");
   static_assert(W_BYTES % 16 == 0 && X_STAGE % 16 == 0 && T_STAGE % 16 == 0, "alignment");
-  static_assert(HR * CT * 16 <= XS * X_STAGE, "exchange buffer does not fit");
+  static_assert(H * CT * 16 <= XS * X_STAGE, "exchange buffer does not fit");
 };
 
 struct DpArgs {
@@ -130,6 +133,7 @@ template <int L, int CT>
 __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArgs a) {
   using G = DpGeom<L, CT>;
   constexpr int H = G::H, P = G::P, RPW = G::RPW, HR = G::HR, NW = G::WORKERS, XS = G::XS;
+  constexpr int CPT = G::CPT, NA = RPW * CPT;  // accumulators (row r, column lane + 32 k) at r CPT + k
   constexpr int NWT = 32 * NW;  // worker threads
   extern __shared__ __align__(128) unsigned char dp_smem[];
   double2* W = reinterpret_cast<double2*>(dp_smem + G::W_OFF);    // [2][H][HR]
@@ -168,17 +172,15 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
 
   if (warp < NW) {
     // ===================== generation + dense application =====================
-    const int ch = warp >> 3;                  // column half (64-column tiles)
-    const int blk = (warp >> 2) & 1;           // 0: U = P S, 1: V = Q D
-    const int r0 = (warp & 3) * RPW;
-    const int c = ch * 32 + lane;              // column within the tile
+    const int blk = warp / G::RG;              // 0: U = P S, 1: V = Q D
+    const int r0 = (warp % G::RG) * RPW;
     // 32-column tiles: complex accumulators as two independent partial sums each (re: w.x x.x |
     // -w.y x.y, im: w.x x.y | w.y x.x), so consecutive FMAs of a row do not wait on each other
-    double2 acc[RPW], acc2[CT == 32 ? RPW : 1];
+    double2 acc[NA], acc2[CT == 32 ? NA : 1];
 #pragma unroll
-    for (int r = 0; r < RPW; ++r) acc[r] = make_double2(0.0, 0.0);
+    for (int r = 0; r < NA; ++r) acc[r] = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int r = 0; r < (CT == 32 ? RPW : 1); ++r) acc2[r] = make_double2(0.0, 0.0);
+    for (int r = 0; r < (CT == 32 ? NA : 1); ++r) acc2[r] = make_double2(0.0, 0.0);
     // One thread waits (bounded) and publishes the outcome across a workers' barrier, so every
     // worker warp takes the same branch and no warp is left waiting at a barrier.
     for (int t = 0; t < n_iter; ++t) {
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
       named_sync(1, NWT);  // W complete, source tile decision published
       if (tid == 0) mbar_arrive(&tfree[st]);
       if (!go[1]) break;
-      const double2* X = reinterpret_cast<const double2*>(xs + sx * G::X_STAGE) + blk * H * CT + c;
+      const double2* X = reinterpret_cast<const double2*>(xs + sx * G::X_STAGE) + blk * H * CT + lane;
       const double2* Wb = W + blk * H * HR + r0;
       if constexpr (CT == 32) {
 #pragma unroll 2
@@ -246,22 +248,31 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
           }
         }
       } else {
-        // fewer registers per thread at 544 threads: one accumulator per row, the two FMAs of
-        // each component issued in separate passes over the rows (RPW instructions apart)
+        // 64 columns, 96 registers per thread: each W entry serves two columns (8 shared loads
+        // per 48 FMAs); one accumulator per row and column, the two FMAs of each component issued
+        // in separate passes (2 RPW instructions apart)
 #pragma unroll 1
         for (int q2 = 0; q2 < H; ++q2) {
-          const double2 xv = X[q2 * CT];
+          double2 xv[CPT];
+#pragma unroll
+          for (int k = 0; k < CPT; ++k) xv[k] = X[q2 * CT + 32 * k];
 #pragma unroll
           for (int r = 0; r < RPW; ++r) {
             const double wx = Wb[q2 * HR + r].x;
-            acc[r].x = fma(wx, xv.x, acc[r].x);
-            acc[r].y = fma(wx, xv.y, acc[r].y);
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+              acc[r * CPT + k].x = fma(wx, xv[k].x, acc[r * CPT + k].x);
+              acc[r * CPT + k].y = fma(wx, xv[k].y, acc[r * CPT + k].y);
+            }
           }
 #pragma unroll
           for (int r = 0; r < RPW; ++r) {
             const double wy = Wb[q2 * HR + r].y;
-            acc[r].x = fma(-wy, xv.y, acc[r].x);
-            acc[r].y = fma(wy, xv.x, acc[r].y);
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+              acc[r * CPT + k].x = fma(-wy, xv[k].y, acc[r * CPT + k].x);
+              acc[r * CPT + k].y = fma(wy, xv[k].x, acc[r * CPT + k].y);
+            }
           }
         }
       }
@@ -270,7 +281,7 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
     }
     if constexpr (CT == 32) {
 #pragma unroll
-      for (int r = 0; r < RPW; ++r) acc[r] = make_double2(acc[r].x + acc2[r].x, acc[r].y + acc2[r].y);
+      for (int r = 0; r < NA; ++r) acc[r] = make_double2(acc[r].x + acc2[r].x, acc[r].y + acc2[r].y);
     }
     // park V in shared memory after every role has finished (below), then combine
     __syncthreads();
@@ -278,37 +289,44 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
       for (int b = 0; b < XS; ++b)
         if (issued[b] >= 0) (void)panel_wait(&xfull[b], (unsigned)((issued[b] / XS) & 1));
     named_sync(1, NWT);
-    double2* xch = reinterpret_cast<double2*>(xs);  // [HR][CT] V
+    double2* xch = reinterpret_cast<double2*>(xs);  // [H][CT] V
     if (blk == 1) {
 #pragma unroll
-      for (int r = 0; r < RPW; ++r) xch[(r0 + r) * CT + c] = acc[r];
+      for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k)
+          if (r0 + r < H) xch[(r0 + r) * CT + 32 * k + lane] = acc[r * CPT + k];
     }
     named_sync(1, NWT);
     const bool aborted = *abort_flag != 0;
     if (aborted && tid == 0) atomicExch(a.err, 1);
-    const int col = tile * CT + c;
-    if (blk == 0 && col < a.nrhs) {
 #pragma unroll
-      for (int r = 0; r < RPW; ++r) {
-        const int q = r0 + r;
-        if (q >= H) break;
-        const double2 v = xch[q * CT + c];
-        double y1r = 0.5 * (acc[r].x + v.x), y1i = 0.5 * (acc[r].y + v.y);
-        double y2r = 0.5 * (acc[r].x - v.x), y2i = 0.5 * (acc[r].y - v.y);
-        if (aborted) y1r = y1i = y2r = y2i = __longlong_as_double(0x7ff8000000000000LL);
+    for (int k = 0; k < CPT; ++k) {
+      const int c = 32 * k + lane, col = tile * CT + c;
+      if (blk == 0 && col < a.nrhs) {
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          const int nn = half * H + q;
-          const double yr = half ? y2r : y1r, yi = half ? y2i : y1i;
-          double2 out;
-          if (a.tmat) {
-            const double2 tv = a.tmat[(size_t)i * a.nmax + nn];
-            const double2 xv = a.x[(size_t)col * a.ld + (size_t)i * a.nmax + nn];
-            out = make_double2(xv.x - (tv.x * yr - tv.y * yi), xv.y - (tv.x * yi + tv.y * yr));
-          } else {
-            out = make_double2(yr, yi);
+        for (int r = 0; r < RPW; ++r) {
+          const int q = r0 + r;
+          if (q >= H) break;
+          const double2 v = xch[q * CT + c];
+          const double2 u = acc[r * CPT + k];
+          double y1r = 0.5 * (u.x + v.x), y1i = 0.5 * (u.y + v.y);
+          double y2r = 0.5 * (u.x - v.x), y2i = 0.5 * (u.y - v.y);
+          if (aborted) y1r = y1i = y2r = y2i = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+          for (int half = 0; half < 2; ++half) {
+            const int nn = half * H + q;
+            const double yr = half ? y2r : y1r, yi = half ? y2i : y1i;
+            double2 out;
+            if (a.tmat) {
+              const double2 tv = a.tmat[(size_t)i * a.nmax + nn];
+              const double2 xv = a.x[(size_t)col * a.ld + (size_t)i * a.nmax + nn];
+              out = make_double2(xv.x - (tv.x * yr - tv.y * yi), xv.y - (tv.x * yi + tv.y * yr));
+            } else {
+              out = make_double2(yr, yi);
+            }
+            a.y[(size_t)col * a.ldy + (size_t)i * a.nmax + nn] = out;
           }
-          a.y[(size_t)col * a.ldy + (size_t)i * a.nmax + nn] = out;
         }
       }
     }
