@@ -5,10 +5,12 @@
 - arithmetic: emulating the kernel's generation in float64 from the schedule (items of an entry
   and its mirror, the A[p][|d|] table, phases e^{i d phi}, P = Wa + Wb, Q = Wa - Wb) and its
   tau-symmetric product (S = X1 + X2, D = X1 - X2, Y1 = (U + V) / 2, Y2 = (U - V) / 2) reproduces
-  the oracle's two-sphere coupling W_ij x_j to rounding; for lmax 7 and 8 the emulation reads the
-  pair table the way the packed kernel variant does (slot q of a step at row p0 + 2q of the lane's
-  term window, zero coefficients outside the item's terms) and checks every read stays inside the
-  written, finite part of the table.
+  the oracle's two-sphere coupling W_ij x_j to rounding. The emulation reads the pair table the
+  way the kernel does: up to lmax 6 slot by slot from the schedule's slot table, for lmax 7 and 8
+  slot q of a step at row p0 + 2q of the lane's term window (zero coefficients outside the item's
+  terms); every read stays inside the written, finite part of the table,
+- slot tables: a half-warp's loads of one slot are bank-conflict-free, and lanes that recompute
+  one item add its terms in the same order.
 """
 
 from __future__ import annotations
@@ -17,7 +19,7 @@ import numpy as np
 import pytest
 
 from oracle import restate as R
-from yasf_b200.panel_sched import WARPS, _lm, mirror, schedule, window_starts
+from yasf_b200.panel_sched import PAD, WARPS, _lm, _wavefronts, mirror, schedule, slot_tables, window_starts
 from yasf_b200.wigner import translation_table_ab5
 
 
@@ -59,6 +61,8 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj, packed=False):
     g[P * P:] = np.exp(1j * np.arange(-2 * L, 2 * L + 1) * phi)
     steps, sched = schedule(L)
     win = window_starts(L, steps, sched)
+    slots = None if packed else slot_tables(L, steps, sched)
+    bases = np.cumsum([0] + [a + b for a, b in steps])
     Pm = np.full((H, H), np.nan, dtype=complex)
     Qm = np.full((H, H), np.nan, dtype=complex)
     tab = np.asarray(table_ab5)
@@ -85,11 +89,25 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj, packed=False):
                             else:
                                 Sb += (tab[H + q2, q1, p].imag if real else 0.0) * g[idx]
                 else:
-                    for p in range(pmin, l1 + l2 + 1):
-                        if (l1 + l2 + p) % 2 == 0:
-                            Sa += tab[q2, q1, p].real * A[p, abs(dl)]
+                    # the kernel's reads: slot by slot from the schedule's slot table
+                    lane = sched[w][kk].index((q1, q2))
+                    seen = []
+                    for s in range(bases[kk], bases[kk + 1]):
+                        v = slots[w][lane][s]
+                        idx = v & 0xFF
+                        assert 0 <= idx < g.size and np.isfinite(g[idx])
+                        if v & PAD:
+                            continue
+                        p, dd = divmod(idx, P)
+                        assert dd == abs(dl) and pmin <= p <= l1 + l2
+                        wa = (l1 + l2 + p) % 2 == 0
+                        assert (s < bases[kk] + steps[kk][0]) == wa  # Wa terms in the Wa slots
+                        seen.append(p)
+                        if wa:
+                            Sa += tab[q2, q1, p].real * g[idx]
                         else:
-                            Sb += tab[H + q2, q1, p].imag * A[p, abs(dl)]
+                            Sb += tab[H + q2, q1, p].imag * g[idx]
+                    assert sorted(seen) == list(range(pmin, l1 + l2 + 1))
                 E = np.exp(1j * dl * phi)
                 Wa, Wb = E * Sa, 1j * E * Sb
                 Pm[q1, q2], Qm[q1, q2] = Wa + Wb, Wa - Wb
@@ -113,3 +131,22 @@ def test_generation_algebra_matches_oracle(L, packed):
     ref = R.coupling_matvec_rows(L, pos, k, tab, x, 0, 1)
     got = _emulate_wx(L, tab, pos[0], pos[1], k, x[nmax:], packed=packed)
     assert np.max(np.abs(got - ref)) <= 1e-11 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("L", [4, 5, 6])
+def test_slot_tables_are_conflict_free(L):
+    """A half-warp's 8-byte pair-table loads of one slot hit different banks (or one address), and
+    lanes that recompute one item add its terms in one order (identical stores)."""
+    steps, sched = schedule(L)
+    st = slot_tables(L, steps, sched)
+    S = sum(a + b for a, b in steps)
+    extra = sum(_wavefronts([st[w][l][q] & 0xFF for l in range(16 * h, 16 * h + 16)]) - 1
+                for w in range(WARPS) for h in range(2) for q in range(S))
+    assert extra <= 0.02 * 2 * WARPS * S
+    bases = np.cumsum([0] + [a + b for a, b in steps])
+    order = {}
+    for k in range(len(steps)):
+        for w in range(WARPS):
+            for lane, e in enumerate(sched[w][k]):
+                seq = tuple(v for v in st[w][lane][bases[k]:bases[k + 1]] if not v & PAD)
+                assert order.setdefault(e, seq) == seq

@@ -30,7 +30,9 @@ static unsigned short half_bits(float f) {
 // Generation data of the panel kernel from the build-time schedule (panel_sched.h). For every
 // generator thread and slot: the real coefficient and the byte offset of A[p][|d|] of one term of
 // the thread's item; for every step: the W-stage byte offsets of the P_r rows of the item's entry
-// and of its mirror, and the byte offset of the entry's phase e^{i d phi}. Packed variant
+// and of its mirror, and the byte offset of the entry's phase e^{i d phi}. Up to lmax 6 the slot
+// of each term, and the entry a slot without a term reads (zero coefficient), come from the
+// schedule's slot table (kPanelSlot: a half-warp's loads of one slot hit different banks). Packed variant
 // (lmax 7-8): goff holds the FP16 coefficients two per word and the third dst row the step's
 // pair-table bases (Wa | Wb << 10 | phase << 20, entry units); slot q of a step's Wa (Wb) terms is
 // the term at p = p0 + 2q, with the window starts p0 from the schedule (kPanelWindow; they keep
@@ -41,7 +43,8 @@ static unsigned short half_bits(float f) {
 // (Wb), which the kernel applies. Terms below 1e-12 of the largest coefficient cannot change a
 // TF32 entry and are dropped.
 template <int L>
-static int build_terms_for(const double* ab5, const unsigned short* entry, const unsigned short* window,
+static int build_terms_for(const double* ab5, const unsigned short* entry, const unsigned short* slots,
+                           const unsigned short* window,
                            const unsigned char* wa, const unsigned char* wb, std::vector<float>& coef,
                            std::vector<unsigned>& goff, std::vector<unsigned>& dst) {
   using Sched = PanelSched<L>;
@@ -97,6 +100,8 @@ static int build_terms_for(const double* ab5, const unsigned short* entry, const
   dst.assign((size_t)3 * NS * kGenThreads, 0u);
   for (int th = 0; th < kGenThreads; ++th) {
     const int w = th >> 5, lane = th & 31;
+    if constexpr (!PK)  // every slot reads its schedule entry; slots without a term keep coefficient 0
+      for (int q = 0; q < S; ++q) goff[(size_t)q * kGenThreads + th] = (slots[(size_t)th * S + q] & 0xFFu) * 8u;
     int base = 0;
     for (int k = 0; k < NS; ++k) {
       const unsigned e = entry[((size_t)w * NS + k) * 32 + lane];
@@ -127,19 +132,21 @@ static int build_terms_for(const double* ab5, const unsigned short* entry, const
           const int which = ((l1 + l2 + p) % 2 == 0) ? 0 : 1;
           double cr, ci;
           coefficient(which, q1, q2, p, cr, ci);
-          const int j = PK ? (p - p0[which]) / 2 : (which == 0 ? na : nb);
+          const int T = which == 0 ? wa[k] : wb[k], off = which == 0 ? base : base + wa[k];
+          int j = -1;
+          if constexpr (PK) {
+            j = (p - p0[which]) % 2 == 0 ? (p - p0[which]) / 2 : -1;
+          } else {
+            // the schedule's slot of this term (entries flagged 0x100 carry no term)
+            for (int q = 0; q < T; ++q)
+              if (slots[(size_t)th * S + off + q] == (unsigned)(p * P + ad)) j = q;
+          }
           which == 0 ? ++na : ++nb;
-          if (na > wa[k] || nb > wb[k] || j < 0 || j >= (which == 0 ? wa[k] : wb[k]) ||
-              (PK && (p - p0[which]) % 2 != 0))
-            return YASF_ERR_INVALID_ARGUMENT;
+          if (na > wa[k] || nb > wb[k] || j < 0 || j >= T) return YASF_ERR_INVALID_ARGUMENT;
           const int slot = which == 0 ? base + j : base + wa[k] + j;
           const float cf = (float)(which == 0 ? cr : ci);
           coef[(size_t)slot * kGenThreads + th] = cf;
-          if constexpr (PK) {
-            goff[(size_t)(slot >> 1) * kGenThreads + th] |= (unsigned)half_bits(cf) << (16 * (slot & 1));
-          } else {
-            goff[(size_t)slot * kGenThreads + th] = (unsigned)(p * P + ad) * 8;
-          }
+          if constexpr (PK) goff[(size_t)(slot >> 1) * kGenThreads + th] |= (unsigned)half_bits(cf) << (16 * (slot & 1));
         }
       }
       base += wa[k] + wb[k];
@@ -156,8 +163,8 @@ int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::v
   dst.clear();
 #define YASF_TERMS(n)                                                                             \
   case n:                                                                                         \
-    return build_terms_for<n>(ab5, kPanelEntry##n, kPanelWindow##n, kPanelStepWa##n, kPanelStepWb##n, \
-                              coef, goff, dst);
+    return build_terms_for<n>(ab5, kPanelEntry##n, kPanelSlot##n, kPanelWindow##n, kPanelStepWa##n,   \
+                              kPanelStepWb##n, coef, goff, dst);
   switch (L) {
     YASF_TERMS(1)
     YASF_TERMS(2)

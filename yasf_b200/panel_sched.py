@@ -27,11 +27,13 @@ Lanes without an item of their class in a step write zeros to a padding entry (r
 beyond the lmax(lmax+2) modes) of that class, or recompute an item that another lane also
 computes (same values, same addresses). The output header holds, per lmax, the step table as a
 macro list, the (warp, step, lane) -> primary entry table used by the plan to lay out
-coefficients, and the term windows of the packed variant (``window_starts``).
+coefficients, the term windows of the packed variant (``window_starts``) and, up to lmax 6, the
+pair-table entry each thread reads in each slot (``slot_tables``).
 """
 
 from __future__ import annotations
 
+import random
 from collections import defaultdict
 from pathlib import Path
 
@@ -184,6 +186,118 @@ def window_starts(L: int, steps, table):
               for (q1, q2) in table[w][k]] for k in range(len(steps))] for w in range(WARPS)]
 
 
+def _terms(L: int, q1: int, q2: int):
+    """Pair-table entries (p P + |d|) of the Wa and Wb terms of entry (q1, q2), in order of p."""
+    H, P = L * (L + 2), 2 * L + 1
+    if q1 >= H or q2 >= H:
+        return [], []
+    l1, m1 = _lm(q1)
+    l2, m2 = _lm(q2)
+    ad = abs(m2 - m1)
+    ps = range(max(abs(l1 - l2), ad), l1 + l2 + 1)
+    return ([p * P + ad for p in ps if (l1 + l2 + p) % 2 == 0],
+            [p * P + ad for p in ps if (l1 + l2 + p) % 2 == 1])
+
+
+def _wavefronts(addrs) -> int:
+    """Shared-memory wavefronts of one half-warp's 8-byte loads (16 banks of 8 bytes)."""
+    by_bank = {}
+    for a in addrs:
+        by_bank.setdefault(a % 16, set()).add(a)
+    return max((len(v) for v in by_bank.values()), default=1)
+
+
+def _place_half(lists, fixed, T, rng, tries):
+    """Slots of one half-warp's terms for one part (Wa or Wb) of one step.
+
+    lists[i]: the lane's terms; fixed[i]: True if their order is already fixed (the lane recomputes
+    an item placed before: the terms keep that order, so both lanes add them in the same order and
+    store the same values). A free lane may put its terms in any slots. Returns (wavefronts,
+    rows) with rows[i][s] the entry read by lane i in slot s (None: zero coefficient)."""
+    n = len(lists)
+    best = None
+    for _ in range(tries):
+        rows = [[None] * T for _ in range(n)]
+        order = sorted(range(n), key=lambda i: (not fixed[i], -len(lists[i]), rng.random()))
+
+        def clash(s, t):
+            return sum(1 for a in {rows[o][s] for o in range(n)} - {None, t} if a % 16 == t % 16)
+
+        for i in order:
+            ts = lists[i]
+            if fixed[i]:
+                # monotone placement of the fixed order: slots s_0 < s_1 < ... (small DP)
+                m = len(ts)
+                INF = 1 << 30
+                cost = [[INF] * (T + 1) for _ in range(m + 1)]
+                cost[0] = [0] * (T + 1)
+                for j in range(1, m + 1):
+                    for s in range(j, T + 1):
+                        cost[j][s] = min(cost[j][s - 1], cost[j - 1][s - 1] + clash(s - 1, ts[j - 1]))
+                s = T
+                for j in range(m, 0, -1):
+                    while cost[j][s] == cost[j][s - 1] and s - 1 >= j:
+                        s -= 1
+                    rows[i][s - 1] = ts[j - 1]
+                    s -= 1
+            else:
+                free = list(range(T))
+                for t in sorted(ts, key=lambda _: rng.random()):
+                    sl = min(free, key=lambda s: (clash(s, t), rng.random()))
+                    rows[i][sl] = t
+                    free.remove(sl)
+        total = sum(_wavefronts([r[s] for r in rows if r[s] is not None] or [0]) for s in range(T))
+        if best is None or total < best[0]:
+            best = (total, rows)
+    return best
+
+
+PAD = 0x100  # flag of a slot without a term of the lane (its entry is read with a zero coefficient)
+
+
+def slot_tables(L: int, steps, table, tries: int = 24):
+    """[warp][lane] -> the pair-table entry read in each of the S slots (lmax <= 6), | PAD on slots
+    without a term of the lane.
+
+    Up to lmax 6 every slot carries its own table offset, so a lane's terms may sit in any of the
+    step's slots. The slots are chosen per half-warp so that the 16 lanes' 8-byte loads of a slot
+    hit different banks (one wavefront); a slot without a term of the lane reads an entry another
+    lane of the half-warp reads in that slot (a broadcast, zero coefficient). Items that occur in
+    more than one lane (recomputed duplicates) keep the term order of their first placement.
+    Deterministic (seeded)."""
+    S = sum(a + b for a, b in steps)
+    out = [[[0] * S for _ in range(32)] for _ in range(WARPS)]
+    canon = {}
+    base = 0
+    for k, (ta, tb) in enumerate(steps):
+        for w in range(WARPS):
+            row = table[w][k]
+            for part, T, off in ((0, ta, base), (1, tb, base + ta)):
+                for h in range(2):
+                    lanes = list(range(16 * h, 16 * h + 16))
+                    keys = [(row[l], part) for l in lanes]
+                    lists = [list(canon.get(key, _terms(L, *row[l])[part])) for key, l in zip(keys, lanes)]
+                    fixed = [key in canon for key in keys]
+                    # a lane repeated inside this half-warp takes the first lane's placement
+                    first = {}
+                    for i, key in enumerate(keys):
+                        first.setdefault(key, i)
+                    uniq = [i for i, key in enumerate(keys) if first[key] == i]
+                    rng = random.Random(hash((L, k, w, part, h)) & 0xFFFFFFFF)
+                    _, rows = _place_half([lists[i] for i in uniq], [fixed[i] for i in uniq], T, rng, tries)
+                    placed = {keys[i]: rows[j] for j, i in enumerate(uniq)}
+                    for s in range(T):
+                        used = [r[s] for r in placed.values() if r[s] is not None]
+                        pad = max(set(used), key=used.count) if used else 0
+                        for i, l in enumerate(lanes):
+                            e = placed[keys[i]][s]
+                            out[w][l][off + s] = (pad | PAD) if e is None else e
+                    for key, r in placed.items():
+                        canon.setdefault(key, tuple(e for e in r if e is not None))
+        base += ta + tb
+    return out
+
+
 def header_text(lmax_values=range(1, 9)) -> str:
     out = [
         "// Generated by yasf_b200/panel_sched.py at build time: the W-generation schedule of the",
@@ -220,6 +334,17 @@ def header_text(lmax_values=range(1, 9)) -> str:
         for i in range(0, len(flat), 16):
             out.append("    " + ", ".join(str(v) for v in flat[i:i + 16]) + ",")
         out.append("};")
+        if L <= 6:
+            st = slot_tables(L, steps, table)
+            flat = [st[w][l][q] for w in range(WARPS) for l in range(32) for q in range(slots)]
+            out.append("// pair-table entry read per slot (lmax <= 6; | 0x100: no term, zero coefficient),")
+            out.append("// [warp][lane][slot]")
+            out.append(f"static const unsigned short kPanelSlot{L}[{len(flat)}] = {{")
+            for i in range(0, len(flat), 24):
+                out.append("    " + ", ".join(str(v) for v in flat[i:i + 24]) + ",")
+            out.append("};")
+        else:
+            out.append(f"static const unsigned short* const kPanelSlot{L} = nullptr;  // packed variant")
         win = window_starts(L, steps, table)
         flat = [a | (b << 8) for w in range(WARPS) for k in range(len(steps)) for (a, b) in win[w][k]]
         out.append("// term windows of the packed variant: p0 of Wa | p0 of Wb << 8, [warp][step][lane]")
