@@ -21,7 +21,7 @@
 // its mirror (l, -m) from one set of loads, and a warp's 32 stores of a step hit 32 different
 // banks; warps 0-3 also read the accumulators at the end. Warp 16 owns tensor memory and its
 // elected thread issues the MMAs. Warps 17 and 18 compute the pair tables of alternate pairs;
-// warp 19 issues the cp.async.bulk copies of the source panels. Three source-panel stages, two W
+// warp 19 issues the cp.async.bulk copies of the source panels. Two source-panel stages, three W
 // stages and four pair-table stages are in flight (lmax 7: two and one; lmax 8: one and one). Every wait is bounded in time: a timeout sets
 // the error word, every role stops, the result is written as NaN and tensor memory is freed.
 #pragma once
@@ -53,13 +53,17 @@ struct PanelGeom {
   static constexpr int A_LBO = (A_ROWS / 8) * 128;   // bytes between 4-column K chunks
   static constexpr int A_BYTES = A_ROWS * HP * 4;
   static constexpr int X_STAGE = 2 * A_BYTES;        // one source panel (S and D operands)
-  static constexpr int X_STAGES = L <= 6 ? 3 : (L == 7 ? 2 : 1);  // what shared memory allows
+  // source-panel stages: two up to lmax 7, one at lmax 8 (what shared memory allows)
+  static constexpr int X_STAGES = L <= 7 ? 2 : 1;
   // B operands [P_r; P_i], [Q_r; Q_i]: 2 HP rows x HP columns
   static constexpr int B_ROWS = 2 * HP;
   static constexpr int B_LBO = (B_ROWS / 8) * 128;
   static constexpr int B_BYTES = B_ROWS * HP * 4;
   static constexpr int W_STAGE = 2 * B_BYTES;
-  static constexpr int W_STAGES = L <= 6 ? 2 : 1;    // lmax 7-8: generation waits for the MMAs
+  // W stages: up to lmax 6 generation runs two pairs ahead of the MMAs (the per-pair hand-off
+  // latency, not a throughput, bounds the kernel: three stages measured 11 % faster than two with
+  // three source-panel stages); lmax 7-8: one, generation waits for the MMAs
+  static constexpr int W_STAGES = L <= 6 ? 3 : 1;
   // lmax 7-8 (40 / 62 generation slots per thread): coefficients are held as FP16 pairs and the
   // pair-table addresses of a step's terms are implicit (see gen_step_packed), so the generation
   // state fits the register budget; up to lmax 6 every slot holds an FP32 coefficient and a byte
@@ -385,13 +389,13 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   unsigned long long* xfull = bars;        // [XS] source panel landed
   unsigned long long* xempty = bars + 3;   // [XS] MMAs of the panel done
   unsigned long long* wfull = bars + 6;    // [WS] W generated (one arrival per generator warp)
-  unsigned long long* wempty = bars + 8;   // [WS] MMAs of the W stage done
-  unsigned long long* gfull = bars + 10;   // [4] pair table ready
-  unsigned long long* gempty = bars + 14;  // [4] pair table consumed (one arrival per generator warp)
-  unsigned long long* accum = bars + 18;   // accumulators final
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 19);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 20);
-  volatile int* issued = reinterpret_cast<volatile int*>(bars + 21);  // [XS] newest unit loaded per stage
+  unsigned long long* wempty = bars + 9;   // [WS] MMAs of the W stage done
+  unsigned long long* gfull = bars + 12;   // [4] pair table ready
+  unsigned long long* gempty = bars + 16;  // [4] pair table consumed (one arrival per generator warp)
+  unsigned long long* accum = bars + 20;   // accumulators final
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + 21);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 22);
+  volatile int* issued = reinterpret_cast<volatile int*>(bars + 23);  // [XS] newest unit loaded per stage
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -446,8 +450,8 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
   if (tid == 0) {
     for (int b = 0; b < 3; ++b) mbar_init(&xfull[b], 1);
     for (int b = 0; b < 3; ++b) mbar_init(&xempty[b], 1);
-    for (int b = 0; b < 2; ++b) mbar_init(&wfull[b], kGenWarps);
-    for (int b = 0; b < 2; ++b) mbar_init(&wempty[b], 1);
+    for (int b = 0; b < 3; ++b) mbar_init(&wfull[b], kGenWarps);
+    for (int b = 0; b < 3; ++b) mbar_init(&wempty[b], 1);
     for (int b = 0; b < 4; ++b) mbar_init(&gfull[b], 1);
     for (int b = 0; b < 4; ++b) mbar_init(&gempty[b], kGenWarps);
     mbar_init(accum, 1);
