@@ -119,7 +119,8 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj, packed=False):
     return np.concatenate([(U + V) / 2, (U - V) / 2])
 
 
-@pytest.mark.parametrize("L, packed", [(2, False), (4, False), (6, False), (7, True), (8, True)])
+@pytest.mark.parametrize("L, packed", [(1, False), (2, False), (3, False), (4, False), (5, False), (6, False),
+                                       (7, True), (8, True)])
 def test_generation_algebra_matches_oracle(L, packed):
     rng = np.random.default_rng(L)
     tab = translation_table_ab5(L)
@@ -150,3 +151,10 @@ def test_slot_tables_are_conflict_free(L):
             for lane, e in enumerate(sched[w][k]):
                 seq = tuple(v for v in st[w][lane][bases[k]:bases[k + 1]] if not v & PAD)
                 assert order.setdefault(e, seq) == seq
+
+
+def test_slot_tables_are_deterministic():
+    """The generated header (and with it the plan's coefficient layout) does not change between
+    builds: the slot search is seeded."""
+    steps, sched = schedule(5)
+    assert slot_tables(5, steps, sched) == slot_tables(5, steps, sched)

@@ -17,13 +17,15 @@
 //
 // Roles (640 threads): warps 0-15 generate P and Q of W_ij into shared memory (canonical K-major
 // no-swizzle layout, values rounded to TF32) following the build-time schedule of panel_sched.h:
-// every thread keeps its coefficients and pair-table offsets in registers, computes an entry and
-// its mirror (l, -m) from one set of loads, and a warp's 32 stores of a step hit 32 different
-// banks; warps 0-3 also read the accumulators at the end. Warp 16 owns tensor memory and its
-// elected thread issues the MMAs. Warps 17 and 18 compute the pair tables of alternate pairs;
-// warp 19 issues the cp.async.bulk copies of the source panels. Two source-panel stages, three W
-// stages and four pair-table stages are in flight (lmax 7: two and one; lmax 8: one and one). Every wait is bounded in time: a timeout sets
-// the error word, every role stops, the result is written as NaN and tensor memory is freed.
+// every thread keeps its coefficients and pair-table offsets in registers (lmax 7-8: FP16
+// coefficient pairs, offsets implicit), computes an entry and its mirror (l, -m) from one set of
+// loads, and a warp's 32 stores of a step hit 32 different banks (up to lmax 6 its pair-table
+// loads are bank-conflict-free as well); warps 0-3 also read the accumulators at the end. Warp 16
+// owns tensor memory and its elected thread issues the MMAs. Warps 17 and 18 compute the pair
+// tables of alternate pairs; warp 19 issues the cp.async.bulk copies of the source panels. Two
+// source-panel stages, three W stages and four pair-table stages are in flight (lmax 7: two and
+// one; lmax 8: one and one). Every wait is bounded in time: a timeout sets the error word, every
+// role stops, the result is written as NaN and tensor memory is freed.
 #pragma once
 
 #include <cuda_fp16.h>
