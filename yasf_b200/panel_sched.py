@@ -283,7 +283,7 @@ def slot_tables(L: int, steps, table, tries: int = 24):
                     for i, key in enumerate(keys):
                         first.setdefault(key, i)
                     uniq = [i for i, key in enumerate(keys) if first[key] == i]
-                    rng = random.Random(hash((L, k, w, part, h)) & 0xFFFFFFFF)
+                    rng = random.Random((((L * 64 + k) * WARPS + w) * 2 + part) * 2 + h)
                     _, rows = _place_half([lists[i] for i in uniq], [fixed[i] for i in uniq], T, rng, tries)
                     placed = {keys[i]: rows[j] for j, i in enumerate(uniq)}
                     for s in range(T):
