@@ -9,7 +9,8 @@ The reference imports with the stand-ins from ``oracle/stubs`` (pywigxjpf via sy
 refidxdb and pyperf as inert stand-ins). Two kinds of fixtures are written:
 
 - ``celes_*.npz``: the MATLAB/CELES golden vectors that the reference's own tests hold
-  (reference tests/data/*.mat, read by tests/test_comparison.py and tests/test_full_simulation.py),
+  (reference tests/data/*.mat, read by tests/test_comparison.py and tests/test_full_simulation.py,
+  and the 500-sphere CELES export tests/data/celes_*.fits, read by tests/test_celes.py),
   converted to particle-major numpy arrays.
 - ``ref_*.npz``: outputs of the reference code path on seeded synthetic inputs (coupling matvec,
   master operator, Mie / incident / right-hand side, GMRES solve, cross sections, and the
@@ -101,6 +102,58 @@ def celes_fixtures():
          initial=f["initial_field_coefficients"].astype(np.complex128),
          mie=f["mie_coefficients"].astype(np.complex128),
          scattered=f["scattered_field_coefficients"].astype(np.complex128))
+
+
+def read_fits(path: Path) -> list[tuple[dict, list[int], bytes]]:
+    """Minimal FITS reader (headers, including HIERARCH cards, and the raw big-endian data of each
+    HDU): enough for the reference's CELES export, read without astropy."""
+    raw = path.read_bytes()
+    pos, hdus = 0, []
+    while pos < len(raw):
+        cards, end = {}, False
+        while not end:
+            block = raw[pos:pos + 2880]
+            pos += 2880
+            for i in range(36):
+                c = block[i * 80:(i + 1) * 80].decode("ascii")
+                if c[:8].strip() == "END":
+                    end = True
+                    break
+                if c.startswith("HIERARCH"):
+                    key, _, val = c[9:].partition("=")
+                elif c[8:10] == "= ":
+                    key, val = c[:8], c[10:]
+                else:
+                    continue
+                val = val.strip()
+                val = val.split("'")[1] if val.startswith("'") else val.split("/")[0].strip()
+                cards[key.strip()] = val
+        naxis = int(cards.get("NAXIS", 0))
+        dims = [int(cards[f"NAXIS{i}"]) for i in range(1, naxis + 1)]
+        size = (abs(int(cards.get("BITPIX", 8))) // 8 * int(np.prod(dims)) + int(cards.get("PCOUNT", 0))) if naxis else 0
+        hdus.append((cards, dims, raw[pos:pos + size]))
+        pos += (size + 2879) // 2880 * 2880
+    return hdus
+
+
+def celes_fits_fixture():
+    """The 500-sphere CELES export the reference's tests/test_celes.py checks (HDU 1 particles,
+    HDU 3 incident field, HDU 4 wavelength and medium, HDU 6 solver, HDU 7 lmax, HDU 8 incident and
+    scattered coefficients as (4, N, nmax): re/im incident, re/im scattered)."""
+    hdus = read_fits(REF / "tests" / "data" / "celes_2023-05-09_21-00-48.fits")
+    part = np.frombuffer(hdus[1][2], dtype=">f8").reshape(-1, 6).astype(float)  # x y z r n k
+    inp = hdus[4][2]
+    wavelength = float(np.frombuffer(inp[0:8], dtype=">f8")[0])
+    medium = np.frombuffer(inp[8:24], dtype=">f8").astype(float)
+    c8, d8, b8 = hdus[8]
+    coeff = np.frombuffer(b8, dtype=">f8").reshape(d8[::-1]).astype(float)  # (4, N, nmax)
+    field = hdus[3][0]
+    save("celes_500.npz", lmax=int(float(hdus[7][0]["L MAX"])), wavelength=wavelength,
+         medium_index=complex(medium[0], medium[1]), positions=part[:, :3], radii=part[:, 3],
+         refractive_index=part[:, 4] + 1j * part[:, 5],
+         polar=float(field["POLAR ANGLE"]), azimuthal=float(field["AZIMUTHAL ANGLE"]),
+         polarization=field["POLARIZATION"], tolerance=float(hdus[6][0]["TOLERANCE"]),
+         initial=coeff[0] + 1j * coeff[1], scattered=coeff[2] + 1j * coeff[3])
 
 
 def translation_fixtures(lmax_values=(1, 2, 3, 4, 5, 6)):
@@ -197,7 +250,11 @@ def main():
     only = set(sys.argv[1:])
     if not only or "tables" in only:
         celes_fixtures()
+        celes_fits_fixture()
         translation_fixtures()
+    if only == {"celes500"}:
+        celes_fits_fixture()
+        return
     c1 = aggregate_c1(seed=0)
     if not only or "c1" in only:
         matvec_fixture("ref_matvec_c1.npz", c1.positions, c1.radii, c1.refractive_index,
