@@ -2,8 +2,8 @@
 
 Nothing in the product (the ``yasf_b200`` package) imports, links or executes
 anything under this directory. Only ``tests/``, ``__graft_entry__.smoke()`` and
-the CPU-baseline leg of ``bench.py`` use it, and only as the checker or as the
-timed CPU baseline.
+the CPU-baseline leg of ``bench.py`` use it, and only as the parity reference or as
+the timed CPU baseline.
 
 Contents
 --------

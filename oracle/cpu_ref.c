@@ -1,6 +1,6 @@
 /*
  * ORACLE — TEST INFRASTRUCTURE ONLY. Plain-C (OpenMP) restatement of the reference's CPU coupling
- * path, used as the parity checker in tests/ and as the timed CPU baseline in bench.py. The
+ * path, used as the parity reference in tests/ and as the timed CPU baseline in bench.py. The
  * product (yasf_b200/) never links or calls this file.
  *
  * Restated functions (file:line within the reference project):

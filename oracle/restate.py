@@ -1,6 +1,6 @@
 """ORACLE — TEST INFRASTRUCTURE ONLY. numpy restatements + ctypes access to ``cpu_ref.c``.
 
-Used by ``tests/`` (as the checker), ``__graft_entry__.smoke()`` (as the checker) and the CPU
+Used by ``tests/`` and ``__graft_entry__.smoke()`` (as the parity reference) and the CPU
 baseline leg of ``bench.py`` (timed). Nothing here is imported by the product package.
 
 Functions and the reference code they restate:

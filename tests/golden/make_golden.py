@@ -17,7 +17,7 @@ refidxdb and pyperf as inert stand-ins). Two kinds of fixtures are written:
   preconditioner block matrices assembled column by column from the reference's own
   master_matrix_multiply).
 
-Nothing on the GPU box reads the reference: the fixtures are committed.
+Nothing reads the reference at test or bench time: the fixtures are committed.
 """
 
 from __future__ import annotations
