@@ -193,7 +193,10 @@ int yasf_precond_bytes(const yasf_precond* pc, size_t* bytes);
  * cycle ends with the true residual ||b - A x|| checked against rtol*||b||; maxiter counts
  * restart cycles. A = I - T W. x holds x0 on entry and the solution on exit. Arnoldi uses
  * classical Gram-Schmidt with one re-orthogonalisation pass; Givens rotations and the Hessenberg
- * solve run on the device in float64.
+ * solve run on the device in float64. A preconditioner (pc, may be NULL) is applied from the
+ * complex64 copy of its block inverses with float64 arithmetic: a fixed linear operator, half the
+ * bytes of the float64 copy (the reference's block factors are complex64 too,
+ * yasfpy/preconditioner.py:391).
  * inner_precision: YASF_C128 for the plain solve; YASF_C64 runs the Krylov iterations on the
  * complex64 matvec and wraps them in float64 iterative refinement (true residual, update and
  * stopping test in float64), see the solve stats.

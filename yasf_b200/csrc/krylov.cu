@@ -299,10 +299,15 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
 
 namespace yasf {
 
-static int psolve(const Operator& op, int precision, const double2* x, double2* y, long long n) {
+// Block-Jacobi apply of a solve. The block inverses are streamed from their complex64 copy with
+// float64 arithmetic (apply_kernel accumulates in double), so the preconditioner stays one fixed
+// linear operator and float64 solves keep their stopping guarantees, while each apply (HBM-bound)
+// reads half the bytes. The reference builds its block factors in complex64 as well
+// (yasfpy/preconditioner.py:391).
+static int psolve(const Operator& op, const double2* x, double2* y, long long n) {
   if (op.pc)
     return yasf_precond_apply(op.pc, reinterpret_cast<const double*>(x), reinterpret_cast<double*>(y),
-                              1, n, precision, op.s);
+                              1, n, YASF_C64, op.s);
   YASF_COUNTED(copy_kernel<<<1024, 256, 0, op.s>>>(n, x, y));
   YASF_CUDA_TRY(cudaGetLastError());
   return YASF_OK;
@@ -364,7 +369,7 @@ static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, 
   const int m = restart;
 
   // Mb_nrm2 = ||psolve(b)||
-  if ((st = psolve(op, prec, b, t, n)) != YASF_OK) return st;
+  if ((st = psolve(op, b, t, n)) != YASF_OK) return st;
   if ((st = norm_into(n, t, part, scal + SL_NORM, s)) != YASF_OK) return st;
   if ((st = read_scalars(scal, s, hs)) != YASF_OK) return st;
   const double Mb_nrm2 = hs[SL_NORM];
@@ -394,7 +399,7 @@ static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, 
 
   for (int iter = 0; iter < maxiter; ++iter) {
     // v0 = psolve(r) / ||.||
-    if ((st = psolve(op, prec, r, Q, n)) != YASF_OK) return st;
+    if ((st = psolve(op, r, Q, n)) != YASF_OK) return st;
     if ((st = norm_into(n, Q, part, scal + SL_NORM, s)) != YASF_OK) return st;
     YASF_COUNTED(scale_kernel<<<1024, 256, 0, s>>>(n, Q, scal + SL_NORM, Q));
     YASF_COUNTED(cycle_start_kernel<<<1, 256, 0, s>>>(m, S, scal));
@@ -406,7 +411,7 @@ static int gmres_core(const Operator& op, const GmresWs& L, char* ws, int prec, 
       double2* hcol = H + (size_t)col * (m + 1);
       if ((st = op_apply(op, prec, vcol, t)) != YASF_OK) return st;
       if (prec == YASF_C128) cnt.mv64++; else cnt.mv_inner++;
-      if ((st = psolve(op, prec, t, w, n)) != YASF_OK) return st;
+      if ((st = psolve(op, t, w, n)) != YASF_OK) return st;
       if ((st = norm_into(n, w, part, scal + SL_H0, s)) != YASF_OK) return st;
       // CGS2: two projection sweeps
       for (int pass = 0; pass < 2; ++pass) {
