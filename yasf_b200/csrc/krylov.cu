@@ -536,21 +536,16 @@ extern "C" int yasf_gmres_solve(const yasf_plan* plan, int n_particles, const do
       if (!std::isfinite(rnorm)) return YASF_ERR_NOT_FINITE;
       if (rnorm <= atol) { info = 0; break; }
       if (it >= max_refine) { info = maxiter; break; }
-      // inner solve A d = r at complex64, d0 = 0; r is preserved in a copy (d region reused)
+      // inner solve A d = r at complex64 from d0 = 0. gmres_core uses r, t and w as scratch, so
+      // the residual (the inner right-hand side) is kept in the basis' last column, which the
+      // inner solve (restricted to m - 1 columns) never writes.
       YASF_CUDA_TRY(cudaMemsetAsync(d, 0, n * sizeof(double2), s));
-      // gmres_core overwrites r/t; keep the residual as the inner rhs in Q's last slot? use w.
-      double2* rhs = reinterpret_cast<double2*>(ws + L.o_w);
-      YASF_COUNTED(copy_kernel<<<1024, 256, 0, s>>>(n, r, rhs));
-      YASF_CUDA_TRY(cudaGetLastError());
-      // rhs lives in w, which the core uses as scratch; move it to the tail of d's neighbour: use
-      // the basis' last column as stable storage for the inner rhs.
       double2* rhs_store = reinterpret_cast<double2*>(ws + L.o_Q) + (size_t)m * n;
-      YASF_COUNTED(copy_kernel<<<1024, 256, 0, s>>>(n, rhs, rhs_store));
+      YASF_COUNTED(copy_kernel<<<1024, 256, 0, s>>>(n, r, rhs_store));
       YASF_CUDA_TRY(cudaGetLastError());
       int inner_info = 0;
       double inner_rn = 0.0;
       const double inner_atol = std::max(inner_rtol * rnorm, 0.5 * atol);
-      // basis restricted to m-1 columns so the rhs column is never overwritten
       st = gmres_core(op, L, ws, YASF_C64, rhs_store, d, rnorm, inner_atol,
                       std::max(1, m - 1), maxiter, false, cnt, &inner_info, &inner_rn);
       if (st != YASF_OK) return st;
