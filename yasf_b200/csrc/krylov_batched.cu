@@ -4,7 +4,9 @@
 // basis (float64, classical Gram-Schmidt with one re-orthogonalisation pass), Givens rotations
 // and Hessenberg solve (float64, on the device); one operator application serves all live columns
 // at once, so every W_ij is generated once per step for the whole panel:
-//   refine:  R_c = B_c - A X_c            (float64 master operator, column by column)
+//   refine:  R_c = B_c - A X_c            (float64 master operator: the dense multi-column kernel
+//                                          for 12 or more live columns up to lmax 6, else column
+//                                          by column)
 //            solve A~ D_c = R_c to inner_rtol (A~: tensor-core TF32 panel, or the complex64 /
 //                                            complex128 coupling kernels), X_c += D_c
 // until ||B_c - A X_c|| <= rtol ||B_c|| for every column. The block-Jacobi preconditioner, when
