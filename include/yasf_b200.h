@@ -62,6 +62,12 @@ int yasf_plan_destroy(yasf_plan* plan);
 /* nmax, stream entries per source particle (all bundles), source-side terms per particle. */
 int yasf_plan_info(const yasf_plan* plan, int* nmax, long long* stream_entries,
                    long long* source_terms);
+/* Host-only check (no device, nothing allocated on a GPU): builds the generation layouts a plan
+ * derives from `translation_ab5` (the tensor-core panel's schedule with its slot tables and term
+ * windows, the float64 dense panel's items) and returns YASF_ERR_INVALID_ARGUMENT if the table
+ * breaks the a5/b5 selection rules or mirror relations they rely on, YASF_ERR_NOT_FINITE for
+ * non-finite entries; yasf_plan_create runs the same check. No reference counterpart. */
+int yasf_plan_check_table(int lmax, const double* translation_ab5);
 
 /* Bytes of caller-provided device workspace needed by the coupling entry points for
  * n_particles spheres and nrhs right-hand sides at `precision`. */

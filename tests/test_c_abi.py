@@ -67,6 +67,35 @@ def test_argument_validation_without_device(lib):
     assert lib.yasf_batched_workspace_size(None, 10, 4, 30, 3, ctypes.byref(n)) == 1
 
 
+@pytest.mark.parametrize("lmax", range(1, 9))
+def test_plan_layouts_accept_the_translation_table(lib, lmax):
+    """The host-side builders a plan runs (the panel schedule with its slot tables and term windows,
+    packed FP16 coefficients at lmax 7-8, the float64 dense panel's items) accept the exact table
+    at every lmax: checked without a device."""
+    import numpy as np
+
+    from yasf_b200.wigner import translation_table_ab5
+
+    tab = np.ascontiguousarray(translation_table_ab5(lmax), dtype=np.complex128)
+    assert lib.yasf_plan_check_table(lmax, ctypes.c_void_p(tab.ctypes.data)) == 0
+
+
+def test_plan_layouts_reject_a_broken_table(lib):
+    import numpy as np
+
+    from yasf_b200.wigner import translation_table_ab5
+
+    tab = np.ascontiguousarray(translation_table_ab5(4), dtype=np.complex128)
+    bad = tab.copy()
+    bad[0, 0, 1] = 0.5  # a tau1 = tau2 term with l1 + l2 + p odd: outside the selection rules
+    assert lib.yasf_plan_check_table(4, ctypes.c_void_p(bad.ctypes.data)) == 1
+    bad = tab.copy()
+    bad[2, 1, 3] = np.nan
+    assert lib.yasf_plan_check_table(4, ctypes.c_void_p(bad.ctypes.data)) == 7
+    assert lib.yasf_plan_check_table(9, ctypes.c_void_p(tab.ctypes.data)) == 2
+    assert lib.yasf_plan_check_table(4, None) == 1
+
+
 def test_no_cpu_fallback_in_product():
     """The product package never imports the oracle."""
     for py in (REPO / "yasf_b200").rglob("*.py"):

@@ -61,6 +61,7 @@ SIGNATURES = {
     "yasf_plan_create": [_i, _vp, _c.POINTER(_vp)],
     "yasf_plan_destroy": [_vp],
     "yasf_plan_info": [_vp, _c.POINTER(_i), _c.POINTER(_ll), _c.POINTER(_ll)],
+    "yasf_plan_check_table": [_i, _vp],
     "yasf_coupling_workspace_size": [_vp, _i, _i, _i, _c.POINTER(_sz)],
     "yasf_coupling_matvec": [_vp, _i, _vp, _d, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],
     "yasf_master_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],

@@ -440,6 +440,24 @@ extern "C" int yasf_plan_destroy(yasf_plan* plan) {
   return YASF_OK;
 }
 
+extern "C" int yasf_plan_check_table(int lmax, const double* ab5) {
+  if (!ab5) return YASF_ERR_INVALID_ARGUMENT;
+  if (lmax < 1 || lmax > YASF_LMAX_MAX) return YASF_ERR_UNSUPPORTED;
+  const int nmax = nmax_of(lmax), P = 2 * lmax + 1;
+  for (size_t i = 0; i < (size_t)nmax * nmax * P * 2; ++i)
+    if (!std::isfinite(ab5[i])) return YASF_ERR_NOT_FINITE;
+  std::vector<float> gen_c1;
+  std::vector<unsigned> gen_meta, gen_dst;
+  std::vector<int4> dgen_chunks;
+  std::vector<int2> dgen_items;
+  std::vector<double> dgen_coef;
+  int st = panel_build_terms(lmax, ab5, gen_c1, gen_meta, gen_dst);
+  if (st == YASF_OK) st = dpanel_build_items(lmax, ab5, dgen_chunks, dgen_items, dgen_coef);
+  if (st != YASF_OK)
+    set_error_text("translation table does not follow the a5/b5 selection rules of the panel schedule");
+  return st;
+}
+
 extern "C" int yasf_plan_info(const yasf_plan* plan, int* nmax, long long* stream_entries,
                               long long* source_terms) {
   if (!plan) return YASF_ERR_INVALID_ARGUMENT;
