@@ -101,3 +101,27 @@ def test_no_cpu_fallback_in_product():
     for py in (REPO / "yasf_b200").rglob("*.py"):
         text = py.read_text()
         assert "import oracle" not in text and "from oracle" not in text, py
+
+
+def test_product_fails_loudly_without_a_gpu():
+    """Without a CUDA device the drop-in API raises instead of computing on the host; an unknown
+    backend name raises ValueError as the reference's if-chain does (yasfpy/simulation.py:95-106)."""
+    import numpy as np
+    import torch
+
+    from yasf_b200 import InitialField, Numerics, Parameters, Particles, Simulation
+    from yasf_b200.device import CouplingDevice
+    from yasf_b200.wigner import translation_table_ab5
+
+    particles = Particles(np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]]), np.array([0.1, 0.1]),
+                          np.array([1.5, 1.5], dtype=complex))
+    params = Parameters(np.array([1.0]), np.array([1.0 + 0j]), particles,
+                        InitialField(beam_width=0, focal_point=np.zeros(3)))
+    with pytest.raises(ValueError):
+        Simulation(params, Numerics(lmax=2, coupling_backend="dense"))
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(RuntimeError):
+        Simulation(params, Numerics(lmax=2))
+    with pytest.raises(RuntimeError, match="CUDA devices only"):
+        CouplingDevice(2, translation_table_ab5(2), particles.position, 1.0, torch.device("cpu"))
