@@ -44,7 +44,7 @@ def test_schedule_structure(L):
     assert collisions <= 4 * WARPS * len(steps)  # a few lanes per step, padding recomputation only
 
 
-def _emulate_wx(L, table_ab5, ri, rj, k, xj, packed=False):
+def _emulate_wx(L, table_ab5, ri, rj, k, xj, packed=False, blocks=False):
     H = L * (L + 2)
     P = 2 * L + 1
     d = np.asarray(ri) - np.asarray(rj)
@@ -114,6 +114,8 @@ def _emulate_wx(L, table_ab5, ri, rj, k, xj, packed=False):
                 Wa2, Wb2 = np.conj(E) * Sa, -1j * np.conj(E) * Sb
                 Pm[mirror(q1), mirror(q2)], Qm[mirror(q1), mirror(q2)] = Wa2 + Wb2, Wa2 - Wb2
     assert not np.isnan(Pm).any() and not np.isnan(Qm).any()
+    if blocks:
+        return Pm, Qm
     x1, x2 = xj[:H], xj[H:]
     U, V = Pm @ (x1 + x2), Qm @ (x1 - x2)
     return np.concatenate([(U + V) / 2, (U - V) / 2])
@@ -158,3 +160,23 @@ def test_slot_tables_are_deterministic():
     builds: the slot search is seeded."""
     steps, sched = schedule(5)
     assert slot_tables(5, steps, sched) == slot_tables(5, steps, sched)
+
+
+@pytest.mark.parametrize("L", [3, 6])
+def test_reverse_pair_blocks_are_sign_flipped_swaps(L):
+    """With r_ji = -r_ij, A_ji[p][d] = (-1)^(p+d) A_ij[p][d] and the phase gains (-1)^d, so every
+    term picks up (-1)^p: (-1)^(l1+l2) on Wa terms and -(-1)^(l1+l2) on Wb terms. Hence
+    P_ji = s Q_ij and Q_ji = s P_ij entrywise with s = (-1)^(l1+l2): one generation per unordered
+    pair could serve both directions."""
+    rng = np.random.default_rng(11)
+    tab = translation_table_ab5(L)
+    k = 2 * np.pi / 0.55
+    ri, rj = np.zeros(3), rng.normal(size=3) * 0.4
+    H = L * (L + 2)
+    Pij, Qij = _emulate_wx(L, tab, ri, rj, k, None, blocks=True)
+    Pji, Qji = _emulate_wx(L, tab, rj, ri, k, None, blocks=True)
+    ls = np.array([_lm(q)[0] for q in range(H)])
+    sgn = (-1.0) ** (ls[:, None] + ls[None, :])
+    scale = max(np.abs(Pij).max(), np.abs(Qij).max())
+    assert np.max(np.abs(Pji - sgn * Qij)) <= 1e-12 * scale
+    assert np.max(np.abs(Qji - sgn * Pij)) <= 1e-12 * scale
