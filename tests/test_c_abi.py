@@ -125,3 +125,30 @@ def test_product_fails_loudly_without_a_gpu():
         Simulation(params, Numerics(lmax=2))
     with pytest.raises(RuntimeError, match="CUDA devices only"):
         CouplingDevice(2, translation_table_ab5(2), particles.position, 1.0, torch.device("cpu"))
+
+
+def test_plain_c_consumer_builds_and_runs(lib, tmp_path):
+    """A C99 program includes the header, links the library and calls it (the binding a C or cgo host
+    would write): ABI version, status strings, and the host-only table check on a zero table
+    (zero is a valid, if useless, a5/b5 table)."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "consumer.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stdlib.h>\n#include "yasf_b200.h"\n'
+        "int main(void) {\n"
+        "  const int lmax = 2, nmax = 2 * lmax * (lmax + 2), P = 2 * lmax + 1;\n"
+        "  double* tab = calloc((size_t)nmax * nmax * P * 2, sizeof(double));\n"
+        "  int ok = yasf_plan_check_table(lmax, tab);\n"
+        '  printf("%d %d %s\\n", yasf_abi_version(), ok, yasf_status_string(YASF_ERR_WORKSPACE));\n'
+        "  free(tab);\n  return 0;\n}\n")
+    libdir = REPO / "yasf_b200" / "_build"
+    exe = tmp_path / "consumer"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", str(src), "-I", str(REPO / "include"), "-L", str(libdir),
+                    "-lyasf_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split(maxsplit=2)
+    assert out[0] == "1" and out[1] == "0" and out[2].strip() == "workspace too small"
