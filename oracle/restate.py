@@ -17,11 +17,10 @@ Functions and the reference code they restate:
 from __future__ import annotations
 
 import ctypes
-from pathlib import Path
 
 import numpy as np
 
-from oracle.build import OUT, build
+from oracle.build import build
 
 _lib = None
 

@@ -9,7 +9,7 @@ import torch
 from conftest import rel_err
 
 from oracle import restate as R
-from yasf_b200._lib import YASF_C64, YASF_C128
+from yasf_b200._lib import YASF_C64
 from yasf_b200.device import CouplingDevice
 from yasf_b200.wigner import translation_table_ab5
 from yasf_b200.workloads import aggregate_c2, rsa_cube

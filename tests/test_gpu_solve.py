@@ -10,7 +10,7 @@ from conftest import rel_err
 
 from yasf_b200 import BlockDiagonalPreconditioner, InitialField, Numerics, Optics, Parameters
 from yasf_b200 import Particles, Simulation, Solver
-from yasf_b200._lib import YASF_C64, YASF_C128, YasfError
+from yasf_b200._lib import YASF_C64, YasfError
 from yasf_b200.device import CouplingDevice, DevicePreconditioner
 from yasf_b200.wigner import translation_table_ab5
 

@@ -8,7 +8,6 @@ failure has already run every other test; it also passes alone in a fresh proces
 
 from __future__ import annotations
 
-import ctypes
 
 import numpy as np
 import pytest

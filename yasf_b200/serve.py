@@ -21,7 +21,6 @@ on what else is in flight: ``solve_request`` alone and inside the loop give the 
 
 from __future__ import annotations
 
-import ctypes
 import threading
 import time
 from collections import deque

@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from yasf_b200.coupling import B200CouplingBackend
-from yasf_b200.device import PRECISIONS, CouplingDevice
+from yasf_b200.device import CouplingDevice
 from yasf_b200.incident import compute_initial_field_coefficients
 from yasf_b200.mie import compute_mie_coefficients
 from yasf_b200.numerics import Numerics
