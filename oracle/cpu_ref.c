@@ -99,9 +99,9 @@ void oracle_legendre(int lmax, double ct, double st, double* out) {
 typedef struct {
   int n;      /* s */
   int tau, l, m;
-} mode_t;
+} mode_desc;
 
-static void modes_of(int lmax, mode_t* md) {
+static void modes_of(int lmax, mode_desc* md) {
   int tau, l, m;
   for (tau = 1; tau <= 2; ++tau)
     for (l = 1; l <= lmax; ++l)
@@ -161,7 +161,7 @@ int oracle_coupling_matvec(int lmax, int N, const double* pos, double k, const d
                            const double* x, int s1_begin, int s1_end, double* wx, int threads) {
   const int nmax = 2 * lmax * (lmax + 2), P = 2 * lmax, NP = P + 1;
   const int nplm = (P + 1) * (P + 2) / 2;
-  mode_t* md = (mode_t*)malloc(sizeof(mode_t) * nmax);
+  mode_desc* md = (mode_desc*)malloc(sizeof(mode_desc) * nmax);
   int s1;
   modes_of(lmax, md);
 #ifdef _OPENMP
@@ -224,7 +224,7 @@ int oracle_scattering_bilinear(int lmax, int N, const double* pos, double k, con
                                const double* b, int s1_begin, int s1_end, double* out, int threads) {
   const int nmax = 2 * lmax * (lmax + 2), P = 2 * lmax, NP = P + 1;
   const int nplm = (P + 1) * (P + 2) / 2;
-  mode_t* md = (mode_t*)malloc(sizeof(mode_t) * nmax);
+  mode_desc* md = (mode_desc*)malloc(sizeof(mode_desc) * nmax);
   double tot_r = 0.0, tot_i = 0.0;
   int s1;
   modes_of(lmax, md);
