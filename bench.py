@@ -32,7 +32,8 @@ Other workloads (--workload):
          first of the 512-request stream); warm-up = requests drawn from the same distribution
          with other seeds; value = right-hand sides solved per second over the makespan, with
          p50/p99 request latency and the C_ext error of sampled requests against float64 solves
-  c5     20000 spheres, lmax 4, rtol 1e-6, 8x8x8 block-Jacobi
+  c5     20000 spheres, lmax 4, R = 2 (TE, TM), 8x8x8 block-Jacobi, rtol 1e-6: plain float64 and
+         mixed-precision solves of both columns, phases timed separately
 
 --impl reference times the reference's CPU algorithm (the oracle port, all host threads) on the
 same workload and prints the same metric with "impl": "reference".
@@ -174,10 +175,10 @@ def host_threads() -> int:
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
-    from yasf_b200.numerics import cached_translation_table
+    from oracle.restate import reference_translation_table
 
     agg, _, _ = workload(args.workload)
-    table = cached_translation_table(agg.lmax)
+    table = reference_translation_table(agg.lmax)  # the reference's own table (committed fixture)
     threads = host_threads()
     per_step = max(3.0, min(30.0, 120.0 / max(1, args.steps + args.warmup)))
     times = []
@@ -383,8 +384,12 @@ def run_b200(args, rank: int, world: int) -> None:
         e1.synchronize()
         b_s = e0.elapsed_time(e1) / 1e3
         colres = bst.pop("column_residuals")
+        errors = None
+        if not args.no_column_errors:
+            errors = all_column_errors(dev, tmat, A_cols, B_cols, Xb, agg.k)
         batched = {"solves_per_s": len(pol) / b_s, "speedup_vs_plain_fp64": len(pol) / b_s / value,
                    "nrhs": len(pol), "seconds": b_s, "max_fp64_relative_residual": max(colres),
+                   "error_vs_fp64_all_columns": errors,
                    "stats": bst,
                    "config": f"same aggregate, {len(pol) // 2} seeded Fibonacci directions x TE/TM, TF32 "
                              f"tensor-core panel inner GMRES (inner rtol {args.inner_rtol:g}, restart 50) in float64 "
@@ -396,7 +401,10 @@ def run_b200(args, rank: int, world: int) -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = host_threads()
-        t_mv_cpu, rows = cpu_matvec_seconds(agg, numerics.translation_ab5, args.cpu_seconds, threads)
+        from oracle.restate import reference_translation_table
+
+        t_mv_cpu, rows = cpu_matvec_seconds(agg, reference_translation_table(agg.lmax), args.cpu_seconds,
+                                            threads)
         mv_per_solve = stats["matvecs_f64"]
         cpu = {"value": 1.0 / (t_mv_cpu * mv_per_solve), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{rows} of {n} receiving-sphere rows of the C-restated particle_interaction_scalar, "
@@ -455,6 +463,39 @@ def cross_sections(dev, a_col, x_col, k: float) -> tuple[float, float]:
     c_ext = -np.real(dev.dotc(a_col, x_col)) / k**2 * np.pi
     c_sca = abs(dev.scattering_bilinear(x_col)) / k**2 * np.pi
     return float(c_ext), float(c_sca)
+
+
+def all_column_errors(dev, tmat, A_cols: np.ndarray, B, X, k: float) -> dict:
+    """Error of every column of a batched solution X against plain float64 GPU solutions.
+
+    The float64 solutions come from the lockstep GMRES with the complex128 inner operator (the
+    float64 dense multi-column kernel for 12 or more columns up to lmax 6, else the complex128
+    coupling kernel), no preconditioner, refined to rtol 1e-10: no reduced precision anywhere.
+    Reported per column: relative coefficient error (2-norm), relative C_ext and C_sca error."""
+    import torch
+
+    X64, st64 = dev.batched_solve(tmat, B, rtol=1e-10, restart=60, max_refine=4, inner_rtol=1e-10,
+                                  inner="c128")
+    R = X.shape[0]
+    coef = (torch.linalg.vector_norm(X - X64, dim=1) / torch.linalg.vector_norm(X64, dim=1)).cpu().numpy()
+    At = torch.from_numpy(np.ascontiguousarray(A_cols)).to(X.device)
+    ce = (-torch.real((At.conj() * X).sum(dim=1)) / k**2 * np.pi).cpu().numpy()
+    ce64 = (-torch.real((At.conj() * X64).sum(dim=1)) / k**2 * np.pi).cpu().numpy()
+    cs = np.array([abs(dev.scattering_bilinear(X[c].contiguous())) for c in range(R)]) / k**2 * np.pi
+    cs64 = np.array([abs(dev.scattering_bilinear(X64[c].contiguous())) for c in range(R)]) / k**2 * np.pi
+    ext_err = np.abs(ce - ce64) / np.abs(ce64)
+    sca_err = np.abs(cs - cs64) / np.abs(cs64)
+    colres = st64.pop("column_residuals")
+
+    def summ(v):
+        return {"max": float(np.max(v)), "median": float(np.median(v)),
+                "per_column": [float(f"{e:.3g}") for e in v]}
+
+    return {"columns": R, "coef_rel_err": summ(coef), "c_ext_rel_err": summ(ext_err),
+            "c_sca_rel_err": summ(sca_err),
+            "fp64_reference": {"max_relative_residual": float(max(colres)), "stats": st64,
+                               "how": "lockstep float64 GMRES, complex128 inner operator (float64 dense "
+                                      "multi-column kernel), no preconditioner, rtol 1e-10"}}
 
 
 def fp64_column(dev, tmat, b_col, rtol=1e-10):
@@ -532,22 +573,8 @@ def run_batched(args, rank: int, world: int) -> None:
     e2e_s = time.perf_counter() - t0
     del Bd, Xe
 
-    # errors against float64 solves of sampled columns
-    samples = []
-    worst = {"c_ext": 0.0, "c_sca": 0.0, "coef": 0.0}
-    for c in sorted({0, R // 2 - 1, R - 1})[: args.error_samples]:
-        x64, st64 = fp64_column(dev, tmat, B[c].contiguous())
-        ac = torch.from_numpy(A[c]).to(device)
-        ce, cs = cross_sections(dev, ac, X[c].contiguous(), agg.k)
-        ce64, cs64 = cross_sections(dev, ac, x64, agg.k)
-        coef = float(torch.linalg.vector_norm(X[c] - x64) / torch.linalg.vector_norm(x64))
-        e = {"column": c, "c_ext": ce, "c_ext_fp64": ce64, "c_ext_rel_err": abs(ce - ce64) / abs(ce64),
-             "c_sca_rel_err": abs(cs - cs64) / abs(cs64), "coef_rel_err": coef, "fp64_info": st64["info"],
-             "fp64_residual": st64["relative_residual"]}
-        samples.append(e)
-        worst["c_ext"] = max(worst["c_ext"], e["c_ext_rel_err"])
-        worst["c_sca"] = max(worst["c_sca"], e["c_sca_rel_err"])
-        worst["coef"] = max(worst["coef"], coef)
+    # errors of every column against plain float64 GPU solutions
+    errors = all_column_errors(dev, tmat, A, B, X, agg.k)
     colres = st.pop("column_residuals")
 
     if rank != 0:
@@ -567,7 +594,7 @@ def run_batched(args, rank: int, world: int) -> None:
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "solve_stats": st,
         "fp64_residual_all_columns": {"max": max(colres), "median": statistics.median(colres)},
-        "error_vs_fp64": {"worst": worst, "samples": samples},
+        "error_vs_fp64_all_columns": errors,
         "e2e": {"value": world * R / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes},
         "gpu_launches": int(launches),
@@ -670,6 +697,129 @@ def run_serve(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_large(args, rank: int, world: int) -> None:
+    """C5: the 20,000-sphere aggregate (lmax 4, 960,000 unknowns, R = 2 polarisations TE/TM along
+    +z), block-Jacobi on 8x8x8 cells, GMRES to rtol 1e-6: plain float64 against mixed precision
+    (complex64 inner GMRES in float64 refinement), each column solved on the device.
+
+    Phases are timed separately: random sequential addition (host), preconditioner prepare
+    (assembly, factorisation, finalize), each float64 solve and each mixed solve (CUDA events),
+    with iteration and matvec counts. A warm-up step is one application of each operator (float64
+    and complex64 master operators, preconditioner), not a solve: one C5 solve takes minutes.
+    value = right-hand sides per second of the mixed form (device-resident); e2e = the same solves
+    with the right-hand side copied from pinned host memory and the solution copied back inside
+    the timed region."""
+    import torch
+
+    from yasf_b200 import _lib
+    from yasf_b200.device import PRECISIONS, CouplingDevice, DevicePreconditioner
+    from yasf_b200.incident import plane_wave_block
+    from yasf_b200.mie import mie_tmatrix_per_sphere
+    from yasf_b200.numerics import cached_translation_table
+    from yasf_b200.preconditioner import make_particle_partition
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    lib = _lib.load()
+    t0 = time.perf_counter()
+    agg, rtol, cells = workload("c5")
+    rsa_s = time.perf_counter() - t0
+    dev = CouplingDevice(agg.lmax, cached_translation_table(agg.lmax), agg.positions, agg.k, device)
+    tm = mie_tmatrix_per_sphere(agg.lmax, agg.k, agg.radii, agg.refractive_index)
+    tmat = torch.from_numpy(tm).to(device)
+    polar, azim, pol = np.zeros(2), np.zeros(2), np.array([1, 2])  # +z, TE and TM
+    a_blk = plane_wave_block(agg.lmax, agg.positions, agg.k, polar, azim, pol)
+    A_cols = np.ascontiguousarray(np.moveaxis(a_blk, 2, 0).reshape(2, -1))
+    B_host = torch.from_numpy(np.ascontiguousarray(A_cols * tm[None, :])).pin_memory()
+    B = B_host.to(device)
+    extent = agg.positions.max(axis=0) - agg.positions.min(axis=0)
+    blocks = make_particle_partition(agg.positions, (extent + 2.0) / cells)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pc = DevicePreconditioner(dev, blocks)
+    phases = pc.prepare(tmat)
+    torch.cuda.synchronize()
+    prepare_s = time.perf_counter() - t0
+
+    restart, maxiter = args.restart_large, 4
+    x = torch.randn(dev.n, dtype=torch.complex128, device=device)
+    for _ in range(args.warmup):
+        dev.master(x, tmat, PRECISIONS["c128"])
+        dev.master(x, tmat, PRECISIONS["c64"])
+        pc.apply(x, PRECISIONS["c64"])
+    torch.cuda.synchronize()
+    del x
+
+    def solve(col, precision, e2e=False):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        w0 = time.perf_counter()
+        b = B_host[col].to(device, non_blocking=True) if e2e else B[col]
+        e0.record()
+        xs = b.clone()
+        st = dev.gmres(tmat, b, xs, rtol, restart, maxiter, PRECISIONS[precision], pc)
+        e1.record()
+        xh = xs.cpu() if e2e else None
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        st["seconds"] = e0.elapsed_time(e1) / 1e3
+        if e2e:
+            st["e2e_seconds"] = wall
+        return xs, xh, st
+
+    launches0 = lib.yasf_kernel_launches()
+    fp64, mixed = [], []
+    with ClockSampler(local) as clk:
+        for c in range(2):
+            fp64.append(solve(c, "c128"))
+        for c in range(2):
+            mixed.append(solve(c, "c64", e2e=True))
+    launches = lib.yasf_kernel_launches() - launches0
+
+    k = agg.k
+    cols = []
+    for c in range(2):
+        x64, xm = fp64[c][0], mixed[c][0]
+        a = torch.from_numpy(A_cols[c]).to(device)
+        ce64 = -np.real(dev.dotc(a, x64)) / k**2 * np.pi
+        cem = -np.real(dev.dotc(a, xm)) / k**2 * np.pi
+        cs64 = abs(dev.scattering_bilinear(x64)) / k**2 * np.pi
+        csm = abs(dev.scattering_bilinear(xm)) / k**2 * np.pi
+        cols.append({"polarisation": ["TE", "TM"][c], "c_ext_fp64": ce64, "c_sca_fp64": cs64,
+                     "c_ext_rel_err_mixed": abs(cem - ce64) / abs(ce64),
+                     "c_sca_rel_err_mixed": abs(csm - cs64) / abs(cs64),
+                     "coef_rel_err_mixed": float(torch.linalg.vector_norm(xm - x64) / torch.linalg.vector_norm(x64)),
+                     "fp64": fp64[c][2], "mixed": mixed[c][2]})
+    fp64_s = sum(f[2]["seconds"] for f in fp64)
+    mixed_s = sum(m[2]["seconds"] for m in mixed)
+    mixed_e2e_s = sum(m[2]["e2e_seconds"] for m in mixed)
+    if rank != 0:
+        return
+    line = {
+        "metric": "solves/s (C5: 20000 spheres, lmax 4, R=2, 8x8x8 block-Jacobi, rtol 1e-6; mixed precision "
+                  "vs plain FP64, C_ext err vs FP64 GPU)",
+        "value": 2 / mixed_s, "unit": UNIT, "n_gpus": world, "steps": 2, "warmup": args.warmup,
+        "ms_per_step": mixed_s * 1e3 / 2, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 inner / c128 refinement", "data": "synthetic (seeded RSA aggregate, no dataset)",
+        "config": {"workload": agg.name + "-R2", "n_spheres": agg.n, "lmax": agg.lmax, "unknowns": dev.n,
+                   "nrhs": 2, "rtol": rtol, "restart": restart,
+                   "preconditioner": f"block-Jacobi {cells}x{cells}x{cells} cells ({len(blocks)} blocks)",
+                   "parallelism": "single GPU",
+                   "l2": "inputs (15 MB per column, 1 GB V stream, 29-58 GB of factors) larger than L2",
+                   "warmup": "one application of each operator per warm-up step (not a solve)"},
+        "fp64_solves_per_s": 2 / fp64_s, "mixed_speedup_vs_fp64": fp64_s / mixed_s,
+        "phases_s": {"rsa_host": rsa_s, "prepare": prepare_s, "prepare_detail": phases,
+                     "fp64_solves": fp64_s, "mixed_solves": mixed_s},
+        "columns": cols,
+        "e2e": {"value": 2 / mixed_e2e_s, "unit": UNIT, "h2d_bytes_per_step": dev.n * 16,
+                "d2h_bytes_per_step": dev.n * 16},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def panel_probe(args) -> None:
     """Four panel matvecs (the first is warm-up) on the first N spheres with --nrhs columns
     (TF32 tensor-core panel, or the float64 dense multi-column kernel with --float64-panel)."""
@@ -746,6 +896,7 @@ def main() -> None:
     ap.add_argument("--float64-panel", action="store_true",
                     help="--panel-probe times the float64 dense multi-column coupling instead")
     ap.add_argument("--restart-batched", type=int, default=50, help="inner GMRES cycle length (c3)")
+    ap.add_argument("--restart-large", type=int, default=250, help="GMRES cycle length (c5)")
     ap.add_argument("--inner-rtol", type=float, default=2e-3,
                     help="batched solves: inner GMRES tolerance per float64 refinement step")
     ap.add_argument("--slots", type=int, default=4, help="serving slots (serve)")
@@ -753,7 +904,9 @@ def main() -> None:
                     help="serve: choose each request's inner operator with the (lmax, N, R) autotuner "
                          "(timed inside the run) instead of the fixed rule")
     ap.add_argument("--serve-rtol", type=float, default=1e-6, help="serving refinement tolerance")
-    ap.add_argument("--error-samples", type=int, default=3, help="float64 check solves (c3, serve)")
+    ap.add_argument("--error-samples", type=int, default=3, help="float64 check solves (serve)")
+    ap.add_argument("--no-column-errors", action="store_true",
+                    help="skip the float64 reference solves behind the batched block's per-column errors")
     args = ap.parse_args()
     if args.matvec_probe:
         matvec_probe(args)
@@ -783,6 +936,8 @@ def main() -> None:
             run_batched(args, rank, world)
         elif args.workload == "serve":
             run_serve(args, rank, world)
+        elif args.workload == "c5":
+            run_large(args, rank, world)
         else:
             run_b200(args, rank, world)
     finally:

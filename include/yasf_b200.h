@@ -51,6 +51,25 @@ const char* yasf_last_cuda_error(void);
  * per-operator matvec_calls / uploads counters of yasfpy/coupling/cuda_dense.py:102-105. */
 unsigned long long yasf_kernel_launches(void);
 
+/* Test hook for failure detection; no counterpart in the reference. Every wait inside a kernel of
+ * this library is bounded: when it runs out, the kernel records an error word, writes NaN outputs,
+ * frees what it holds and returns, so the CUDA context stays usable and the host sees
+ * YASF_ERR_NOT_FINITE from a solve. This call makes such a wait run out on purpose for the next
+ * launches FROM THIS HOST THREAD: `role` names one producer that never delivers (the first stage
+ * copy of every block of the coupling contraction; the pair-table warps of the tensor-core panel;
+ * the helper warp of the float64 dense panel), `contract_polls` (> 0) replaces the contraction's
+ * poll limit per stage wait (2^22) and `panel_wait_seconds` (> 0, <= 10) the panels' wait bound
+ * (1 s). 0 keeps a default. YASF_STALL_NONE restores normal launches. The error word a kernel
+ * sets is the int at byte offset (required workspace bytes - 256) of the call's workspace, for
+ * the coupling, panel and dense-panel entry points alike (0: every wait completed). */
+enum yasf_stall_role {
+  YASF_STALL_NONE = 0,
+  YASF_STALL_CONTRACT = 1,
+  YASF_STALL_PANEL = 2,
+  YASF_STALL_DPANEL = 3
+};
+int yasf_test_stall(int role, int contract_polls, double panel_wait_seconds);
+
 /* ---- plan: the a5/b5 translation table in the layout the kernels stream -----------------
  * Replaces the per-Simulation table handling of yasfpy/coupling/cpu_dense.py:45-64 and
  * yasfpy/coupling/cuda_dense.py:52-158. `translation_ab5` is the HOST complex128 array

@@ -12,17 +12,30 @@ Functions and the reference code they restate:
   scipy_gmres_solve         yasfpy/scattered_field_coefficients.py:95-144 + yasfpy/solver.py:108-121
   block_matrix              (I - T W)[B, B] column by column from master_matvec, the preconditioner
                             pin (yasfpy/preconditioner.py:92-175 cannot build multi-sphere blocks)
+  reference_translation_table  the reference's own Numerics.translation_ab5 (yasfpy/numerics.py:187-281)
+                            for lmax 1-8, as generated by tests/golden/make_golden.py
 """
 
 from __future__ import annotations
 
 import ctypes
+from pathlib import Path
 
 import numpy as np
 
 from oracle.build import build
 
 _lib = None
+
+GOLDEN = Path(__file__).resolve().parents[1] / "tests" / "golden"
+
+
+def reference_translation_table(lmax: int) -> np.ndarray:
+    """The a5/b5 table computed by the reference itself (committed fixtures), indexed
+    [n_source, n_receiver, p] as particle_interaction_scalar reads it."""
+    name = "ref_translation.npz" if lmax <= 6 else "ref_translation_l78.npz"
+    with np.load(GOLDEN / name) as z:
+        return np.ascontiguousarray(z[f"lmax{lmax}"], dtype=np.complex128)
 
 
 def lib() -> ctypes.CDLL:

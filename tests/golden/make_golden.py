@@ -1,9 +1,12 @@
 """Generate the golden fixtures in tests/golden/ by running the upstream reference itself.
 
-Run in a container where the reference ``yasfpy`` source tree is available (read-only) at
-``$YASF_REFERENCE`` (default ``/root/reference``):
+Run in a container where the reference ``yasfpy`` source tree is available (read-only); its
+location must be given in ``$YASF_REFERENCE`` (there is no default):
 
-    python tests/golden/make_golden.py
+    YASF_REFERENCE=<path to the yasfpy checkout> python tests/golden/make_golden.py [part ...]
+
+Parts: ``tables`` (CELES goldens and translation tables lmax 1-6), ``c1``, ``l78`` (translation
+tables lmax 7 and 8 and reference matvec fixtures at those orders), ``celes500``; no part = all.
 
 The reference imports with the stand-ins from ``oracle/stubs`` (pywigxjpf via sympy's exact 3j,
 refidxdb and pyperf as inert stand-ins). Two kinds of fixtures are written:
@@ -31,7 +34,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path(os.environ.get("YASF_REFERENCE", "/root/reference"))
+if not os.environ.get("YASF_REFERENCE"):
+    sys.exit("make_golden.py: set YASF_REFERENCE to the reference (yasfpy) source tree")
+REF = Path(os.environ["YASF_REFERENCE"])
 sys.path.insert(0, str(REPO))
 sys.path.insert(0, str(REPO / "oracle" / "stubs"))
 sys.path.insert(0, str(REF))
@@ -156,7 +161,7 @@ def celes_fits_fixture():
          initial=coeff[0] + 1j * coeff[1], scattered=coeff[2] + 1j * coeff[3])
 
 
-def translation_fixtures(lmax_values=(1, 2, 3, 4, 5, 6)):
+def translation_fixtures(lmax_values=(1, 2, 3, 4, 5, 6), name="ref_translation.npz"):
     _, Numerics, *_ = ref_modules()
     out = {}
     for L in lmax_values:
@@ -164,8 +169,22 @@ def translation_fixtures(lmax_values=(1, 2, 3, 4, 5, 6)):
         num = Numerics(lmax=L, sampling_points_number=np.array([10]))
         num.compute_translation_table(force_compute=True)
         out[f"lmax{L}"] = num.translation_ab5
-        print(f"  translation table lmax={L}: {time.time() - t0:.1f}s")
-    save("ref_translation.npz", **out)
+        print(f"  translation table lmax={L}: {time.time() - t0:.1f}s", flush=True)
+    save(name, **out)
+
+
+def high_order_fixtures():
+    """lmax 7 and 8 (the serving stream draws lmax up to 8): the reference's own translation
+    tables and coupling / master matvecs of small seeded aggregates at those orders."""
+    translation_fixtures((7, 8), name="ref_translation_l78.npz")
+    rng = np.random.default_rng(17)
+    r7 = rng.uniform(0.05, 0.2, size=10)
+    p7 = rsa_cube(r7, 0.15, rng, max_attempts=200_000)
+    matvec_fixture("ref_matvec_l7.npz", p7, r7, 1.7 + 0.01j, 0.45, 7, seed=14)
+    rng = np.random.default_rng(19)
+    r8 = rng.uniform(0.05, 0.2, size=9)
+    p8 = rsa_cube(r8, 0.12, rng, max_attempts=200_000)
+    matvec_fixture("ref_matvec_l8.npz", p8, r8, 1.35 + 0.05j, 0.4, 8, seed=15)
 
 
 def matvec_fixture(name, positions, radii, m, wavelength, lmax, seed):
@@ -254,6 +273,9 @@ def main():
         translation_fixtures()
     if only == {"celes500"}:
         celes_fits_fixture()
+        return
+    if only == {"l78"}:
+        high_order_fixtures()
         return
     c1 = aggregate_c1(seed=0)
     if not only or "c1" in only:

@@ -67,6 +67,16 @@ def test_argument_validation_without_device(lib):
     assert lib.yasf_batched_workspace_size(None, 10, 4, 30, 3, ctypes.byref(n)) == 1
 
 
+def test_stall_hook_validates_its_arguments(lib):
+    # the failure-detection test hook is host state only: no device is touched here
+    assert lib.yasf_test_stall(7, 0, 0.0) == 1
+    assert lib.yasf_test_stall(2, -1, 0.0) == 1
+    assert lib.yasf_test_stall(2, 0, 100.0) == 1
+    assert lib.yasf_test_stall(2, 0, float("nan")) == 1
+    assert lib.yasf_test_stall(1, 4096, 0.05) == 0
+    assert lib.yasf_test_stall(0, 0, 0.0) == 0
+
+
 @pytest.mark.parametrize("lmax", range(1, 9))
 def test_plan_layouts_accept_the_translation_table(lib, lmax):
     """The host-side builders a plan runs (the panel schedule with its slot tables and term windows,

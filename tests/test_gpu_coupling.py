@@ -27,7 +27,8 @@ def _t(a, device):
 
 
 @pytest.mark.parametrize("fixture,lmax", [("ref_matvec_c1.npz", 4), ("ref_matvec_l6.npz", 6),
-                                          ("ref_matvec_l3.npz", 3)])
+                                          ("ref_matvec_l3.npz", 3), ("ref_matvec_l7.npz", 7),
+                                          ("ref_matvec_l8.npz", 8)])
 def test_matvec_matches_reference(golden, cuda_device, fixture, lmax):
     g = golden(fixture)
     k = 2 * np.pi / float(g["wavelength"])

@@ -56,3 +56,17 @@ def test_panel_single_sphere_is_zero(cuda_device):
     X = torch.ones((2, dev.n), dtype=torch.complex128, device=cuda_device)
     Y = dev.panel(X).cpu().numpy()
     assert np.all(Y == 0)
+
+
+@pytest.mark.parametrize("fixture,lmax", [("ref_matvec_l7.npz", 7), ("ref_matvec_l8.npz", 8)])
+def test_panel_high_orders_match_reference(golden, cuda_device, fixture, lmax):
+    # lmax 7-8 pack the generation coefficients as FP16 pairs: checked against the reference's own
+    # coupling matvec and master operator at those orders
+    g = golden(fixture)
+    k = 2 * np.pi / float(g["wavelength"])
+    dev = CouplingDevice(lmax, translation_table_ab5(lmax), g["positions"], k, cuda_device)
+    X = torch.from_numpy(np.ascontiguousarray(g["x"][None, :])).to(cuda_device)
+    T = torch.from_numpy(np.ascontiguousarray(g["tmat"])).to(cuda_device)
+    assert rel_err(dev.panel(X).cpu().numpy()[0], g["wx"]) < TOL
+    mx = dev.panel(X, T).cpu().numpy()[0]
+    assert rel_err(g["x"] - mx, g["x"] - g["mx"]) < TOL

@@ -31,6 +31,15 @@ def test_translation_table_matches_reference(golden, lmax):
     assert np.max(np.abs(ours - ref)) <= 1e-14 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("lmax", [7, 8])
+def test_translation_table_high_orders_match_reference(golden, lmax):
+    # lmax 7 and 8 (drawn by the serving stream): the reference's own Numerics tables
+    ref = golden("ref_translation_l78.npz")[f"lmax{lmax}"]
+    ours = translation_table_ab5(lmax)
+    assert ours.shape == ref.shape
+    assert np.max(np.abs(ours - ref)) <= 1e-14 * np.max(np.abs(ref))
+
+
 def test_translation_table_matches_celes_golden(golden):
     celes = golden("celes_translation_lmax3.npz")["table"]
     np.testing.assert_allclose(translation_table_ab5(3), celes, rtol=1e-5, atol=1e-7)

@@ -15,7 +15,7 @@ import torch
 from conftest import rel_err
 
 from yasf_b200 import _lib
-from yasf_b200._lib import YASF_C128
+from yasf_b200._lib import YASF_C64, YASF_C128
 from yasf_b200.device import CouplingDevice, _ptr, _stream_ptr
 from yasf_b200.wigner import translation_table_ab5
 from yasf_b200.workloads import rsa_cube
@@ -45,6 +45,40 @@ def test_noalloc_matches_regular_entry_point_twice(cuda_device):
         ref = dev.coupling(x)  # regular entry point, caller-provided workspace
         torch.cuda.synchronize()
         assert rel_err(y.cpu().numpy(), ref.cpu().numpy()) < 1e-12, f"call {call}"
+
+
+def _aggregate(device, lmax, n, seed):
+    rng = np.random.default_rng(seed)
+    radii = rng.uniform(0.05, 0.12, size=n)
+    pos = rsa_cube(radii, 0.15, rng)
+    return CouplingDevice(lmax, translation_table_ab5(lmax), pos, 2 * np.pi / 0.55, device), rng
+
+
+def test_noalloc_smaller_problem_after_larger_one(cuda_device):
+    # The shared scratch keeps what the larger call left; the smaller call must not read any of it
+    # (its stream and partial sums are written in full before they are read).
+    big, rng = _aggregate(cuda_device, 5, 120, 31)
+    small, _ = _aggregate(cuda_device, 3, 17, 32)
+    assert big.coupling_ws_bytes(YASF_C128) > small.coupling_ws_bytes(YASF_C128)
+    assert big.coupling_ws_bytes(YASF_C128) <= 64 * 1024 * 1024
+    for dev in (big, small, big, small):  # all on the current stream, in order
+        x = torch.from_numpy(rng.normal(size=dev.n) + 1j * rng.normal(size=dev.n)).to(cuda_device)
+        st, y = _noalloc(dev, x)
+        assert st == 0, _lib.load().yasf_status_string(st)
+        ref = dev.coupling(x)
+        torch.cuda.synchronize()
+        assert rel_err(y.cpu().numpy(), ref.cpu().numpy()) < 1e-12
+
+
+def test_noalloc_complex64_matches_regular_complex64(cuda_device):
+    dev, rng = _aggregate(cuda_device, 4, 60, 33)
+    for call in range(2):
+        x = torch.from_numpy(rng.normal(size=dev.n) + 1j * rng.normal(size=dev.n)).to(cuda_device)
+        st, y = _noalloc(dev, x, YASF_C64)
+        assert st == 0, _lib.load().yasf_status_string(st)
+        ref = dev.coupling(x, YASF_C64)  # regular complex64 call, caller-provided workspace
+        torch.cuda.synchronize()
+        assert rel_err(y.cpu().numpy(), ref.cpu().numpy()) < 2e-5, f"call {call}"
 
 
 def test_noalloc_rejects_problems_beyond_the_static_scratch(cuda_device):

@@ -58,6 +58,7 @@ SIGNATURES = {
     "yasf_status_string": [_i],
     "yasf_last_cuda_error": [],
     "yasf_kernel_launches": [],
+    "yasf_test_stall": [_i, _i, _d],
     "yasf_plan_create": [_i, _vp, _c.POINTER(_vp)],
     "yasf_plan_destroy": [_vp],
     "yasf_plan_info": [_vp, _c.POINTER(_i), _c.POINTER(_ll), _c.POINTER(_ll)],
@@ -129,3 +130,16 @@ def check(func: str, status: int) -> None:
 def call(name: str, *args) -> None:
     """Call a status-returning entry point and raise ``YasfError`` on failure."""
     check(name, getattr(load(), name)(*args))
+
+
+YASF_STALL_NONE = 0
+YASF_STALL_CONTRACT = 1
+YASF_STALL_PANEL = 2
+YASF_STALL_DPANEL = 3
+
+
+def test_stall(role: int, contract_polls: int = 0, panel_wait_seconds: float = 0.0) -> None:
+    """Failure-detection test hook (yasf_test_stall): the next launches from this host thread keep
+    one producer role from delivering, with shortened wait bounds. ``YASF_STALL_NONE`` restores
+    normal launches."""
+    call("yasf_test_stall", int(role), int(contract_polls), float(panel_wait_seconds))

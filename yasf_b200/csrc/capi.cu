@@ -1,4 +1,5 @@
 // C-ABI: library status, translation plan, coupling matvec, cross-section reductions.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <atomic>
@@ -11,6 +12,9 @@ namespace yasf {
 
 static thread_local std::string g_last_error;
 static std::atomic<unsigned long long> g_launches{0};
+static thread_local StallHook g_stall;
+
+const StallHook& stall_hook() { return g_stall; }
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -55,7 +59,10 @@ static int sm_count_of(int device) {
 
 CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int precision) {
   CouplingLayout lay;
+  // partial sums: complex at the kernel's precision; V stream: 16-byte entries at both precisions
+  // (complex64 entries carry (re, im, -im, re) for the packed FMAs)
   const size_t csize = (precision == YASF_C64) ? sizeof(float2) : sizeof(double2);
+  const size_t vsize = (precision == YASF_C64) ? sizeof(float4) : sizeof(double2);
   const int N = n_particles;
   // Receivers per block: whole warps, at most 4.
   const int warps = std::min(4, std::max(1, (N + 31) / 32));
@@ -73,7 +80,7 @@ CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int preci
   lay.sources_per_chunk = (N + chunks - 1) / chunks;
   lay.chunks = (N + lay.sources_per_chunk - 1) / lay.sources_per_chunk;
   auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-  lay.v_bytes = up((size_t)N * plan->total_entries * csize);
+  lay.v_bytes = up((size_t)N * plan->total_entries * vsize);
   lay.partial_bytes = up(per_chunk * lay.chunks);
   lay.dot_bytes = up(1024 * sizeof(double2) + 256);  // block sums + the stage-timeout word
   lay.total = lay.v_bytes + lay.partial_bytes + lay.dot_bytes;
@@ -86,6 +93,19 @@ int validate_coupling(const yasf_plan* plan, int n_particles, const double* posi
   if (precision != YASF_C128 && precision != YASF_C64) return YASF_ERR_INVALID_ARGUMENT;
   if (!std::isfinite(k) || k <= 0.0) return YASF_ERR_UNSUPPORTED;
   if (reinterpret_cast<uintptr_t>(positions) & 7u) return YASF_ERR_ALIGNMENT;
+  // The plan's tables live on plan->device: launching with another device current would make the
+  // kernels read a different GPU's memory.
+  return check_current_device(plan->device);
+}
+
+int check_current_device(int device) {
+  int dev = -1;
+  YASF_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev != device) {
+    set_error_text("the current CUDA device (" + std::to_string(dev) +
+                   ") is not the device the plan was created on (" + std::to_string(device) + ")");
+    return YASF_ERR_INVALID_ARGUMENT;
+  }
   return YASF_OK;
 }
 
@@ -140,6 +160,8 @@ int coupling_column(const yasf_plan* plan, int n_particles, const double* positi
   }
   ca.partial = partial;
   ca.err = err;
+  ca.poll_limit = stall_hook().contract_polls;
+  ca.stall = stall_hook().role == YASF_STALL_CONTRACT ? 1 : 0;
   int st = dispatch_contract(plan->lmax, precision, regular, ca, lay.tiles, lay.chunks,
                              lay.threads, stream);
   if (st != YASF_OK) return st;
@@ -235,6 +257,19 @@ extern "C" const char* yasf_status_string(int status) {
 }
 
 extern "C" const char* yasf_last_cuda_error(void) { return g_last_error.c_str(); }
+
+extern "C" int yasf_test_stall(int role, int contract_polls, double panel_wait_seconds) {
+  if (role < YASF_STALL_NONE || role > YASF_STALL_DPANEL) return YASF_ERR_INVALID_ARGUMENT;
+  if (contract_polls < 0 || !(panel_wait_seconds >= 0.0) || panel_wait_seconds > 10.0)
+    return YASF_ERR_INVALID_ARGUMENT;
+  StallHook h;
+  h.role = role;
+  if (contract_polls > 0) h.contract_polls = contract_polls;
+  if (panel_wait_seconds > 0.0)
+    h.panel_wait_ns = std::max(1000ull, (unsigned long long)(panel_wait_seconds * 1e9));
+  g_stall = h;
+  return YASF_OK;
+}
 
 extern "C" unsigned long long yasf_kernel_launches(void) {
   return g_launches.load(std::memory_order_relaxed);

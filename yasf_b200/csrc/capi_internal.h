@@ -82,6 +82,19 @@ int dispatch_contract(int lmax, int precision, bool regular, const ContractArgs&
 int validate_coupling(const yasf_plan* plan, int n_particles, const double* positions,
                       double k, int precision);
 
+// YASF_OK when `device` is the current CUDA device, else YASF_ERR_INVALID_ARGUMENT with an error
+// text (objects' device memory must not be used with another device current).
+int check_current_device(int device);
+
+// Wait bounds and the withheld role of the next launches from this host thread (set by
+// yasf_test_stall; defaults: nothing withheld, 2^22 polls, one second).
+struct StallHook {
+  int role = YASF_STALL_NONE;
+  int contract_polls = 1 << 22;
+  unsigned long long panel_wait_ns = 1000000000ull;
+};
+const StallHook& stall_hook();
+
 int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::vector<unsigned>& goff,
                       std::vector<unsigned>& dst);
 int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std::vector<int2>& items,

@@ -43,11 +43,12 @@ template <typename Real> struct Cplx;
 template <> struct Cplx<double> { using T = double2; };
 template <> struct Cplx<float> { using T = float2; };
 
-// Stage reads: the V stream sits in shared memory (plain loads; __ldg is global-only).
-template <typename Real>
-__device__ __forceinline__ typename Cplx<Real>::T load_c(const typename Cplx<Real>::T* p) {
-  return *p;
-}
+// One entry of the V stream. Float64: (re, im). Complex64: (re, im, -im, re), 16 bytes, so that
+// one broadcast shared load feeds a complex multiply-add as two packed FP32 FMAs (FFMA2):
+//   (y_re, y_im) += (g_re, g_re) * (re, im) + (g_im, g_im) * (-im, re).
+template <typename Real> struct VEntry;
+template <> struct VEntry<double> { using T = double2; };
+template <> struct VEntry<float> { using T = float4; };
 
 // ---------------------------------------------------------------------------------------------
 // Source side: V[bundle][s][entry] = sum_terms coef * x[s][n2].
@@ -64,12 +65,12 @@ struct VBuildArgs {
   const int* term_n2;            // source mode index of each term
   const double2* term_coef;      // complex coefficient of each term
   const double2* x;              // source coefficients (complex128), column base
-  void* v;                       // output stream buffer (Real2)
+  void* v;                       // output stream buffer (VEntry<Real>)
 };
 
 template <typename Real>
 __global__ void __launch_bounds__(256) vbuild_kernel(VBuildArgs a) {
-  using C = typename Cplx<Real>::T;
+  using C = typename VEntry<Real>::T;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= a.total_entries) return;
   int b = 0;
@@ -90,10 +91,11 @@ __global__ void __launch_bounds__(256) vbuild_kernel(VBuildArgs a) {
     }
     C* out = reinterpret_cast<C*>(a.v) + (size_t)a.bundle_begin[b] * a.n_particles +
              (size_t)s * a.bundle_len[b] + (g - a.bundle_begin[b]);
-    C val;
-    val.x = (Real)re;
-    val.y = (Real)im;
-    *out = val;
+    if constexpr (sizeof(Real) == 8) {
+      *out = make_double2(re, im);
+    } else {
+      *out = make_float4((float)re, (float)im, -(float)im, (float)re);
+    }
   }
 }
 
@@ -148,12 +150,15 @@ struct ContractArgs {
   int sources_per_chunk;
   double k;
   const double* pos;             // (N,3)
-  const void* v;                 // stream buffer (Real2), bundle-major
+  const void* v;                 // stream buffer (VEntry<Real>), bundle-major
   const LegendreTables* leg;     // device Legendre recurrence constants
   int bundle_begin[8];           // stream offset of each bundle (entries, per-source layout)
   int bundle_len[8];             // padded stream length per source
   void* partial;                 // (chunks, N, nmax) Real2 partial sums
   int* err;                      // set to 1 if a shared-memory stage wait timed out
+  int poll_limit;                // polls of one stage wait before it gives up (2^22 normally)
+  int stall;                     // test hook: 1 = the first stage copy of every block is never
+                                 // issued, so its wait runs out (0 normally)
 };
 
 // ---- bulk async copy (TMA, non-tensor) into shared memory with an mbarrier --------------------
@@ -179,11 +184,12 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
 }
-// Bounded wait for phase `parity` of `bar`; returns false after ~2^22 polls.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+// Bounded wait for phase `parity` of `bar`; returns false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity,
+                                          int limit = 1 << 22) {
   const unsigned a = smem_addr(bar);
 #pragma unroll 1
-  for (int spin = 0; spin < (1 << 22); ++spin) {
+  for (int spin = 0; spin < limit; ++spin) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -200,6 +206,8 @@ template <int L, int BID, typename Real, bool REGULAR>
 __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
                                               unsigned long long* bars) {
   using C = typename Cplx<Real>::T;
+  using VE = typename VEntry<Real>::T;
+  constexpr bool F64 = sizeof(Real) == 8;
   constexpr BundleInfo bi = make_bundle(L, BID);
   constexpr int NR = bi.rows;
   constexpr int PMAX = 2 * L;
@@ -211,25 +219,36 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
   const double y1 = __ldg(a.pos + 3 * s1c + 1);
   const double z1 = __ldg(a.pos + 3 * s1c + 2);
 
-  Real yr[NR], yi[NR];
+  // accumulators: float64 as separate real / imaginary arrays, complex64 as packed float2 pairs
+  Real yr[F64 ? NR : 1], yi[F64 ? NR : 1];
+  float2 yc[F64 ? 1 : NR];
 #pragma unroll
-  for (int r = 0; r < NR; ++r) { yr[r] = (Real)0; yi[r] = (Real)0; }
+  for (int r = 0; r < NR; ++r) {
+    if constexpr (F64) { yr[r] = (Real)0; yi[r] = (Real)0; }
+    else yc[r] = make_float2(0.f, 0.f);
+  }
 
   const int c = blockIdx.y;
   const int sb = c * a.sources_per_chunk;
   const int se = min(a.n_particles, sb + a.sources_per_chunk);
-  const C* vbase = reinterpret_cast<const C*>(a.v) + (size_t)a.bundle_begin[BID] * a.n_particles;
+  const VE* vbase = reinterpret_cast<const VE*>(a.v) + (size_t)a.bundle_begin[BID] * a.n_particles;
   const int vstride = a.bundle_len[BID];
-  const unsigned stage_bytes = (unsigned)(vstride * sizeof(C));
-  C* const stage0 = reinterpret_cast<C*>(smem);
-  C* const stage1 = stage0 + vstride;
+  const unsigned stage_bytes = (unsigned)(vstride * sizeof(VE));
+  VE* const stage0 = reinterpret_cast<VE*>(smem);
+  VE* const stage1 = stage0 + vstride;
   if (threadIdx.x == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     mbar_fence_init();
   }
   __syncthreads();
-  if (threadIdx.x == 0 && sb < se) bulk_load(stage0, vbase + (size_t)sb * vstride, stage_bytes, &bars[0]);
+  // Thread 0 issues every stage copy and remembers, per stage, the iteration whose copy it issued
+  // last (-1: none), so that a block that gives up drains exactly the copies still in flight.
+  int issued_it[2] = {-1, -1};
+  if (threadIdx.x == 0 && sb < se && !a.stall) {
+    bulk_load(stage0, vbase + (size_t)sb * vstride, stage_bytes, &bars[0]);
+    issued_it[0] = 0;
+  }
   bool timed_out = false;
   int last_it = 0;
 
@@ -239,9 +258,11 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     const int cur = it & 1;
     // prefetch the next source's stream into the other stage (read last in iteration it-1,
     // released by the barrier at the end of that iteration)
-    if (threadIdx.x == 0 && s2 + 1 < se)
+    if (threadIdx.x == 0 && s2 + 1 < se) {
       bulk_load(cur ? stage0 : stage1, vbase + (size_t)(s2 + 1) * vstride, stage_bytes,
                 &bars[cur ^ 1]);
+      issued_it[cur ^ 1] = it + 1;
+    }
     // ---- pair geometry: d = pos[s1] - pos[s2] (yasfpy/functions/misc.py:149-166) ----
     const double dx = x1 - __ldg(a.pos + 3 * s2 + 0);
     const double dy = y1 - __ldg(a.pos + 3 * s2 + 1);
@@ -280,14 +301,14 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     }
 
     // block-uniform decision: every thread polls (bounded), then all agree before using the stage
-    const bool ok = mbar_wait(&bars[cur], (unsigned)((it >> 1) & 1));
+    const bool ok = mbar_wait(&bars[cur], (unsigned)((it >> 1) & 1), a.poll_limit);
     if (__syncthreads_or(!ok)) {
       timed_out = true;
       last_it = it;
       if (threadIdx.x == 0) atomicExch(a.err, 1);
       break;
     }
-    const C* vp = cur ? stage1 : stage0;
+    const VE* vp = cur ? stage1 : stage0;
     const Real ctR = (Real)ct, stR = (Real)st;
     const Real eR = (Real)ephr, eI = (Real)ephi;
     Real st_d = (Real)1, ph_r = (Real)1, ph_i = (Real)0;
@@ -338,6 +359,11 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
           if (sgn == 1 && d == 0) break;
           const Real gr = sgn == 0 ? gpr : gmr;
           const Real gi = sgn == 0 ? gpi : gmi;
+          float2 grr, gii;  // (g_re, g_re), (g_im, g_im): packed FMA operands (complex64 only)
+          if constexpr (!F64) {
+            grr = make_float2((float)gr, (float)gr);
+            gii = make_float2((float)gi, (float)gi);
+          }
 #pragma unroll
           for (int i = 0; i < bi.count; ++i) {
             const int m1 = bi.m1[i];
@@ -348,11 +374,16 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
 #pragma unroll
             for (int rr = 0; rr < 2 * L; ++rr) {
               if (rr < rows_of_m(L, m1) && rr < nv) {
-                const C v = load_c<Real>(vp + rr);
-                yr[off + rr] = fma(gr, v.x, yr[off + rr]);
-                yr[off + rr] = fma(-gi, v.y, yr[off + rr]);
-                yi[off + rr] = fma(gr, v.y, yi[off + rr]);
-                yi[off + rr] = fma(gi, v.x, yi[off + rr]);
+                const VE v = vp[rr];  // shared-memory stage (plain load; __ldg is global-only)
+                if constexpr (F64) {
+                  yr[off + rr] = fma(gr, v.x, yr[off + rr]);
+                  yr[off + rr] = fma(-gi, v.y, yr[off + rr]);
+                  yi[off + rr] = fma(gr, v.y, yi[off + rr]);
+                  yi[off + rr] = fma(gi, v.x, yi[off + rr]);
+                } else {
+                  yc[off + rr] = __ffma2_rn(grr, make_float2(v.x, v.y), yc[off + rr]);
+                  yc[off + rr] = __ffma2_rn(gii, make_float2(v.z, v.w), yc[off + rr]);
+                }
               }
             }
             vp += nv;
@@ -375,12 +406,16 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     __syncthreads();  // every warp is done with this stage before it is refilled
   }
   if (timed_out) {
-    // give the copies still in flight (stage of iteration last_it and the prefetch for
-    // last_it + 1) a bounded chance to land before the block exits
+    // No copy may still be landing in shared memory when the block exits. Iterations before
+    // last_it consumed their stages, so a copy is outstanding exactly where thread 0 issued one
+    // for iteration last_it or later; wait (bounded) for each of those. Should a drain itself run
+    // out, the block exits with that copy's state undefined; the error word is already set and the
+    // result is poisoned.
     if (threadIdx.x == 0) {
-      (void)mbar_wait(&bars[last_it & 1], (unsigned)((last_it >> 1) & 1));
-      if (sb + last_it + 1 < se)
-        (void)mbar_wait(&bars[(last_it + 1) & 1], (unsigned)(((last_it + 1) >> 1) & 1));
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        if (issued_it[b] >= last_it)
+          (void)mbar_wait(&bars[b], (unsigned)((issued_it[b] >> 1) & 1));
     }
     return;
   }
@@ -395,8 +430,12 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
         if (rr < rows_of_m(L, m1)) {
           const int n1 = mode_index(L, row_tau(rr), row_l(L, rr), m1);
           C val;
-          val.x = yr[bi.row_off[i] + rr];
-          val.y = yi[bi.row_off[i] + rr];
+          if constexpr (F64) {
+            val.x = yr[bi.row_off[i] + rr];
+            val.y = yi[bi.row_off[i] + rr];
+          } else {
+            val = yc[bi.row_off[i] + rr];
+          }
           out[n1] = val;
         }
       }

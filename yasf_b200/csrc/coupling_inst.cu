@@ -15,7 +15,7 @@ cudaError_t launch_contract<YASF_INST_L>(int precision, bool regular, const Cont
   constexpr int L = YASF_INST_L;
   const dim3 grid(tiles, chunks, num_bundles(L));
   const size_t stage64 = 2 * (size_t)max_bundle_stream<L>() * sizeof(double2);
-  const size_t stage32 = 2 * (size_t)max_bundle_stream<L>() * sizeof(float2);
+  const size_t stage32 = 2 * (size_t)max_bundle_stream<L>() * sizeof(float4);
   cudaError_t e;
   if (regular) {
     e = cudaFuncSetAttribute(contract_kernel<L, double, true>,

@@ -74,6 +74,9 @@ struct DpArgs {
   const double2* tmat;       // T, master epilogue when non-null
   double2* y;
   int* err;
+  unsigned long long wait_ns;  // bound of one wait (1 s normally)
+  int stall;                   // test hook: 1 = the helper warp never delivers a pair table, so the
+                               // workers' waits run out (0 normally)
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -185,7 +188,8 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
     // worker warp takes the same branch and no warp is left waiting at a barrier.
     for (int t = 0; t < n_iter; ++t) {
       const int st = t & 1, sx = t % XS;
-      if (tid == 0) go[0] = wait_or_abort(&tfull[st], (unsigned)((t >> 1) & 1), abort_flag) ? 1 : 0;
+      if (tid == 0)
+        go[0] = wait_or_abort(&tfull[st], (unsigned)((t >> 1) & 1), abort_flag, a.wait_ns) ? 1 : 0;
       named_sync(1, NWT);
       if (!go[0]) break;
       const double2* T = reinterpret_cast<const double2*>(ts + st * G::T_STAGE);
@@ -228,7 +232,8 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
         W[mq2 * HR + mq1] = make_double2(ma.x + mb.y, ma.y - mb.x);
         W[(H + mq2) * HR + mq1] = make_double2(ma.x - mb.y, ma.y + mb.x);
       }
-      if (tid == 0) go[1] = wait_or_abort(&xfull[sx], (unsigned)((t / XS) & 1), abort_flag) ? 1 : 0;
+      if (tid == 0)
+        go[1] = wait_or_abort(&xfull[sx], (unsigned)((t / XS) & 1), abort_flag, a.wait_ns) ? 1 : 0;
       named_sync(1, NWT);  // W complete, source tile decision published
       if (tid == 0) mbar_arrive(&tfree[st]);
       if (!go[1]) break;
@@ -336,12 +341,13 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
     // tile is copied once the apply of pair t - XS has released its stage. With one tile stage the
     // table of pair t + 1 is computed while the workers generate and apply pair t.
     const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
-    for (int t = 0; t < n_iter; ++t) {
+    for (int t = 0; t < n_iter && !a.stall; ++t) {
       const int st = t & 1, sx = t % XS;
       const int j = t < i ? t : t + 1;
       int ok = 1;
       if (lane == 0)
-        ok = t < 2 ? !*abort_flag : wait_or_abort(&tfree[st], (unsigned)(((t >> 1) - 1) & 1), abort_flag);
+        ok = t < 2 ? !*abort_flag
+                   : wait_or_abort(&tfree[st], (unsigned)(((t >> 1) - 1) & 1), abort_flag, a.wait_ns);
       __syncwarp();
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
@@ -352,7 +358,8 @@ __global__ void __launch_bounds__(DpGeom<L, CT>::THREADS, 1) dpanel_kernel(DpArg
       if (lane == 0) {
         mbar_arrive(&tfull[st]);
         ok = t < XS ? !*abort_flag
-                    : wait_or_abort(&xfree[sx], (unsigned)(((t / XS) - 1) & 1), abort_flag);
+                    : wait_or_abort(&xfree[sx], (unsigned)(((t / XS) - 1) & 1), abort_flag,
+                                    a.wait_ns);
         if (ok) {
           issued[sx] = t;
           bulk_load(xs + sx * G::X_STAGE,
@@ -590,6 +597,8 @@ extern "C" int yasf_dpanel_matvec(const yasf_plan* plan, int n_particles, const 
   da.tmat = reinterpret_cast<const double2*>(tmat);
   da.y = reinterpret_cast<double2*>(y);
   da.err = err;
+  da.wait_ns = stall_hook().panel_wait_ns;
+  da.stall = stall_hook().role == YASF_STALL_DPANEL ? 1 : 0;
   switch (plan->lmax) {
     case 1: return launch_dpanel<1>(da, s);
     case 2: return launch_dpanel<2>(da, s);

@@ -18,7 +18,11 @@
 //   order them on one stream.
 // - The first call on each device looks up the array's device address with that device current
 //   (cudaGetSymbolAddress, which may load the module); make that first call before any stream
-//   capture begins.
+//   capture begins. The address is cached together with the unique id of the CUDA context it was
+//   looked up in: after cudaDeviceReset (or any other teardown of the primary context) the next
+//   call sees a new context id and looks the address up again instead of using a stale one.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "capi_internal.h"
@@ -31,18 +35,68 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 void* g_scratch_ptr[kMaxDevices] = {nullptr};
+unsigned long long g_scratch_ctx[kMaxDevices] = {0};
 
-// Device address of the static scratch for the current device (looked up once per device).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id (for the life of the process) of the CUDA context current on this thread. The driver
+// functions are fetched through the runtime, so the library needs no link against libcuda.
+int current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static int looked_up = 0;
+  if (!looked_up) {
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    YASF_CUDA_TRY(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1));
+    YASF_CUDA_TRY(cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2));
+    if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      set_error_text("driver lacks cuCtxGetCurrent / cuCtxGetId");
+      return YASF_ERR_CUDA;
+    }
+    get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    looked_up = 1;
+  }
+  CUcontext ctx = nullptr;
+  *id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS) {
+    set_error_text("cuCtxGetCurrent failed");
+    return YASF_ERR_CUDA;
+  }
+  if (!ctx) return YASF_OK;  // no context bound to this thread yet: id 0
+  if (get_id(ctx, id) != CUDA_SUCCESS) {
+    set_error_text("cuCtxGetId failed");
+    return YASF_ERR_CUDA;
+  }
+  return YASF_OK;
+}
+
+// Device address of the static scratch for the current device, looked up once per device and
+// context (g_scratch_mu also guards the one-time driver lookup above).
 int static_scratch(void** out) {
   int dev = -1;
   YASF_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return YASF_ERR_UNSUPPORTED;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+  unsigned long long ctx = 0;
+  if (int st = current_context_id(&ctx)) return st;
+  if (ctx == 0 || !g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
+    // binds the device's primary context to this thread if no runtime call did so yet
     YASF_CUDA_TRY(cudaGetSymbolAddress(&p, g_static_scratch));
     if (!p) return YASF_ERR_CUDA;
+    if (ctx == 0) {
+      if (int st = current_context_id(&ctx)) return st;
+      if (ctx == 0) {
+        set_error_text("no CUDA context current after the symbol lookup");
+        return YASF_ERR_CUDA;
+      }
+    }
     g_scratch_ptr[dev] = p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_ptr[dev];
   return YASF_OK;

@@ -279,6 +279,8 @@ extern "C" int yasf_panel_matvec(const yasf_plan* plan, int n_particles, const d
   pa.tmat = reinterpret_cast<const double2*>(tmat);
   pa.y = reinterpret_cast<double2*>(y);
   pa.err = err;
+  pa.wait_ns = stall_hook().panel_wait_ns;
+  pa.stall = stall_hook().role == YASF_STALL_PANEL ? 1 : 0;
   const int groups = (nrhs + 63) / 64;
   switch (plan->lmax) {
     case 1: return launch_panel<1>(pa, groups, s);

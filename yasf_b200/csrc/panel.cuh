@@ -129,6 +129,9 @@ struct PanelArgs {
   const double2* tmat;           // T (N*nmax), master epilogue when non-null
   double2* y;                    // output columns
   int* err;
+  unsigned long long wait_ns;    // bound of one wait (1 s normally)
+  int stall;                     // test hook: 1 = the pair-table warps never deliver a table, so
+                                 // the generation warps' waits run out (0 normally)
 };
 
 // ---- tcgen05 helpers -------------------------------------------------------------------------
@@ -198,10 +201,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Wait for phase `parity` of `bar`, bounded in time (about one second) rather than in polls.
-// Each try_wait may suspend the thread for up to 2 us (it resumes when the phase completes), so
-// waiting warps take few issue slots.
-__device__ __forceinline__ bool panel_wait(unsigned long long* bar, unsigned parity) {
+// Wait for phase `parity` of `bar`, bounded in time (`bound_ns`, one second unless a launch asks
+// for less) rather than in polls. Each try_wait may suspend the thread for up to 2 us (it resumes
+// when the phase completes), so waiting warps take few issue slots.
+__device__ __forceinline__ bool panel_wait(unsigned long long* bar, unsigned parity,
+                                           unsigned long long bound_ns = 1000000000ull) {
   const unsigned a = smem_addr(bar);
   unsigned long long t0 = 0;
 #pragma unroll 1
@@ -216,7 +220,7 @@ __device__ __forceinline__ bool panel_wait(unsigned long long* bar, unsigned par
     if (done) return true;
     if (spin == 0) {
       t0 = global_ns();
-    } else if ((spin & 7) == 0 && global_ns() - t0 > 1000000000ull) {
+    } else if ((spin & 7) == 0 && global_ns() - t0 > bound_ns) {
       return false;
     }
   }
@@ -224,9 +228,10 @@ __device__ __forceinline__ bool panel_wait(unsigned long long* bar, unsigned par
 
 // Bounded wait that also gives up when another role has already aborted.
 __device__ __forceinline__ bool wait_or_abort(unsigned long long* bar, unsigned parity,
-                                              volatile int* abort_flag) {
+                                              volatile int* abort_flag,
+                                              unsigned long long bound_ns = 1000000000ull) {
   if (*abort_flag) return false;
-  if (panel_wait(bar, parity)) return true;
+  if (panel_wait(bar, parity, bound_ns)) return true;
   *abort_flag = 1;
   return false;
 }
@@ -481,8 +486,9 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       const int sw = t % WS, sg = t & 3;
       int ok = 1;
       if (lane == 0) {
-        ok = (t < WS || wait_or_abort(&wempty[sw], (unsigned)(((t / WS) - 1) & 1), abort_flag)) &&
-             wait_or_abort(&gfull[sg], (unsigned)((t >> 2) & 1), abort_flag);
+        ok = (t < WS || wait_or_abort(&wempty[sw], (unsigned)(((t / WS) - 1) & 1), abort_flag,
+                                      a.wait_ns)) &&
+             wait_or_abort(&gfull[sg], (unsigned)((t >> 2) & 1), abort_flag, a.wait_ns);
       }
       __syncwarp();  // orders the other lanes' reads after lane 0's acquire
       ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -527,13 +533,13 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       bool stop = false;
       for (int t = 0; t < n_iter && !stop; ++t) {
         const int sw = t % WS;
-        if (!wait_or_abort(&wfull[sw], (unsigned)((t / WS) & 1), abort_flag)) break;
+        if (!wait_or_abort(&wfull[sw], (unsigned)((t / WS) & 1), abort_flag, a.wait_ns)) break;
         const unsigned long long dw = db0 + (unsigned long long)sw * (unsigned long long)(G::W_STAGE >> 4);
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           const int u = t * NG + g;  // source-panel unit: pair t, group g
           const int sx = u % XS;
-          if (!wait_or_abort(&xfull[sx], (unsigned)((u / XS) & 1), abort_flag)) {
+          if (!wait_or_abort(&xfull[sx], (unsigned)((u / XS) & 1), abort_flag, a.wait_ns)) {
             stop = true;
             break;
           }
@@ -562,7 +568,9 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
         const int sx = u % XS;
         const int j = t < i ? t : t + 1;
         if (*abort_flag) break;
-        if (u >= XS && !wait_or_abort(&xempty[sx], (unsigned)(((u / XS) - 1) & 1), abort_flag)) break;
+        if (u >= XS &&
+            !wait_or_abort(&xempty[sx], (unsigned)(((u / XS) - 1) & 1), abort_flag, a.wait_ns))
+          break;
         const unsigned char* src =
             reinterpret_cast<const unsigned char*>(a.xp) + ((size_t)(grp0 + g) * N + j) * G::X_STAGE;
         issued[sx] = u;  // written before the copy: the next load into this stage waits for its MMAs
@@ -575,13 +583,14 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
     const int par = warp - kGeomWarp0;
     const double xi = a.pos[3 * i], yi = a.pos[3 * i + 1], zi = a.pos[3 * i + 2];
     const float kf = (float)a.k;
-    for (int t = par; t < n_iter; t += 2) {
+    for (int t = par; t < n_iter && !a.stall; t += 2) {
       const int sg = t & 3;
       const int j = t < i ? t : t + 1;
       int ok = 1;
       if (lane == 0)
         ok = t < 4 ? !*abort_flag
-                   : wait_or_abort(&gempty[sg], (unsigned)(((t >> 2) - 1) & 1), abort_flag);
+                   : wait_or_abort(&gempty[sg], (unsigned)(((t >> 2) - 1) & 1), abort_flag,
+                                   a.wait_ns);
       __syncwarp();
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
@@ -631,7 +640,7 @@ __global__ void __launch_bounds__(kPanelThreads, 1) panel_kernel(PanelArgs a) {
       for (int b = 0; b < XS; ++b)
         if (issued[b] >= 0) (void)panel_wait(&xfull[b], (unsigned)((issued[b] / XS) & 1));
     // wait (bounded) for the MMAs before reading tensor memory
-    const bool ok = n_iter == 0 || panel_wait(accum, 0);
+    const bool ok = n_iter == 0 || panel_wait(accum, 0, a.wait_ns);
     tc_fence_after();
     named_sync(1, 128);  // the drain above precedes every write to the exchange buffer
     const bool aborted = *abort_flag != 0;

@@ -304,6 +304,7 @@ extern "C" int yasf_precond_assemble(yasf_precond* pc, const double* positions, 
   if (!std::isfinite(k_medium) || k_medium <= 0.0) return YASF_ERR_UNSUPPORTED;
   if (!aligned16(tmat)) return YASF_ERR_ALIGNMENT;
   const yasf_plan* plan = pc->plan;
+  if (int st = check_current_device(plan->device)) return st;
   AsmArgs a{};
   a.L = plan->lmax;
   a.nmax = plan->nmax;
@@ -366,6 +367,7 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
   if (nrhs > 1 && ld < n) return YASF_ERR_INVALID_ARGUMENT;
   if (nrhs == 1) ld = n;
   if (!aligned16(x) || !aligned16(y)) return YASF_ERR_ALIGNMENT;
+  if (int st = check_current_device(pc->plan->device)) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int blocks = (pc->total_rows + 7) / 8;
   const double2* xx = reinterpret_cast<const double2*>(x);

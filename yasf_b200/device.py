@@ -263,16 +263,27 @@ class DevicePreconditioner:
                  ctypes.byref(handle))
         self.handle = handle
 
-    def prepare(self, tmat: torch.Tensor) -> None:
+    def prepare(self, tmat: torch.Tensor) -> dict:
+        """Assemble, invert and finalize every block; returns the seconds of each phase."""
+        import time
+
+        t0 = time.perf_counter()
         call("yasf_precond_assemble", self.handle, _ptr(self.dev.pos), self.dev.k, _ptr(tmat),
              _stream_ptr())
+        torch.cuda.synchronize(self.dev.device)
+        t1 = time.perf_counter()
         for b in range(len(self.blocks)):
             ptr = ctypes.c_void_p()
             dim = ctypes.c_int()
             call("yasf_precond_block", self.handle, b, ctypes.byref(ptr), ctypes.byref(dim))
             blk = _wrap_device_matrix(ptr.value, dim.value, self.dev.device)
             blk.copy_(torch.linalg.inv(blk))
+        torch.cuda.synchronize(self.dev.device)
+        t2 = time.perf_counter()
         call("yasf_precond_finalize", self.handle, _stream_ptr())
+        torch.cuda.synchronize(self.dev.device)
+        t3 = time.perf_counter()
+        return {"assemble_s": t1 - t0, "factor_s": t2 - t1, "finalize_s": t3 - t2}
 
     def block_matrix(self, b: int) -> torch.Tensor:
         ptr = ctypes.c_void_p()
