@@ -47,3 +47,32 @@ def rel_err(a, b) -> float:
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def reference_package_root():
+    """Directory holding the reference ``yasfpy`` package: $YASF_REFERENCE, else the local
+    install under baseline/_ref (git-ignored). None when neither is present."""
+    import os
+
+    for cand in (os.environ.get("YASF_REFERENCE"), str(REPO / "baseline" / "_ref")):
+        if cand and (Path(cand) / "yasfpy" / "simulation.py").exists():
+            return Path(cand)
+    return None
+
+
+@pytest.fixture(scope="session")
+def reference_yasfpy(tmp_path_factory):
+    """Import the reference's own ``yasfpy`` (with the oracle's stand-ins for its third-party
+    modules: exact 3j for pywigxjpf, inert refidxdb / pyperf) or skip with the reason."""
+    import os
+
+    root = reference_package_root()
+    if root is None:
+        pytest.skip("reference yasfpy not importable here (no $YASF_REFERENCE, no baseline/_ref)")
+    for p in (str(REPO / "oracle" / "stubs"), str(root)):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    os.environ["HOME"] = str(tmp_path_factory.mktemp("yasfpy_home"))
+    import yasfpy  # noqa: F401
+
+    return root
