@@ -176,6 +176,17 @@ int yasf_batched_solve(const yasf_plan* plan, int n_particles, const double* pos
                        size_t workspace_bytes, double* stats, double* column_residuals,
                        void* stream);
 
+/* ---- right-hand sides of R plane-wave incidences ---------------------------------------------
+ * Replaces compute_initial_field_coefficients for plane waves (yasfpy/initial_field_coefficients.py:
+ * 79-142) and compute_right_hand_side (yasfpy/simulation.py:189-205) for R incidences at once:
+ * a[r][s*nmax + n] = coef[r][n] e^{i kvec_r . (pos_s - focal_point)}, b = tmat (.) a.
+ * coef (device, nrhs x nmax complex128): 4 E0 e^{-i m alpha_r} B^dagger_{tau l m}(beta_r) per incidence;
+ * kvec (device, nrhs x 3): the wave vectors; focal_point: host (3,) or NULL for the origin; positions:
+ * device (N, 3). a or b may be NULL (b needs tmat). Columns have leading dimension ld. Asynchronous. */
+int yasf_plane_wave_rhs(int lmax, int n_particles, const double* positions, int nrhs,
+                        const double* kvec, const double* coef, const double* focal_point,
+                        const double* tmat, double* a, double* b, long long ld, void* stream);
+
 /* ---- cross sections (yasfpy/optics.py:55-156) ------------------------------------------------
  * out[0..1] (device) <- sum_{s,n} conj(b) (W_reg b), the bilinear form of
  * compute_scattering_cross_section (yasfpy/functions/cpu_numba.py:410-457): regular spherical
@@ -190,9 +201,12 @@ int yasf_dotc(long long n, const double* a, const double* b, double* out, void* 
 /* ---- block-Jacobi preconditioner (yasfpy/preconditioner.py:58-219) ---------------------------
  * Blocks are given as a particle list per block (CSR: block_ptr[n_blocks+1], particles[]); the
  * library assembles M_B = (I - T W)[B,B] on the device with the same generator as the matvec
- * (particle-major rows and columns, receiver Mie factor), the caller replaces every block by its
- * inverse in place (any dense complex128 inversion on the device, e.g. a cuSOLVER getrf/getrs),
- * and finalize makes the complex64 copy used by YASF_C64 applications.
+ * (particle-major rows and columns, receiver Mie factor), factors every block in place with its own
+ * batched LU (yasf_precond_factor) and keeps, after finalize, the complex64 factors the solves
+ * stream. Protocol: create -> assemble -> factor -> finalize -> apply (any number of times).
+ * (A caller may instead invert every block in place between assemble and finalize, with any dense
+ * complex128 inversion; finalize then keeps complex128 and complex64 copies of those inverses and
+ * apply streams them.)
  * apply: y = M^{-1} x, block by block (x and y must not alias). */
 int yasf_precond_create(const yasf_plan* plan, int n_particles, int n_blocks,
                         const int* block_ptr /*host*/, const int* particles /*host*/,
@@ -202,11 +216,27 @@ int yasf_precond_destroy(yasf_precond* pc);
 int yasf_precond_assemble(yasf_precond* pc, const double* positions, double k_medium,
                           const double* tmat, void* stream);
 /* Device pointer and order of block `block`: row-major (dim, dim) complex128, dim = n_B*nmax,
- * rows/columns in the block's particle order, particle-major inside. */
+ * rows/columns in the block's particle order, particle-major inside. Available from assemble until
+ * a finalize that releases the complex128 factors (YASF_ERR_NOT_PREPARED afterwards). */
 int yasf_precond_block(const yasf_precond* pc, int block, double** matrix, int* dim);
-/* Call after every block holds its inverse. */
+/* Replaces the block LU of prepare() (yasfpy/preconditioner.py:445-468, scipy.linalg.lu on complex64
+ * blocks): every block factored in place in complex128, P_B M_B = L_B U_B, by a right-looking tile LU
+ * (64 x 64 tiles, partial pivoting inside each diagonal tile, so P_B permutes rows only within each
+ * tile row); all blocks of the preconditioner in one sequence of launches. Asynchronous. */
+int yasf_precond_factor(yasf_precond* pc, void* stream);
+/* Whether finalize keeps the complex128 factors beside the complex64 copy (default 0: released,
+ * halving the resident bytes; YASF_C128 applies then also stream the complex64 factors). */
+int yasf_precond_keep_float64(yasf_precond* pc, int keep);
+/* Call after factor (or after the caller's in-place inversion). Makes the complex64 copy and, after
+ * factor, the inverses of the diagonal tiles of L and U; YASF_ERR_NOT_FINITE for a zero pivot.
+ * Synchronises the stream. */
 int yasf_precond_finalize(yasf_precond* pc, void* stream);
-/* Replaces BlockDiagonalPreconditioner.apply (yasfpy/preconditioner.py:177-219). */
+/* Replaces BlockDiagonalPreconditioner.apply (yasfpy/preconditioner.py:177-219, the unit-lower and
+ * upper triangular solves of :470-519): gather with the pivots, a forward sweep with L and a
+ * backward sweep with U over tile rows (one launch per tile row, float64 arithmetic on the complex64
+ * factors, or the complex128 ones when kept and precision is YASF_C128), scatter. The first apply with
+ * more columns than any before allocates the preconditioner's sweep buffer; applies of ONE
+ * preconditioner on different streams at the same time race on that buffer. */
 int yasf_precond_apply(const yasf_precond* pc, const double* x, double* y, int nrhs, long long ld,
                        int precision, void* stream);
 /* Device bytes held by the factors. */

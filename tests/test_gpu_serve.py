@@ -66,3 +66,23 @@ def test_mixed_precision_extinction_within_target(cuda_device):
         assert st["info"] == 0
         c64 = -np.real(np.vdot(a[:, :, c].ravel(), x.cpu().numpy())) / agg.k**2 * np.pi
         assert abs(res.c_ext[c] - c64) <= 1e-6 * abs(c64)
+
+
+def test_admission_footprint_covers_the_device_memory_of_a_request(cuda_device):
+    """The admission footprint (the library's workspace query plus the request's vectors) is at
+    least the device memory a request's solve allocates, and not grossly more."""
+    from yasf_b200.serve import footprint_bytes
+
+    cfg = ServeConfig(max_slots=1, rtol=1e-6)
+    for req in _requests()[:4]:
+        fp = footprint_bytes(req, cfg, cuda_device)
+        solve_request(req, cfg, cuda_device)  # plans, kernels and caches set up
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        base = torch.cuda.memory_allocated(cuda_device)
+        torch.cuda.reset_peak_memory_stats(cuda_device)
+        solve_request(req, cfg, cuda_device)
+        torch.cuda.synchronize()
+        peak = torch.cuda.max_memory_allocated(cuda_device) - base
+        assert peak <= fp, (req.rid, peak, fp)
+        assert fp <= 2 * peak + (16 << 20), (req.rid, peak, fp)

@@ -102,7 +102,7 @@ def test_preconditioner_blocks_match_reference(golden, cuda_device):
         assert rel_err(M, g[f"block{b}"]) < 1e-12
     with pytest.raises(YasfError):
         pc.apply(torch.zeros(dev.n, dtype=torch.complex128, device=cuda_device))  # not finalized
-    pc.prepare(tmat)
+    pc.prepare(tmat, keep_float64=True)  # the library's block LU; complex128 factors kept
     rng = np.random.default_rng(0)
     y = rng.normal(size=dev.n) + 1j * rng.normal(size=dev.n)
     # M y block by block, then apply(M y) must return y

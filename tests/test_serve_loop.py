@@ -90,3 +90,31 @@ def test_inner_kind_rule():
     assert [inner_kind(6, r) for r in (1, 2, 3, 64)] == ["c64", "c64", "tf32", "tf32"]
     assert [inner_kind(7, r) for r in (4, 5)] == ["c64", "tf32"]
     assert [inner_kind(8, r) for r in (3, 4, 64)] == ["c64", "tf32", "tf32"]
+
+
+def test_admission_never_exceeds_the_budget():
+    """Random footprints and durations: at every moment the footprints of the requests in flight
+    sum to at most the budget, and every request that fits alone is served."""
+    rng = np.random.default_rng(4)
+    budget = 1000
+    fp = {i: int(rng.integers(50, 600)) for i in range(40)}
+    lock = threading.Lock()
+    state = {"used": 0, "peak": 0}
+
+    def solve(req, cfg, device):
+        with lock:
+            state["used"] += fp[req.rid]
+            state["peak"] = max(state["peak"], state["used"])
+            assert state["used"] <= budget
+        time.sleep(float(rng.uniform(0.0, 0.01)))
+        with lock:
+            state["used"] -= fp[req.rid]
+        agg = req.aggregate
+        return RequestResult(req.rid, agg.n, agg.lmax, len(req.pol), c_ext=np.zeros(len(req.pol)))
+
+    reqs = [_req(i, 0.001 * i) for i in range(40)]
+    srv = Server(ServeConfig(max_slots=8, hbm_budget_bytes=budget), device="cpu", solve_fn=solve,
+                 footprint_fn=lambda r, c: fp[r.rid])
+    res = srv.run(reqs)
+    assert all(r.error is None for r in res)
+    assert state["peak"] <= budget and state["peak"] > 600  # several in flight at once

@@ -59,6 +59,7 @@ SIGNATURES = {
     "yasf_last_cuda_error": [],
     "yasf_kernel_launches": [],
     "yasf_test_stall": [_i, _i, _d],
+    "yasf_plane_wave_rhs": [_i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _vp],
     "yasf_plan_create": [_i, _vp, _c.POINTER(_vp)],
     "yasf_plan_destroy": [_vp],
     "yasf_plan_info": [_vp, _c.POINTER(_i), _c.POINTER(_ll), _c.POINTER(_ll)],
@@ -81,6 +82,8 @@ SIGNATURES = {
     "yasf_precond_assemble": [_vp, _vp, _d, _vp, _vp],
     "yasf_precond_block": [_vp, _i, _c.POINTER(_vp), _c.POINTER(_i)],
     "yasf_precond_finalize": [_vp, _vp],
+    "yasf_precond_factor": [_vp, _vp],
+    "yasf_precond_keep_float64": [_vp, _i],
     "yasf_precond_apply": [_vp, _vp, _vp, _i, _ll, _i, _vp],
     "yasf_precond_bytes": [_vp, _c.POINTER(_sz)],
     "yasf_gmres_workspace_size": [_vp, _i, _i, _i, _c.POINTER(_sz)],

@@ -1,0 +1,480 @@
+// Batched LU factorisation of the block-Jacobi blocks and the triangular sweeps that apply it.
+//
+// The reference factors each block with LU and applies it by a unit-lower then an upper
+// triangular solve (yasfpy/preconditioner.py:445-519, scipy.linalg.lu on complex64 blocks,
+// :391). Here every block of one preconditioner is factored on the device in one sequence of
+// launches (variable block orders batched together), in complex128, in place:
+//
+//   right-looking tile LU, tiles of kLuT = 64 rows / columns. Step k factors the diagonal tile
+//   with partial pivoting inside it (its 64 rows; the interchanges are applied to the whole tile
+//   row, left and right), solves the tile row for U and the tile column for L, and updates the
+//   trailing tiles A_ij -= L_ik U_kj. The result is P A = L U with P block diagonal (a permutation
+//   within each tile row). Pivoting inside the diagonal tile rather than over the whole column
+//   keeps every step parallel over tiles; on the blocks of I - T W the growth factor stays near 1.
+//
+// Each step is three launches over all blocks that still have a tile k; host-built prefix sums
+// (one row per step) map a CTA index to (block, tile). Ragged edges (block order not a multiple of
+// 64) are padded with the identity in the diagonal tile and zeros elsewhere; padded entries are
+// never stored.
+//
+// Apply (finalize keeps only a complex64 copy of the factors plus the complex64 inverses of the
+// diagonal tiles of L and U, and frees the complex128 matrices): z = P x gathered from the
+// particle-major vector, forward sweep with L, backward sweep with U, scattered back. Sweep step
+// s of the forward pass: every tile row i >= s subtracts L_{i,s-1} z_{s-1} (z_{s-1} was finished
+// by the previous launch), and tile row s then multiplies by L_ss^{-1}; the backward pass mirrors
+// it. One launch per step, no inter-CTA waits, no atomics: every element is written by one CTA per
+// launch in a fixed order, so the apply is deterministic. Arithmetic is float64 throughout.
+#pragma once
+
+#include "capi_internal.h"
+
+namespace yasf {
+
+constexpr int kLuT = 64;        // tile order
+constexpr int kLuS = kLuT + 1;  // shared-memory row stride (complex128), breaks bank conflicts
+
+struct LuGeom {
+  const long long* mat_off;  // element offset of block b's matrix (row-major, order dim[b])
+  const int* dim;            // order of block b
+  const int* row0;           // first flattened row of block b
+  const int* tile0;          // first flattened diagonal tile of block b
+  int n_blocks;
+};
+
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 c_sub_mul(double2 c, double2 a, double2 b) {  // c - a b
+  return make_double2(c.x - (a.x * b.x - a.y * b.y), c.y - (a.x * b.y + a.y * b.x));
+}
+__device__ __forceinline__ double2 c_inv(double2 d, bool* zero) {
+  const double m = d.x * d.x + d.y * d.y;
+  if (m == 0.0) { *zero = true; return make_double2(0.0, 0.0); }
+  return make_double2(d.x / m, -d.y / m);
+}
+
+// Block of work item `item` given the prefix sums pre[0..n_blocks] of one step.
+__device__ __forceinline__ int lu_block_of(const int* pre, int n_blocks, int item) {
+  int lo = 0, hi = n_blocks;  // pre[lo] <= item < pre[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= item) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int lu_tiles(int dim) { return (dim + kLuT - 1) / kLuT; }
+
+// ---- step k, part 1: the diagonal tile, partial pivoting inside it -----------------------------
+// piv[row0 + k*64 + r] = local source row (0..63) of row r after the interchanges.
+__global__ void __launch_bounds__(256) lu_diag_kernel(LuGeom g, const int* pre, int k, double2* mat,
+                                                      int* piv, int* err) {
+  extern __shared__ double2 lu_smem[];
+  double2* t = lu_smem;  // [64][kLuS]
+  __shared__ int perm[kLuT];
+  __shared__ int pivrow;
+  __shared__ int singular;
+  const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
+  const int dim = g.dim[b];
+  const int k0 = k * kLuT;
+  const int v = min(kLuT, dim - k0);
+  double2* A = mat + g.mat_off[b];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+    const int r = e >> 6, c = e & 63;
+    t[r * kLuS + c] = (r < v && c < v) ? A[(size_t)(k0 + r) * dim + k0 + c]
+                                       : make_double2(r == c ? 1.0 : 0.0, 0.0);
+  }
+  if (tid < kLuT) perm[tid] = tid;
+  if (tid == 0) singular = 0;
+  for (int c = 0; c < kLuT; ++c) {
+    __syncthreads();
+    if (warp == 0) {
+      // argmax |t[r][c]|, r >= c (ties: the smaller row)
+      double best = -1.0;
+      int br = c;
+      for (int r = c + lane; r < kLuT; r += 32) {
+        const double2 x = t[r * kLuS + c];
+        const double m = x.x * x.x + x.y * x.y;
+        if (m > best) { best = m; br = r; }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, off);
+        const int orow = __shfl_down_sync(0xffffffffu, br, off);
+        if (ob > best || (ob == best && orow < br)) { best = ob; br = orow; }
+      }
+      if (lane == 0) pivrow = br;
+    }
+    __syncthreads();
+    const int p = pivrow;
+    if (p != c) {
+      if (tid < kLuT) {
+        const double2 a = t[c * kLuS + tid];
+        t[c * kLuS + tid] = t[p * kLuS + tid];
+        t[p * kLuS + tid] = a;
+      }
+      if (tid == 0) {
+        const int q = perm[c];
+        perm[c] = perm[p];
+        perm[p] = q;
+      }
+      __syncthreads();
+    }
+    bool zero = false;
+    const double2 inv = c_inv(t[c * kLuS + c], &zero);
+    if (zero && tid == 0) singular = 1;
+    const int rem = kLuT - 1 - c;
+    if (tid < rem) {
+      const int r = c + 1 + tid;
+      t[r * kLuS + c] = c_mul(t[r * kLuS + c], inv);
+    }
+    __syncthreads();
+    for (int e = tid; e < rem * rem; e += blockDim.x) {
+      const int r = c + 1 + e / rem, j = c + 1 + e % rem;
+      t[r * kLuS + j] = c_sub_mul(t[r * kLuS + j], t[r * kLuS + c], t[c * kLuS + j]);
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+    const int r = e >> 6, c = e & 63;
+    if (r < v && c < v) A[(size_t)(k0 + r) * dim + k0 + c] = t[r * kLuS + c];
+  }
+  if (tid < v) piv[g.row0[b] + k0 + tid] = perm[tid];
+  if (tid == 0 && singular) atomicExch(err, 1);
+}
+
+// ---- step k, part 2: tile row k (interchanges; U_kj = L_kk^{-1} P A_kj) and tile column k
+// (L_ik = A_ik U_kk^{-1}) --------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre, int k, double2* mat,
+                                                       const int* piv) {
+  extern __shared__ double2 lu_smem[];
+  double2* X = lu_smem;               // [64][kLuS] the tile being solved
+  double2* D = lu_smem + kLuT * kLuS;  // [64][kLuS] the factored diagonal tile
+  const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
+  const int item = blockIdx.x - pre[b];
+  const int dim = g.dim[b];
+  const int nt = lu_tiles(dim);
+  const int k0 = k * kLuT;
+  const int vk = min(kLuT, dim - k0);
+  double2* A = mat + g.mat_off[b];
+  const int tid = threadIdx.x;
+  const int nrow = nt - 1;
+  if (item < nrow) {
+    // tile (k, j), j != k: rows interchanged; for j > k then solved with the unit lower L_kk
+    const int j = item < k ? item : item + 1;
+    const int j0 = j * kLuT, vj = min(kLuT, dim - j0);
+    const int* p = piv + g.row0[b] + k0;
+    for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+      const int r = e >> 6, c = e & 63;
+      X[r * kLuS + c] = (r < vk && c < vj) ? A[(size_t)(k0 + p[r]) * dim + j0 + c] : make_double2(0.0, 0.0);
+    }
+    if (j > k) {
+      for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+        const int r = e >> 6, c = e & 63;
+        D[r * kLuS + c] = (r < vk && c < vk) ? A[(size_t)(k0 + r) * dim + k0 + c] : make_double2(0.0, 0.0);
+      }
+      for (int c = 0; c < vk; ++c) {
+        __syncthreads();
+        const int rem = vk - 1 - c;
+        for (int e = tid; e < rem * vj; e += blockDim.x) {
+          const int r = c + 1 + e / vj, col = e % vj;
+          X[r * kLuS + col] = c_sub_mul(X[r * kLuS + col], D[r * kLuS + c], X[c * kLuS + col]);
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+      const int r = e >> 6, c = e & 63;
+      if (r < vk && c < vj) A[(size_t)(k0 + r) * dim + j0 + c] = X[r * kLuS + c];
+    }
+  } else {
+    // tile (i, k), i > k: X U_kk = A_ik
+    const int i = k + 1 + (item - nrow);
+    const int i0 = i * kLuT, vi = min(kLuT, dim - i0);
+    for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+      const int r = e >> 6, c = e & 63;
+      X[r * kLuS + c] = (r < vi && c < vk) ? A[(size_t)(i0 + r) * dim + k0 + c] : make_double2(0.0, 0.0);
+      D[r * kLuS + c] = (r < vk && c < vk) ? A[(size_t)(k0 + r) * dim + k0 + c] : make_double2(0.0, 0.0);
+    }
+    for (int c = 0; c < vk; ++c) {
+      __syncthreads();
+      bool zero = false;
+      const double2 inv = c_inv(D[c * kLuS + c], &zero);  // zero pivots were flagged by the diag step
+      if (tid < vi) X[tid * kLuS + c] = c_mul(X[tid * kLuS + c], inv);
+      __syncthreads();
+      const int rem = vk - 1 - c;
+      for (int e = tid; e < vi * rem; e += blockDim.x) {
+        const int r = e / rem, jj = c + 1 + e % rem;
+        X[r * kLuS + jj] = c_sub_mul(X[r * kLuS + jj], X[r * kLuS + c], D[c * kLuS + jj]);
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+      const int r = e >> 6, c = e & 63;
+      if (r < vi && c < vk) A[(size_t)(i0 + r) * dim + k0 + c] = X[r * kLuS + c];
+    }
+  }
+}
+
+// ---- step k, part 3: trailing update A_ij -= L_ik U_kj for i, j > k ----------------------------
+// 256 threads, 4 x 4 outputs each (rows ty + 16p, columns tx + 16q); the inner dimension is
+// staged in two chunks of 32 (L transposed, U as is).
+constexpr int kLuKc = 32;
+constexpr size_t kLuUpdateSmem = 2 * (size_t)kLuKc * kLuS * sizeof(double2);
+__global__ void __launch_bounds__(256, 2) lu_update_kernel(LuGeom g, const int* pre, int k, double2* mat) {
+  extern __shared__ double2 lu_smem[];
+  double2(*Ls)[kLuS] = reinterpret_cast<double2(*)[kLuS]>(lu_smem);                 // Ls[kk][row] = L_ik[row][kc + kk]
+  double2(*Us)[kLuS] = reinterpret_cast<double2(*)[kLuS]>(lu_smem + kLuKc * kLuS);  // Us[kk][col] = U_kj[kc + kk][col]
+  const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
+  const int item = blockIdx.x - pre[b];
+  const int dim = g.dim[b];
+  const int nt = lu_tiles(dim);
+  const int nc = nt - k - 1;
+  const int i = k + 1 + item / nc, j = k + 1 + item % nc;
+  const int k0 = k * kLuT, i0 = i * kLuT, j0 = j * kLuT;
+  const int vk = min(kLuT, dim - k0), vi = min(kLuT, dim - i0), vj = min(kLuT, dim - j0);
+  double2* A = mat + g.mat_off[b];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double2 acc[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[p][q] = make_double2(0.0, 0.0);
+  for (int kc = 0; kc < vk; kc += kLuKc) {
+    __syncthreads();
+    for (int e = tid; e < kLuT * kLuKc; e += blockDim.x) {
+      const int r = e / kLuKc, kk = e % kLuKc;  // L: consecutive threads along the row
+      Ls[kk][r] = (r < vi && kc + kk < vk) ? A[(size_t)(i0 + r) * dim + k0 + kc + kk] : make_double2(0.0, 0.0);
+      const int kk2 = e / kLuT, c = e % kLuT;   // U: consecutive threads along the row
+      Us[kk2][c] = (kc + kk2 < vk && c < vj) ? A[(size_t)(k0 + kc + kk2) * dim + j0 + c]
+                                             : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < kLuKc; ++kk) {
+      double2 l[4], u[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) l[p] = Ls[kk][ty + 16 * p];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) u[q] = Us[kk][tx + 16 * q];
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[p][q].x = fma(l[p].x, u[q].x, acc[p][q].x);
+          acc[p][q].x = fma(-l[p].y, u[q].y, acc[p][q].x);
+          acc[p][q].y = fma(l[p].x, u[q].y, acc[p][q].y);
+          acc[p][q].y = fma(l[p].y, u[q].x, acc[p][q].y);
+        }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int r = ty + 16 * p;
+    if (r >= vi) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = tx + 16 * q;
+      if (c >= vj) continue;
+      double2* a = A + (size_t)(i0 + r) * dim + j0 + c;
+      const double2 o = *a;
+      *a = make_double2(o.x - acc[p][q].x, o.y - acc[p][q].y);
+    }
+  }
+}
+
+// ---- finalize: complex64 factors and the inverses of the diagonal tiles ------------------------
+// dinv[(tile0[b] + t) * 2 + 0] = L_tt^{-1} (unit lower), [.. + 1] = U_tt^{-1}, each 64 x 64
+// row-major complex64 (identity in the padded part); dinv64 (may be null) the same in complex128.
+__global__ void __launch_bounds__(256) lu_diag_inverse_kernel(LuGeom g, const int* pre, const double2* mat,
+                                                              float2* dinv, double2* dinv64, int* err) {
+  extern __shared__ double2 lu_smem[];
+  double2* D = lu_smem;                // [64][kLuS] factored diagonal tile
+  double2* X = lu_smem + kLuT * kLuS;  // [64][kLuS] inverse under construction
+  const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
+  const int t = blockIdx.x - pre[b];
+  const int dim = g.dim[b];
+  const int t0 = t * kLuT, v = min(kLuT, dim - t0);
+  const double2* A = mat + g.mat_off[b];
+  const int tid = threadIdx.x;
+  __shared__ int singular;
+  if (tid == 0) singular = 0;
+  for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+    const int r = e >> 6, c = e & 63;
+    D[r * kLuS + c] = (r < v && c < v) ? A[(size_t)(t0 + r) * dim + t0 + c] : make_double2(r == c ? 1.0 : 0.0, 0.0);
+    X[r * kLuS + c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+  }
+  // L X = I (unit lower): row c of X is final before rows below use it
+  for (int c = 0; c < kLuT; ++c) {
+    __syncthreads();
+    const int rem = kLuT - 1 - c;
+    for (int e = tid; e < rem * kLuT; e += blockDim.x) {
+      const int r = c + 1 + e / kLuT, col = e % kLuT;
+      X[r * kLuS + col] = c_sub_mul(X[r * kLuS + col], D[r * kLuS + c], X[c * kLuS + col]);
+    }
+  }
+  __syncthreads();
+  const size_t obase = (size_t)(g.tile0[b] + t) * 2 * kLuT * kLuT;
+  float2* out = dinv + obase;
+  for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+    const int r = e >> 6, c = e & 63;
+    const double2 x = X[r * kLuS + c];
+    out[e] = make_float2((float)x.x, (float)x.y);
+    if (dinv64) dinv64[obase + e] = x;
+    X[r * kLuS + c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+  }
+  // U X = I: rows from the bottom
+  for (int c = kLuT - 1; c >= 0; --c) {
+    __syncthreads();
+    bool zero = false;
+    const double2 inv = c_inv(D[c * kLuS + c], &zero);
+    if (zero && tid == 0) singular = 1;
+    if (tid < kLuT) X[c * kLuS + tid] = c_mul(X[c * kLuS + tid], inv);
+    __syncthreads();
+    for (int e = tid; e < c * kLuT; e += blockDim.x) {
+      const int r = e / kLuT, col = e % kLuT;
+      X[r * kLuS + col] = c_sub_mul(X[r * kLuS + col], D[r * kLuS + c], X[c * kLuS + col]);
+    }
+  }
+  __syncthreads();
+  out += kLuT * kLuT;
+  for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
+    const double2 x = X[(e >> 6) * kLuS + (e & 63)];
+    out[e] = make_float2((float)x.x, (float)x.y);
+    if (dinv64) dinv64[obase + kLuT * kLuT + e] = x;
+  }
+  if (tid == 0 && singular) atomicExch(err, 1);
+}
+
+// ---- apply ---------------------------------------------------------------------------------------
+// z[row0[b] + r][col] = x[col][global index of block-local row (r & ~63) + piv[row0[b] + r]]
+__global__ void lu_gather_kernel(int total_rows, int nmax, int nrhs, long long ld, const int* row_block,
+                                 const int* row_local, const int* block_ptr, const int* particles,
+                                 const int* row0, const int* piv, const double2* x, double2* z) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)total_rows * nrhs;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(e % total_rows), col = (int)(e / total_rows);
+    const int b = row_block[q], r = row_local[q];
+    const int src = (r & ~(kLuT - 1)) + piv[q];
+    const int gi = particles[block_ptr[b] + src / nmax] * nmax + src % nmax;
+    z[(size_t)col * total_rows + q] = x[(size_t)col * ld + gi];
+  }
+}
+
+__global__ void lu_scatter_kernel(int total_rows, int nmax, int nrhs, long long ld, const int* row_block,
+                                  const int* row_local, const int* block_ptr, const int* particles,
+                                  const double2* z, double2* y) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)total_rows * nrhs;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(e % total_rows), col = (int)(e / total_rows);
+    const int b = row_block[q], r = row_local[q];
+    const int gi = particles[block_ptr[b] + r / nmax] * nmax + r % nmax;
+    y[(size_t)col * ld + gi] = z[(size_t)col * total_rows + q];
+  }
+}
+
+// One step of a sweep. Forward (upper = 0), launch s: tile rows i = s .. nt-1 of every block with
+// s < nt: z_i -= L_{i,s-1} z_{s-1} (s > 0), then z_s = L_ss^{-1} z_s. Backward (upper = 1), launch
+// t, s = nt - 1 - t: tile rows i = 0 .. s: z_i -= U_{i,s+1} z_{s+1} (t > 0), then z_s = U_ss^{-1} z_s.
+// 256 threads: thread (row = tid >> 2, part = tid & 3) sums 16 of the 64 products of its row; the
+// four parts are combined by shuffles. Right-hand sides are processed kLuCols at a time.
+// FT: float2 (the complex64 factors the solves stream) or double2 (complex128 factors, when kept).
+constexpr int kLuCols = 8;
+template <typename FT>
+__global__ void __launch_bounds__(256) lu_sweep_kernel(LuGeom g, const int* pre, int step, int upper,
+                                                       const FT* lu, const FT* dinv, int nrhs,
+                                                       int total_rows, double2* z) {
+  __shared__ double2 zin[kLuCols][kLuT];   // z of the eliminated tile row
+  __shared__ double2 zacc[kLuCols][kLuT];  // the diagonal tile row before its inverse is applied
+  const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
+  const int item = blockIdx.x - pre[b];
+  const int dim = g.dim[b];
+  const int nt = lu_tiles(dim);
+  const int s = upper ? nt - 1 - step : step;        // diagonal tile row of this step
+  const int i = upper ? item : s + item;              // tile row of this CTA
+  const int e_tile = upper ? s + 1 : s - 1;           // tile row eliminated in this step
+  const bool has_e = step > 0;
+  const int i0 = i * kLuT, vi = min(kLuT, dim - i0);
+  const int e0 = e_tile * kLuT, ve = has_e ? min(kLuT, dim - e0) : 0;
+  const FT* M = lu + g.mat_off[b];
+  const int tid = threadIdx.x, row = tid >> 2, part = tid & 3;
+  const size_t zb = g.row0[b];
+  for (int c0 = 0; c0 < nrhs; c0 += kLuCols) {
+    const int nc = min(kLuCols, nrhs - c0);
+    __syncthreads();
+    if (has_e)
+      for (int e = tid; e < kLuCols * kLuT; e += blockDim.x) {
+        const int cc = e / kLuT, r = e % kLuT;
+        zin[cc][r] = (cc < nc && r < ve) ? z[(size_t)(c0 + cc) * total_rows + zb + e0 + r] : make_double2(0.0, 0.0);
+      }
+    __syncthreads();
+    double2 acc[kLuCols];
+#pragma unroll
+    for (int cc = 0; cc < kLuCols; ++cc) acc[cc] = make_double2(0.0, 0.0);
+    if (has_e && row < vi) {
+      const FT* mr = M + (size_t)(i0 + row) * dim + e0;
+#pragma unroll 4
+      for (int q = part; q < ve; q += 4) {
+        const FT m = mr[q];
+        const double mx = m.x, my = m.y;
+#pragma unroll
+        for (int cc = 0; cc < kLuCols; ++cc) {
+          const double2 zv = zin[cc][q];
+          acc[cc].x = fma(mx, zv.x, fma(-my, zv.y, acc[cc].x));
+          acc[cc].y = fma(mx, zv.y, fma(my, zv.x, acc[cc].y));
+        }
+      }
+    }
+#pragma unroll
+    for (int cc = 0; cc < kLuCols; ++cc) {
+      acc[cc].x += __shfl_xor_sync(0xffffffffu, acc[cc].x, 1);
+      acc[cc].y += __shfl_xor_sync(0xffffffffu, acc[cc].y, 1);
+      acc[cc].x += __shfl_xor_sync(0xffffffffu, acc[cc].x, 2);
+      acc[cc].y += __shfl_xor_sync(0xffffffffu, acc[cc].y, 2);
+    }
+    if (i != s) {
+      if (part == 0 && row < vi)
+        for (int cc = 0; cc < nc; ++cc) {
+          double2* zp = z + (size_t)(c0 + cc) * total_rows + zb + i0 + row;
+          const double2 o = *zp;
+          *zp = make_double2(o.x - acc[cc].x, o.y - acc[cc].y);
+        }
+      continue;
+    }
+    // diagonal tile row: r = z_s - (eliminated part), then z_s = inverse(diagonal tile) r
+    if (part == 0)
+      for (int cc = 0; cc < kLuCols; ++cc) {
+        double2 o = make_double2(0.0, 0.0);
+        if (row < vi && cc < nc) o = z[(size_t)(c0 + cc) * total_rows + zb + i0 + row];
+        zacc[cc][row] = make_double2(o.x - acc[cc].x, o.y - acc[cc].y);
+      }
+    __syncthreads();
+    const FT* inv = dinv + ((size_t)(g.tile0[b] + s) * 2 + (upper ? 1 : 0)) * kLuT * kLuT + (size_t)row * kLuT;
+    double2 out[kLuCols];
+#pragma unroll
+    for (int cc = 0; cc < kLuCols; ++cc) out[cc] = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int q = part; q < kLuT; q += 4) {
+      const FT m = inv[q];
+      const double mx = m.x, my = m.y;
+#pragma unroll
+      for (int cc = 0; cc < kLuCols; ++cc) {
+        const double2 zv = zacc[cc][q];
+        out[cc].x = fma(mx, zv.x, fma(-my, zv.y, out[cc].x));
+        out[cc].y = fma(mx, zv.y, fma(my, zv.x, out[cc].y));
+      }
+    }
+#pragma unroll
+    for (int cc = 0; cc < kLuCols; ++cc) {
+      out[cc].x += __shfl_xor_sync(0xffffffffu, out[cc].x, 1);
+      out[cc].y += __shfl_xor_sync(0xffffffffu, out[cc].y, 1);
+      out[cc].x += __shfl_xor_sync(0xffffffffu, out[cc].x, 2);
+      out[cc].y += __shfl_xor_sync(0xffffffffu, out[cc].y, 2);
+    }
+    if (part == 0 && row < vi)
+      for (int cc = 0; cc < nc; ++cc) z[(size_t)(c0 + cc) * total_rows + zb + i0 + row] = out[cc];
+  }
+}
+
+}  // namespace yasf

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <new>
 
+#include "blocklu.cuh"
 #include "capi_internal.h"
 
 struct yasf_precond {
@@ -32,6 +33,24 @@ struct yasf_precond {
   size_t mat_elems = 0;
   bool assembled = false;
   bool prepared = false;
+  // batched LU (yasf_precond_factor): per-block geometry, per-step work prefix sums, pivots, the
+  // complex64 factors' diagonal-tile inverses (and complex128 ones when the float64 factors are
+  // kept), the sweep buffer of the apply
+  bool factored = false;   // blocks hold LU factors (else: the caller's inverses)
+  bool keep_f64 = false;   // finalize keeps the complex128 factors (yasf_precond_keep_float64)
+  int lu_steps = 0;        // tiles of the largest block
+  int n_tiles = 0;         // diagonal tiles of all blocks
+  std::vector<int> pre_diag, pre_panel, pre_update, pre_sweep;  // [step][n_blocks + 1]
+  int* d_dim = nullptr;
+  int* d_row0 = nullptr;
+  int* d_tile0 = nullptr;
+  int* d_pre = nullptr;    // the four prefix tables, one after the other
+  int* d_piv = nullptr;
+  int* d_err = nullptr;
+  float2* d_dinv = nullptr;
+  double2* d_dinv64 = nullptr;
+  double2* d_z = nullptr;
+  int z_cols = 0;
 };
 
 namespace yasf {
@@ -273,6 +292,44 @@ extern "C" int yasf_precond_create(const yasf_plan* plan, int n_particles, int n
   up(&pc->d_mat_off, pc->mat_off.data(), pc->mat_off.size());
   up(&pc->d_row_block, row_block.data(), row_block.size());
   up(&pc->d_row_local, row_local.data(), row_local.size());
+  // LU geometry: block orders, first rows, first diagonal tiles; per step k the prefix sums over
+  // blocks of the CTAs of the diagonal / panel / update launches and of sweep step k
+  {
+    std::vector<int> dims(n_blocks), row0(n_blocks), tile0(n_blocks);
+    int rows = 0, tiles = 0, steps = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+      dims[b] = (block_ptr[b + 1] - block_ptr[b]) * nmax;
+      row0[b] = rows;
+      tile0[b] = tiles;
+      rows += dims[b];
+      const int nt = (dims[b] + kLuT - 1) / kLuT;
+      tiles += nt;
+      steps = std::max(steps, nt);
+    }
+    pc->lu_steps = steps;
+    pc->n_tiles = tiles;
+    const int W = n_blocks + 1;
+    for (auto* v : {&pc->pre_diag, &pc->pre_panel, &pc->pre_update, &pc->pre_sweep}) v->assign((size_t)steps * W, 0);
+    for (int k = 0; k < steps; ++k)
+      for (int b = 0; b < n_blocks; ++b) {
+        const int nt = (dims[b] + kLuT - 1) / kLuT;
+        const int live = k < nt;
+        const int rest = live ? nt - k - 1 : 0;
+        pc->pre_diag[(size_t)k * W + b + 1] = pc->pre_diag[(size_t)k * W + b] + live;
+        pc->pre_panel[(size_t)k * W + b + 1] = pc->pre_panel[(size_t)k * W + b] + (live ? nt - 1 + rest : 0);
+        pc->pre_update[(size_t)k * W + b + 1] = pc->pre_update[(size_t)k * W + b] + rest * rest;
+        pc->pre_sweep[(size_t)k * W + b + 1] = pc->pre_sweep[(size_t)k * W + b] + (live ? nt - k : 0);
+      }
+    std::vector<int> pre;
+    for (auto* v : {&pc->pre_diag, &pc->pre_panel, &pc->pre_update, &pc->pre_sweep})
+      pre.insert(pre.end(), v->begin(), v->end());
+    up(&pc->d_dim, dims.data(), dims.size());
+    up(&pc->d_row0, row0.data(), row0.size());
+    up(&pc->d_tile0, tile0.data(), tile0.size());
+    up(&pc->d_pre, pre.data(), pre.size());
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&pc->d_piv), std::max(1, rows) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&pc->d_err), sizeof(int));
+  }
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&pc->d_mat), pc->mat_elems * sizeof(double2));
   if (e != cudaSuccess) {
     set_cuda_error(e);
@@ -294,7 +351,78 @@ extern "C" int yasf_precond_destroy(yasf_precond* pc) {
   cudaFree(pc->d_row_local);
   cudaFree(pc->d_mat);
   cudaFree(pc->d_mat32);
+  cudaFree(pc->d_dim);
+  cudaFree(pc->d_row0);
+  cudaFree(pc->d_tile0);
+  cudaFree(pc->d_pre);
+  cudaFree(pc->d_piv);
+  cudaFree(pc->d_err);
+  cudaFree(pc->d_dinv);
+  cudaFree(pc->d_dinv64);
+  cudaFree(pc->d_z);
   delete pc;
+  return YASF_OK;
+}
+
+namespace {
+yasf::LuGeom lu_geom(const yasf_precond* pc) {
+  yasf::LuGeom g;
+  g.mat_off = pc->d_mat_off;
+  g.dim = pc->d_dim;
+  g.row0 = pc->d_row0;
+  g.tile0 = pc->d_tile0;
+  g.n_blocks = pc->n_blocks;
+  return g;
+}
+// prefix table `which` (0 diag, 1 panel, 2 update, 3 sweep) of step k on the device, and its CTA count
+const int* lu_pre(const yasf_precond* pc, int which, int k, int* ctas) {
+  const size_t W = (size_t)pc->n_blocks + 1;
+  const std::vector<int>* v[4] = {&pc->pre_diag, &pc->pre_panel, &pc->pre_update, &pc->pre_sweep};
+  *ctas = (*v[which])[(size_t)k * W + pc->n_blocks];
+  return pc->d_pre + (size_t)which * pc->lu_steps * W + (size_t)k * W;
+}
+int lu_smem_attributes() {
+  static int done = 0;
+  if (done) return YASF_OK;
+  const int one = (int)(yasf::kLuT * yasf::kLuS * sizeof(double2));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     2 * one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)yasf::kLuUpdateSmem));
+  done = 1;
+  return YASF_OK;
+}
+}  // namespace
+
+extern "C" int yasf_precond_factor(yasf_precond* pc, void* stream) {
+  if (!pc) return YASF_ERR_INVALID_ARGUMENT;
+  if (!pc->assembled || !pc->d_mat) return YASF_ERR_NOT_PREPARED;
+  if (int st = check_current_device(pc->plan->device)) return st;
+  if (int st = lu_smem_attributes()) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const LuGeom g = lu_geom(pc);
+  const int one = (int)(kLuT * kLuS * sizeof(double2));
+  YASF_CUDA_TRY(cudaMemsetAsync(pc->d_err, 0, sizeof(int), s));
+  for (int k = 0; k < pc->lu_steps; ++k) {
+    int n = 0;
+    const int* pre = lu_pre(pc, 0, k, &n);
+    if (n) YASF_COUNTED(lu_diag_kernel<<<n, 256, one, s>>>(g, pre, k, pc->d_mat, pc->d_piv, pc->d_err));
+    pre = lu_pre(pc, 1, k, &n);
+    if (n) YASF_COUNTED(lu_panel_kernel<<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat, pc->d_piv));
+    pre = lu_pre(pc, 2, k, &n);
+    if (n) YASF_COUNTED(lu_update_kernel<<<n, 256, kLuUpdateSmem, s>>>(g, pre, k, pc->d_mat));
+    YASF_CUDA_TRY(cudaGetLastError());
+  }
+  pc->factored = true;
+  pc->prepared = false;
+  return YASF_OK;
+}
+
+extern "C" int yasf_precond_keep_float64(yasf_precond* pc, int keep) {
+  if (!pc) return YASF_ERR_INVALID_ARGUMENT;
+  pc->keep_f64 = keep != 0;
   return YASF_OK;
 }
 
@@ -305,6 +433,14 @@ extern "C" int yasf_precond_assemble(yasf_precond* pc, const double* positions, 
   if (!aligned16(tmat)) return YASF_ERR_ALIGNMENT;
   const yasf_plan* plan = pc->plan;
   if (int st = check_current_device(plan->device)) return st;
+  if (!pc->d_mat) {  // released by a finalize that kept only the complex64 factors
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&pc->d_mat), pc->mat_elems * sizeof(double2));
+    if (e != cudaSuccess) {
+      set_cuda_error(e);
+      pc->d_mat = nullptr;
+      return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
+    }
+  }
   AsmArgs a{};
   a.L = plan->lmax;
   a.nmax = plan->nmax;
@@ -330,11 +466,16 @@ extern "C" int yasf_precond_assemble(yasf_precond* pc, const double* positions, 
   YASF_CUDA_TRY(cudaGetLastError());
   pc->assembled = true;
   pc->prepared = false;
+  pc->factored = false;
   return YASF_OK;
 }
 
 extern "C" int yasf_precond_block(const yasf_precond* pc, int block, double** matrix, int* dim) {
   if (!pc || !matrix || !dim || block < 0 || block >= pc->n_blocks) return YASF_ERR_INVALID_ARGUMENT;
+  if (!pc->d_mat) {
+    set_error_text("the complex128 blocks were released by finalize");
+    return YASF_ERR_NOT_PREPARED;
+  }
   *matrix = reinterpret_cast<double*>(pc->d_mat + pc->mat_off[block]);
   *dim = (pc->block_ptr[block + 1] - pc->block_ptr[block]) * pc->plan->nmax;
   return YASF_OK;
@@ -342,18 +483,48 @@ extern "C" int yasf_precond_block(const yasf_precond* pc, int block, double** ma
 
 extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
   if (!pc) return YASF_ERR_INVALID_ARGUMENT;
-  if (!pc->assembled) return YASF_ERR_NOT_PREPARED;
+  if (!pc->assembled || !pc->d_mat) return YASF_ERR_NOT_PREPARED;
+  if (int st = check_current_device(pc->plan->device)) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (!pc->d_mat32) {
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&pc->d_mat32), pc->mat_elems * sizeof(float2));
+  auto alloc = [&](void** p, size_t bytes) -> int {
+    if (*p) return YASF_OK;
+    cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
       set_cuda_error(e);
-      pc->d_mat32 = nullptr;
+      *p = nullptr;
       return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
     }
-  }
+    return YASF_OK;
+  };
+  if (int st = alloc(reinterpret_cast<void**>(&pc->d_mat32), pc->mat_elems * sizeof(float2))) return st;
   YASF_COUNTED(to_c64_kernel<<<2048, 256, 0, s>>>(pc->mat_elems, pc->d_mat, pc->d_mat32));
   YASF_CUDA_TRY(cudaGetLastError());
+  if (pc->factored) {
+    if (int st = lu_smem_attributes()) return st;
+    const size_t tile_elems = (size_t)pc->n_tiles * 2 * kLuT * kLuT;
+    if (int st = alloc(reinterpret_cast<void**>(&pc->d_dinv), tile_elems * sizeof(float2))) return st;
+    if (pc->keep_f64)
+      if (int st = alloc(reinterpret_cast<void**>(&pc->d_dinv64), tile_elems * sizeof(double2))) return st;
+    int n = 0;
+    // every diagonal tile of every block: the sweep prefix of step 0 counts nt per block
+    const int* pre = lu_pre(pc, 3, 0, &n);
+    const int one = (int)(kLuT * kLuS * sizeof(double2));
+    YASF_COUNTED(lu_diag_inverse_kernel<<<n, 256, 2 * one, s>>>(lu_geom(pc), pre, pc->d_mat, pc->d_dinv,
+                                                                 pc->keep_f64 ? pc->d_dinv64 : nullptr,
+                                                                 pc->d_err));
+    YASF_CUDA_TRY(cudaGetLastError());
+    int err = 0;
+    YASF_CUDA_TRY(cudaMemcpyAsync(&err, pc->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    YASF_CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) {
+      set_error_text("a block has a zero pivot (singular diagonal tile)");
+      return YASF_ERR_NOT_FINITE;
+    }
+    if (!pc->keep_f64) {  // the solves stream the complex64 factors only
+      YASF_CUDA_TRY(cudaFree(pc->d_mat));
+      pc->d_mat = nullptr;
+    }
+  }
   pc->prepared = true;
   return YASF_OK;
 }
@@ -369,6 +540,45 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
   if (!aligned16(x) || !aligned16(y)) return YASF_ERR_ALIGNMENT;
   if (int st = check_current_device(pc->plan->device)) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (pc->factored) {
+    if (precision != YASF_C64 && precision != YASF_C128) return YASF_ERR_INVALID_ARGUMENT;
+    const bool f64 = precision == YASF_C128 && pc->d_mat && pc->d_dinv64;
+    if (nrhs > pc->z_cols) {  // the sweep buffer grows to the widest apply seen
+      double2* z = nullptr;
+      cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&z), (size_t)pc->total_rows * nrhs * sizeof(double2));
+      if (e != cudaSuccess) {
+        set_cuda_error(e);
+        return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
+      }
+      YASF_CUDA_TRY(cudaStreamSynchronize(s));
+      cudaFree(pc->d_z);
+      const_cast<yasf_precond*>(pc)->d_z = z;
+      const_cast<yasf_precond*>(pc)->z_cols = nrhs;
+    }
+    const int gb = (int)std::min<long long>(((long long)pc->total_rows * nrhs + 255) / 256, 8192);
+    YASF_COUNTED(lu_gather_kernel<<<gb, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld, pc->d_row_block,
+                                                     pc->d_row_local, pc->d_block_ptr, pc->d_particles,
+                                                     pc->d_row0, pc->d_piv, reinterpret_cast<const double2*>(x),
+                                                     pc->d_z));
+    const LuGeom g = lu_geom(pc);
+    for (int upper = 0; upper < 2; ++upper)
+      for (int step = 0; step < pc->lu_steps; ++step) {
+        int n = 0;
+        const int* pre = lu_pre(pc, 3, step, &n);
+        if (!n) continue;
+        if (f64)
+          YASF_COUNTED(lu_sweep_kernel<double2><<<n, 256, 0, s>>>(g, pre, step, upper, pc->d_mat, pc->d_dinv64,
+                                                                  nrhs, pc->total_rows, pc->d_z));
+        else
+          YASF_COUNTED(lu_sweep_kernel<float2><<<n, 256, 0, s>>>(g, pre, step, upper, pc->d_mat32, pc->d_dinv,
+                                                                 nrhs, pc->total_rows, pc->d_z));
+      }
+    YASF_COUNTED(lu_scatter_kernel<<<gb, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld, pc->d_row_block,
+                                                      pc->d_row_local, pc->d_block_ptr, pc->d_particles, pc->d_z,
+                                                      reinterpret_cast<double2*>(y)));
+    YASF_CUDA_TRY(cudaGetLastError());
+    return YASF_OK;
+  }
   const int blocks = (pc->total_rows + 7) / 8;
   const double2* xx = reinterpret_cast<const double2*>(x);
   double2* yy = reinterpret_cast<double2*>(y);
@@ -394,6 +604,9 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
 
 extern "C" int yasf_precond_bytes(const yasf_precond* pc, size_t* bytes) {
   if (!pc || !bytes) return YASF_ERR_INVALID_ARGUMENT;
-  *bytes = pc->mat_elems * (sizeof(double2) + (pc->d_mat32 ? sizeof(float2) : 0));
+  const size_t tiles = (size_t)pc->n_tiles * 2 * kLuT * kLuT;
+  *bytes = pc->mat_elems * ((pc->d_mat ? sizeof(double2) : 0) + (pc->d_mat32 ? sizeof(float2) : 0)) +
+           (pc->d_dinv ? tiles * sizeof(float2) : 0) + (pc->d_dinv64 ? tiles * sizeof(double2) : 0) +
+           (size_t)pc->total_rows * pc->z_cols * sizeof(double2);
   return YASF_OK;
 }

@@ -176,6 +176,23 @@ class CouplingDevice:
              _ptr(cols), _ptr(y), R, self.n, self.n, _ptr(ws), nb.value, _stream_ptr())
         return y.reshape(x.shape)
 
+    def plane_wave_rhs(self, tmat: torch.Tensor | None, polar, azimuthal, pol, amplitude: float = 1.0,
+                       focal_point=(0.0, 0.0, 0.0), want_a: bool = True):
+        """(A, B) for R plane-wave incidences on the device, each (R, n) complex128: the incident
+        coefficients a (or None) and the right-hand sides b = T (.) a (or None without tmat)."""
+        from yasf_b200.incident import plane_wave_mode_factors, wave_vectors
+
+        coef = plane_wave_mode_factors(self.lmax, polar, azimuthal, pol, amplitude)
+        R = coef.shape[0]
+        kv = torch.from_numpy(wave_vectors(polar, azimuthal, self.k)).to(self.device)
+        ct = torch.from_numpy(np.ascontiguousarray(coef)).to(self.device)
+        A = torch.empty((R, self.n), dtype=torch.complex128, device=self.device) if want_a else None
+        B = torch.empty((R, self.n), dtype=torch.complex128, device=self.device) if tmat is not None else None
+        f = np.ascontiguousarray(np.asarray(focal_point, dtype=np.float64).reshape(3))
+        call("yasf_plane_wave_rhs", self.lmax, self.n_particles, _ptr(self.pos), R, _ptr(kv), _ptr(ct),
+             f.ctypes.data_as(ctypes.c_void_p), _ptr(tmat), _ptr(A), _ptr(B), self.n, _stream_ptr())
+        return A, B
+
     INNER_KINDS = {"tf32": 0, "c64": 1, "c128": 2}
 
     def batched_solve(self, tmat: torch.Tensor, B: torch.Tensor, rtol: float, restart: int = 50,
@@ -263,27 +280,28 @@ class DevicePreconditioner:
                  ctypes.byref(handle))
         self.handle = handle
 
-    def prepare(self, tmat: torch.Tensor) -> dict:
-        """Assemble, invert and finalize every block; returns the seconds of each phase."""
+    def prepare(self, tmat: torch.Tensor, keep_float64: bool = False) -> dict:
+        """Assemble, factor (the library's batched block LU) and finalize every block; returns the
+        seconds of each phase. keep_float64 keeps the complex128 factors beside the complex64 copy
+        the solves stream."""
         import time
 
+        s = _stream_ptr()
         t0 = time.perf_counter()
-        call("yasf_precond_assemble", self.handle, _ptr(self.dev.pos), self.dev.k, _ptr(tmat),
-             _stream_ptr())
+        call("yasf_precond_assemble", self.handle, _ptr(self.dev.pos), self.dev.k, _ptr(tmat), s)
         torch.cuda.synchronize(self.dev.device)
         t1 = time.perf_counter()
-        for b in range(len(self.blocks)):
-            ptr = ctypes.c_void_p()
-            dim = ctypes.c_int()
-            call("yasf_precond_block", self.handle, b, ctypes.byref(ptr), ctypes.byref(dim))
-            blk = _wrap_device_matrix(ptr.value, dim.value, self.dev.device)
-            blk.copy_(torch.linalg.inv(blk))
+        call("yasf_precond_factor", self.handle, s)
         torch.cuda.synchronize(self.dev.device)
         t2 = time.perf_counter()
-        call("yasf_precond_finalize", self.handle, _stream_ptr())
-        torch.cuda.synchronize(self.dev.device)
+        call("yasf_precond_keep_float64", self.handle, 1 if keep_float64 else 0)
+        call("yasf_precond_finalize", self.handle, s)
         t3 = time.perf_counter()
         return {"assemble_s": t1 - t0, "factor_s": t2 - t1, "finalize_s": t3 - t2}
+
+    def assemble(self, tmat: torch.Tensor) -> None:
+        """Only the block assembly: every block holds M_B = (I - T W)[B, B] (see ``block_matrix``)."""
+        call("yasf_precond_assemble", self.handle, _ptr(self.dev.pos), self.dev.k, _ptr(tmat), _stream_ptr())
 
     def block_matrix(self, b: int) -> torch.Tensor:
         ptr = ctypes.c_void_p()

@@ -1,8 +1,10 @@
 """Plane-wave incident-field VSWF coefficients (yasfpy/initial_field_coefficients.py:79-142).
 
 ``spherical_functions_trigon`` restates yasfpy/functions/spherical_functions_trigon.py:11-96 and
-``transformation_coefficients`` restates yasfpy/functions/misc.py:70-114. ``plane_wave_block``
-evaluates R incidences (direction, polarisation) at once for the multi-right-hand-side solves.
+``transformation_coefficients`` restates yasfpy/functions/misc.py:70-114 (one mode, one incidence;
+kept for the host tests). ``plane_wave_mode_factors`` evaluates the same coefficients for R
+incidences at once (vectorised over incidences); ``plane_wave_block`` forms the host block from them,
+and ``CouplingDevice.plane_wave_rhs`` the same block and the right-hand sides on the device.
 """
 
 from __future__ import annotations
@@ -59,33 +61,53 @@ def mode_index(lmax: int, tau: int, l: int, m: int) -> int:
     return (tau - 1) * lmax * (lmax + 2) + (l - 1) * (l + 1) + l + m
 
 
-def plane_wave_block(lmax: int, positions: np.ndarray, k: complex, polar: np.ndarray,
-                     azimuthal: np.ndarray, pol: np.ndarray, amplitude: float = 1.0,
-                     focal_point=(0.0, 0.0, 0.0)) -> np.ndarray:
-    """Plane-wave coefficients a[s, n, r] for R incidences (complex128, (N, nmax, R))."""
+def plane_wave_mode_factors(lmax: int, polar, azimuthal, pol, amplitude: float = 1.0) -> np.ndarray:
+    """coef[r, n] = 4 E0 e^{-i m alpha_r} B^dagger_{tau l m}(beta_r): the sphere-independent factor
+    of the plane-wave coefficients of incidence r (yasfpy/initial_field_coefficients.py:79-142),
+    (R, nmax) complex128. Vectorised over incidences: one pass over the nmax modes."""
     polar = np.atleast_1d(np.asarray(polar, dtype=float))
     azimuthal = np.atleast_1d(np.asarray(azimuthal, dtype=float))
     pol = np.atleast_1d(np.asarray(pol, dtype=int))
     R = polar.size
-    N = positions.shape[0]
     nmax = 2 * lmax * (lmax + 2)
     pilm, taulm = spherical_functions_trigon(lmax, np.cos(polar), np.sin(polar))  # (L+1, L+1, R)
-    kvec = np.stack((np.sin(polar) * np.cos(azimuthal), np.sin(polar) * np.sin(azimuthal),
-                     np.cos(polar)), axis=0) * k  # (3, R)
+    coef = np.zeros((R, nmax), dtype=complex)
+    ifac = -1j  # B^dagger
+    for m in range(-lmax, lmax + 1):
+        phase = 4.0 * amplitude * np.exp(-1j * m * azimuthal)  # (R,)
+        for l in range(max(1, abs(m)), lmax + 1):
+            pre = -1.0 / np.power(ifac, l + 1) / np.sqrt(2 * l * (l + 1))
+            tau_l, pi_l = taulm[l, abs(m)], m * pilm[l, abs(m)]  # (R,)
+            for tau in (1, 2):
+                # TE (pol 1) / TM (pol 2): tau == pol selects tau_lm, else m pi_lm; unpolarised: mean
+                spher = np.where(pol == tau, tau_l, pi_l)
+                pfac = np.where(pol == 1, ifac, 1.0)
+                tc = pre * pfac * spher
+                unp = pre * (ifac + 1) * (tau_l + pi_l) / 2
+                tc = np.where((pol == 1) | (pol == 2), tc, unp)
+                coef[:, mode_index(lmax, tau, l, m)] = phase * tc
+    return coef
+
+
+def wave_vectors(polar, azimuthal, k: float) -> np.ndarray:
+    """(R, 3) wave vectors of the incidences (direction from the polar / azimuthal angles)."""
+    polar = np.atleast_1d(np.asarray(polar, dtype=float))
+    azimuthal = np.atleast_1d(np.asarray(azimuthal, dtype=float))
+    return np.ascontiguousarray(np.stack((np.sin(polar) * np.cos(azimuthal), np.sin(polar) * np.sin(azimuthal),
+                                          np.cos(polar)), axis=1) * float(np.real(k)))
+
+
+def plane_wave_block(lmax: int, positions: np.ndarray, k: complex, polar: np.ndarray,
+                     azimuthal: np.ndarray, pol: np.ndarray, amplitude: float = 1.0,
+                     focal_point=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Plane-wave coefficients a[s, n, r] for R incidences (complex128, (N, nmax, R)), host."""
+    coef = plane_wave_mode_factors(lmax, polar, azimuthal, pol, amplitude)  # (R, nmax)
+    kvec = np.stack((np.sin(np.atleast_1d(polar)) * np.cos(np.atleast_1d(azimuthal)),
+                     np.sin(np.atleast_1d(polar)) * np.sin(np.atleast_1d(azimuthal)),
+                     np.cos(np.atleast_1d(polar))), axis=0) * k  # (3, R)
     rel = positions - np.asarray(focal_point, dtype=float)
     eikr = np.exp(1j * (rel @ kvec))  # (N, R)
-    out = np.zeros((N, nmax, R), dtype=complex)
-    for m in range(-lmax, lmax + 1):
-        phase = np.exp(-1j * m * azimuthal)  # (R,)
-        for tau in (1, 2):
-            for l in range(max(1, abs(m)), lmax + 1):
-                n = mode_index(lmax, tau, l, m)
-                tc = np.empty(R, dtype=complex)
-                for r in range(R):
-                    tc[r] = transformation_coefficients(pilm[:, :, r], taulm[:, :, r], tau, l, m,
-                                                        int(pol[r]), dagger=True)
-                out[:, n, :] = 4 * amplitude * phase[None, :] * eikr * tc[None, :]
-    return out
+    return eikr[:, None, :] * coef.T[None, :, :]
 
 
 def compute_initial_field_coefficients(lmax: int, positions: np.ndarray, k_medium: np.ndarray,

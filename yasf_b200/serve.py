@@ -4,8 +4,8 @@ Each request carries an aggregate (spheres, refractive index, wavelength, lmax) 
 incidences (directions x polarisations = R right-hand sides). The loop:
 
 - admits a request once its arrival time has passed, a slot is free and its device footprint
-  (the Krylov bases of its R columns, its panels and workspaces) fits in the HBM budget that the
-  requests in flight leave; a request that can never fit is rejected with an error;
+  (the library's own workspace query for its batched solve, plus its vectors) fits in the HBM
+  budget that the requests in flight leave; a request that can never fit is rejected with an error;
 - runs every admitted request on its own CUDA stream, so the kernels of in-flight solves
   interleave on the device while their GMRES state stays resident there;
 - solves in mixed precision: the batched refined solve (yasf_batched_solve) with the tensor-core
@@ -32,7 +32,6 @@ import torch
 
 from yasf_b200._lib import call
 from yasf_b200.device import CouplingDevice
-from yasf_b200.incident import plane_wave_block
 from yasf_b200.mie import mie_tmatrix_per_sphere
 from yasf_b200.numerics import cached_translation_table
 from yasf_b200.workloads import Request
@@ -82,18 +81,41 @@ def inner_kind(lmax: int, nrhs: int) -> str:
     return "tf32" if lmax <= 8 and nrhs >= _PANEL_MIN_COLUMNS.get(lmax, 3) else "c64"
 
 
-def footprint_bytes(req: Request, cfg: ServeConfig, dev_plan_handle=None) -> int:
-    """Device bytes a request holds while in flight (workspace + its vectors)."""
+def footprint_bytes(req: Request, cfg: ServeConfig, device: torch.device | None = None) -> int:
+    """Device bytes a request holds while in flight, from the library's own size query.
+
+    The workspace of its refined batched solve is what ``yasf_batched_workspace_size`` returns for
+    the request's plan, sphere count, columns and restart length, taking the larger of the two inner
+    operators (TF32 panel, complex64 columns) when the autotuner may choose either; then its device
+    vectors: T (n), the incident coefficients, the right-hand sides and the solution (R n each,
+    complex128), the positions, the incidences' mode factors and wave vectors. Each allocation is
+    rounded up to the caching allocator's 2 MiB granularity. The translation plan is shared by every
+    request of the same lmax and not counted here."""
+    import ctypes
+
+    from yasf_b200.device import Plan
+
     agg = req.aggregate
     nmax = 2 * agg.lmax * (agg.lmax + 2)
     n = agg.n * nmax
     R = len(req.pol)
-    restart = min(cfg.restart, n)
-    # Krylov bases and panels dominate: R (m+1) n + 6 R n complex128 + source panels + V stream
-    basis = R * (restart + 1) * n * 16
-    panels = 6 * R * n * 16
-    v_stream = agg.n * nmax * 150 * 16 // 2  # per-source V stream (complex128), generous
-    return int(basis + panels + v_stream + (64 << 20))
+    restart = int(max(1, min(cfg.restart, 512, n)))
+    device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+    plan = Plan.get(agg.lmax, cached_translation_table(agg.lmax), device)
+    kinds = ("tf32", "c64") if cfg.tuner is not None else (inner_kind(agg.lmax, R),)
+    ws = 0
+    for kind in kinds:
+        nb = ctypes.c_size_t()
+        call("yasf_batched_workspace_size", plan.handle, agg.n, R, restart,
+             CouplingDevice.INNER_KINDS[kind], ctypes.byref(nb))
+        ws = max(ws, nb.value)
+    gran = 2 << 20
+
+    def rounded(b):
+        return (int(b) + gran - 1) // gran * gran
+
+    return (rounded(ws) + rounded(n * 16) + 3 * rounded(R * n * 16) + rounded(agg.n * 24)
+            + rounded(R * nmax * 16) + rounded(R * 24) + rounded(R * 16) + rounded(256))
 
 
 def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> RequestResult:
@@ -103,22 +125,19 @@ def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> Reque
     res = RequestResult(req.rid, agg.n, agg.lmax, R)
     table = cached_translation_table(agg.lmax)
     tm = mie_tmatrix_per_sphere(agg.lmax, agg.k, agg.radii, agg.refractive_index)
-    a = plane_wave_block(agg.lmax, agg.positions, agg.k, req.polar, req.azimuthal, req.pol)
-    A = np.ascontiguousarray(np.moveaxis(a, 2, 0).reshape(R, -1))
-    B = A * tm[None, :]
     dev = CouplingDevice(agg.lmax, table, agg.positions, agg.k, device)
     tmat = torch.from_numpy(tm).to(device)
-    Bt = torch.from_numpy(B).to(device)
+    # incident coefficients and right-hand sides of the R incidences, formed on the device
+    A, Bt = dev.plane_wave_rhs(tmat, req.polar, req.azimuthal, req.pol)
     inner = cfg.tuner.decide(dev, tmat, R).inner if cfg.tuner is not None else inner_kind(agg.lmax, R)
     X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
                               inner_rtol=cfg.inner_rtol, inner=inner)
-    Xh = X.cpu().numpy()
-    res.c_ext = -np.real(np.einsum("rn,rn->r", A.conj(), Xh)) / agg.k**2 * np.pi
+    res.c_ext = (-torch.real((A.conj() * X).sum(dim=1)) / agg.k**2 * np.pi).cpu().numpy()
     st.pop("column_residuals", None)
     st["inner"] = inner
     res.stats = st
     if cfg.keep_solutions:
-        res.x = Xh
+        res.x = X.cpu().numpy()
     return res
 
 
@@ -133,7 +152,7 @@ class Server:
             free, _ = torch.cuda.mem_get_info(self.device)
             self.cfg.hbm_budget_bytes = int(0.8 * free)
         self._solve = solve_fn or solve_request
-        self._footprint = footprint_fn or footprint_bytes
+        self._footprint = footprint_fn or (lambda r, c: footprint_bytes(r, c, self.device))
         self._tls = threading.local()
 
     def _worker(self, req: Request, t0: float) -> RequestResult:
