@@ -106,6 +106,16 @@ int yasf_coupling_matvec(const yasf_plan* plan, int n_particles, const double* p
                          double k_medium, const double* x, double* y, int nrhs, long long ld,
                          int precision, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Near-field variant: the same product restricted to the pairs with |pos_i - pos_j| <= radius
+ * (self pairs excluded), all others dropped: the semantics of the reference's NearFarCouplingBackend
+ * (yasfpy/coupling/backends.py:259-459, numerics.coupling_near_field_radius), which is CPU-only
+ * there. Sources that no receiver of a thread block is near are skipped as a whole. Same workspace
+ * as yasf_coupling_matvec; radius >= 0 and finite. */
+int yasf_coupling_matvec_nearfield(const yasf_plan* plan, int n_particles, const double* positions,
+                                   double k_medium, double near_field_radius, const double* x,
+                                   double* y, int nrhs, long long ld, int precision, void* workspace,
+                                   size_t workspace_bytes, void* stream);
+
 /* No counterpart in the reference. For callers that cannot allocate device memory when they
  * call (all device memory reserved at start-up, an embedding runtime that owns the allocator, or
  * only fixed buffers to hand over): the same y = W x as yasf_coupling_matvec for one right-hand

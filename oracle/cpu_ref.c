@@ -156,9 +156,21 @@ static void lookups_row(int lmax, int N, const double* pos, double k, int s1, in
 }
 
 /* wx[(s1 - s1_begin) * nmax + n1] = (W x)[s1, n1] for s1 in [s1_begin, s1_end).
- * The interaction loop follows particle_interaction_scalar: j1 -> s2 != s1 -> j2 -> p. */
+ * The interaction loop follows particle_interaction_scalar: j1 -> s2 != s1 -> j2 -> p.
+ * cutoff2 >= 0 keeps only the pairs with |pos[s1] - pos[s2]|^2 <= cutoff2, the near-field pairs of
+ * the reference's NearFarCouplingBackend (yasfpy/coupling/backends.py:259-459); < 0 keeps all. */
+int oracle_coupling_matvec_cutoff(int lmax, int N, const double* pos, double k, const double* ab5,
+                                  const double* x, int s1_begin, int s1_end, double* wx, int threads,
+                                  double cutoff2);
+
 int oracle_coupling_matvec(int lmax, int N, const double* pos, double k, const double* ab5,
                            const double* x, int s1_begin, int s1_end, double* wx, int threads) {
+  return oracle_coupling_matvec_cutoff(lmax, N, pos, k, ab5, x, s1_begin, s1_end, wx, threads, -1.0);
+}
+
+int oracle_coupling_matvec_cutoff(int lmax, int N, const double* pos, double k, const double* ab5,
+                                  const double* x, int s1_begin, int s1_end, double* wx, int threads,
+                                  double cutoff2) {
   const int nmax = 2 * lmax * (lmax + 2), P = 2 * lmax, NP = P + 1;
   const int nplm = (P + 1) * (P + 2) / 2;
   mode_desc* md = (mode_desc*)malloc(sizeof(mode_desc) * nmax);
@@ -183,6 +195,11 @@ int oracle_coupling_matvec(int lmax, int N, const double* pos, double k, const d
       int s2, n2, p;
       for (s2 = 0; s2 < N; ++s2) {
         if (s2 == s1) continue;
+        if (cutoff2 >= 0.0) {
+          const double dx = pos[3 * s1] - pos[3 * s2], dy = pos[3 * s1 + 1] - pos[3 * s2 + 1],
+                       dz = pos[3 * s1 + 2] - pos[3 * s2 + 2];
+          if (dx * dx + dy * dy + dz * dz > cutoff2) continue;
+        }
         for (n2 = 0; n2 < nmax; ++n2) {
           const int tau2 = md[n2].tau, l2 = md[n2].l, m2 = md[n2].m;
           const int dtau = abs(tau1 - tau2), dl = abs(l1 - l2), dm = abs(m1 - m2);

@@ -4,7 +4,8 @@ Used by ``tests/`` and ``__graft_entry__.smoke()`` (as the parity reference) and
 baseline leg of ``bench.py`` (timed). Nothing here is imported by the product package.
 
 Functions and the reference code they restate:
-  coupling_matvec_rows      yasfpy/functions/cpu_numba.py:22-95 via cpu_ref.c
+  coupling_matvec_rows      yasfpy/functions/cpu_numba.py:22-95 via cpu_ref.c (and the near-field
+                            pair selection of yasfpy/coupling/backends.py:259-459)
   scattering_bilinear_rows  yasfpy/functions/cpu_numba.py:410-457 via cpu_ref.c
   sph_bessel                yasfpy/functions/misc.py:183-193 (SciPy spherical_jn / spherical_yn)
   legendre                  yasfpy/functions/legendre_normalized_trigon.py:12-95
@@ -48,6 +49,9 @@ def lib() -> ctypes.CDLL:
         L.oracle_legendre.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, dp]
         L.oracle_coupling_matvec.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_double, dp, dp,
                                              ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+        L.oracle_coupling_matvec_cutoff.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_double, dp, dp,
+                                                    ctypes.c_int, ctypes.c_int, dp, ctypes.c_int,
+                                                    ctypes.c_double]
         L.oracle_scattering_bilinear.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_double, dp,
                                                  dp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
         L.oracle_max_threads.argtypes = []
@@ -77,8 +81,11 @@ def legendre(lmax: int, ct: float, st: float) -> np.ndarray:
 
 
 def coupling_matvec_rows(lmax: int, positions: np.ndarray, k: float, table: np.ndarray, x: np.ndarray,
-                         s1_begin: int = 0, s1_end: int | None = None, threads: int = 0) -> np.ndarray:
-    """(W x) for receiving particles [s1_begin, s1_end), flattened particle-major."""
+                         s1_begin: int = 0, s1_end: int | None = None, threads: int = 0,
+                         near_field_radius: float | None = None) -> np.ndarray:
+    """(W x) for receiving particles [s1_begin, s1_end), flattened particle-major. With
+    near_field_radius, only pairs at most that far apart contribute (the near-field pairs of
+    yasfpy/coupling/backends.py:259-459)."""
     pos = np.ascontiguousarray(positions, dtype=np.float64)
     N = pos.shape[0]
     s1_end = N if s1_end is None else s1_end
@@ -86,9 +93,10 @@ def coupling_matvec_rows(lmax: int, positions: np.ndarray, k: float, table: np.n
     tab = np.ascontiguousarray(table, dtype=np.complex128)
     xv = np.ascontiguousarray(x, dtype=np.complex128).reshape(-1)
     out = np.zeros((s1_end - s1_begin) * nmax, dtype=np.complex128)
-    lib().oracle_coupling_matvec(lmax, N, _dp(pos), float(k), _dp(tab.view(np.float64)),
-                                 _dp(xv.view(np.float64)), s1_begin, s1_end, _dp(out.view(np.float64)),
-                                 threads)
+    cutoff2 = -1.0 if near_field_radius is None else float(near_field_radius) ** 2
+    lib().oracle_coupling_matvec_cutoff(lmax, N, _dp(pos), float(k), _dp(tab.view(np.float64)),
+                                        _dp(xv.view(np.float64)), s1_begin, s1_end,
+                                        _dp(out.view(np.float64)), threads, cutoff2)
     return out
 
 

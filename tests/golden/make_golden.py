@@ -6,7 +6,8 @@ location must be given in ``$YASF_REFERENCE`` (there is no default):
     YASF_REFERENCE=<path to the yasfpy checkout> python tests/golden/make_golden.py [part ...]
 
 Parts: ``tables`` (CELES goldens and translation tables lmax 1-6), ``c1``, ``l78`` (translation
-tables lmax 7 and 8 and reference matvec fixtures at those orders), ``celes500``; no part = all.
+tables lmax 7 and 8 and reference matvec fixtures at those orders), ``nearfar`` (the near-field
+backend), ``celes500``; no part = all.
 
 The reference imports with the stand-ins from ``oracle/stubs`` (pywigxjpf via sympy's exact 3j,
 refidxdb and pyperf as inert stand-ins). Two kinds of fixtures are written:
@@ -27,6 +28,7 @@ from __future__ import annotations
 
 import os
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -40,7 +42,8 @@ REF = Path(os.environ["YASF_REFERENCE"])
 sys.path.insert(0, str(REPO))
 sys.path.insert(0, str(REPO / "oracle" / "stubs"))
 sys.path.insert(0, str(REF))
-os.environ.setdefault("HOME", "/tmp/yasf_golden_home")
+# the reference caches its translation tables under $HOME: keep that cache in a temporary directory
+os.environ["HOME"] = tempfile.mkdtemp(prefix="yasf_golden_home_")
 
 from scipy.io import loadmat  # noqa: E402
 
@@ -234,6 +237,27 @@ def solve_fixture(name, agg, tol, restart=100):
     print(f"  {name}: C_ext={opt.c_ext[0]:.10g} C_sca={opt.c_sca[0]:.10g} ({t_solve:.1f}s)")
 
 
+def nearfar_fixture():
+    """The reference's NearFarCouplingBackend (near-field pairs only, yasfpy/coupling/
+    backends.py:259-459) on a seeded aggregate, with its dense W x for comparison."""
+    rng = np.random.default_rng(23)
+    radii = rng.uniform(0.05, 0.12, size=40)
+    pos = rsa_cube(radii, 0.12, rng, max_attempts=200_000)
+    lmax, wl, m, radius = 3, 0.55, 1.5 + 0.01j, 0.6
+    sim, _ = ref_simulation(pos, radii, m, wl, lmax)
+    sim.numerics.coupling_near_field_radius = radius
+    sim.numerics.coupling_tile_size = 16
+    from yasfpy.coupling.backends import NearFarCouplingBackend
+
+    n = pos.shape[0] * sim.numerics.nmax
+    x = rng.normal(size=n) + 1j * rng.normal(size=n)
+    wx_dense = sim.coupling_matrix_multiply(x, idx=0)
+    wx_near = NearFarCouplingBackend(sim).multiply(x, idx=0)
+    save("ref_matvec_nearfar.npz", lmax=lmax, wavelength=wl, positions=pos, radii=radii,
+         near_field_radius=radius, x=x, wx_near=np.asarray(wx_near).reshape(-1),
+         wx_dense=np.asarray(wx_dense).reshape(-1))
+
+
 def precond_fixture():
     """Reference-derived block matrices for a geometry whose cells hold several spheres."""
     from yasfpy.preconditioner import make_particle_partition
@@ -277,6 +301,9 @@ def main():
     if only == {"l78"}:
         high_order_fixtures()
         return
+    if only == {"nearfar"}:
+        nearfar_fixture()
+        return
     c1 = aggregate_c1(seed=0)
     if not only or "c1" in only:
         matvec_fixture("ref_matvec_c1.npz", c1.positions, c1.radii, c1.refractive_index,
@@ -290,6 +317,7 @@ def main():
     p3 = rsa_cube(r3, 0.12, rng, max_attempts=200_000)
     matvec_fixture("ref_matvec_l3.npz", p3, r3, 1.45 + 0.03j, 0.5, 3, seed=13)
     multichannel_fixture()
+    nearfar_fixture()
     solve_fixture("ref_solve_c1_tol1e-8.npz", c1, 1e-8)
     solve_fixture("ref_solve_c1_tol1e-13.npz", c1, 1e-13)
     precond_fixture()

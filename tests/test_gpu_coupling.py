@@ -124,3 +124,36 @@ def test_full_size_properties(cuda_device):
     for s in (0, 977, 1999):
         ref = R.coupling_matvec_rows(agg.lmax, agg.positions, agg.k, table, x1, s, s + 1)
         assert rel_err(y1.cpu().numpy()[s * nmax:(s + 1) * nmax], ref) < 1e-11
+
+
+def test_near_field_matvec_matches_reference_nearfar(golden, cuda_device):
+    """yasf_coupling_matvec_nearfield against the reference's NearFarCouplingBackend (the pairs
+    within the radius only, yasfpy/coupling/backends.py:259-459), at 1e-12; complex64 at 2e-5."""
+    g = golden("ref_matvec_nearfar.npz")
+    lmax = int(g["lmax"])
+    k = 2 * np.pi / float(g["wavelength"])
+    dev, _ = _dev(lmax, g["positions"], k, cuda_device)
+    x = _t(g["x"], cuda_device)
+    radius = float(g["near_field_radius"])
+    assert rel_err(dev.coupling_nearfield(x, radius).cpu().numpy(), g["wx_near"]) < 1e-12
+    assert rel_err(dev.coupling_nearfield(x, radius, YASF_C64).cpu().numpy(), g["wx_near"]) < 2e-5
+
+
+@pytest.mark.parametrize("n,radius", [(300, 0.35), (129, 0.8)])
+def test_near_field_matvec_matches_oracle_and_limits(cuda_device, n, radius):
+    """Spatially scattered receivers, so many thread blocks skip whole sources; a radius beyond
+    every distance gives the dense product, one below every distance gives zero."""
+    rng = np.random.default_rng(n)
+    radii = rng.uniform(0.05, 0.1, size=n)
+    pos = rsa_cube(radii, 0.1, rng)
+    k = 2 * np.pi / 0.6
+    lmax = 3
+    dev, table = _dev(lmax, pos, k, cuda_device)
+    nmax = 2 * lmax * (lmax + 2)
+    x = rng.normal(size=n * nmax) + 1j * rng.normal(size=n * nmax)
+    xt = _t(x, cuda_device)
+    ref = R.coupling_matvec_rows(lmax, pos, k, table, x, near_field_radius=radius)
+    assert rel_err(dev.coupling_nearfield(xt, radius).cpu().numpy(), ref) < 1e-12
+    far = 10.0 * float(np.ptp(pos, axis=0).max() + 1.0)
+    assert rel_err(dev.coupling_nearfield(xt, far).cpu().numpy(), dev.coupling(xt).cpu().numpy()) < 1e-14
+    assert np.all(dev.coupling_nearfield(xt, 0.0).cpu().numpy() == 0)

@@ -99,3 +99,20 @@ def test_oracle_precond_blocks_match_reference(golden):
         assert rel_err(M, g[f"block{b}"]) < 1e-12
         multi += len(blk) > 1
     assert multi > 0, "fixture must hold at least one multi-sphere block"
+
+
+def test_oracle_near_field_matches_reference_nearfar_backend(golden):
+    """The oracle's near-field selection against the reference's NearFarCouplingBackend
+    (yasfpy/coupling/backends.py:259-459), and without a cutoff against the reference's dense W x."""
+    g = golden("ref_matvec_nearfar.npz")
+    lmax = int(g["lmax"])
+    k = 2 * np.pi / float(g["wavelength"])
+    from yasf_b200.wigner import translation_table_ab5
+
+    table = translation_table_ab5(lmax)
+    near = R.coupling_matvec_rows(lmax, g["positions"], k, table, g["x"],
+                                  near_field_radius=float(g["near_field_radius"]))
+    assert rel_err(near, g["wx_near"]) < 1e-12
+    dense = R.coupling_matvec_rows(lmax, g["positions"], k, table, g["x"])
+    assert rel_err(dense, g["wx_dense"]) < 1e-12
+    assert rel_err(near, dense) > 1e-3  # the cutoff drops pairs that matter

@@ -66,6 +66,7 @@ SIGNATURES = {
     "yasf_plan_check_table": [_i, _vp],
     "yasf_coupling_workspace_size": [_vp, _i, _i, _i, _c.POINTER(_sz)],
     "yasf_coupling_matvec": [_vp, _i, _vp, _d, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],
+    "yasf_coupling_matvec_nearfield": [_vp, _i, _vp, _d, _d, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],
     "yasf_master_matvec": [_vp, _i, _vp, _d, _vp, _vp, _vp, _i, _ll, _i, _vp, _sz, _vp],
     "yasf_coupling_matvec_noalloc": [_vp, _i, _vp, _d, _vp, _vp, _i, _vp],
     "yasf_panel_workspace_size": [_vp, _i, _i, _c.POINTER(_sz)],

@@ -52,3 +52,28 @@ class B200CouplingBackend(CouplingBackend):
             xt = torch.from_numpy(np.ascontiguousarray(xw.reshape(jmax))).to(dev.device)
             out[:, w] = dev.coupling(xt, prec).cpu().numpy()
         return out
+
+
+class B200NearFieldCouplingBackend(B200CouplingBackend):
+    """The reference's ``nearfar`` semantics (yasfpy/coupling/backends.py:259-459) on the B200:
+    only pairs at most ``numerics.coupling_near_field_radius`` apart contribute (self pairs
+    excluded), the rest of W is dropped; C ABI ``yasf_coupling_matvec_nearfield``. The reference's
+    version is CPU-only and needs the radius set; so does this one (``ValueError`` otherwise)."""
+
+    def multiply(self, x: np.ndarray, idx: int | None = None) -> np.ndarray:
+        sim = self._sim
+        radius = getattr(sim.numerics, "coupling_near_field_radius", None)
+        if radius is None:
+            raise ValueError("nearfar backend requires numerics.coupling_near_field_radius to be set.")
+        prec = PRECISIONS[sim.numerics.b200_precision]
+        jmax = sim.parameters.particles.number * sim.numerics.nmax
+        channels = sim.parameters.k_medium.shape[0]
+        x = np.asarray(x, dtype=np.complex128)
+        ws = [idx] if idx is not None else list(range(channels))
+        out = np.zeros((jmax, len(ws)), dtype=np.complex128)
+        for c, w in enumerate(ws):
+            xw = x if (idx is not None or x.ndim == 1) else x[:, w]
+            dev = sim.device_state(w)
+            xt = torch.from_numpy(np.ascontiguousarray(xw.reshape(jmax))).to(dev.device)
+            out[:, c] = dev.coupling_nearfield(xt, float(radius), prec).cpu().numpy()
+        return out[:, 0] if idx is not None else out

@@ -111,7 +111,7 @@ int check_current_device(int device) {
 
 int coupling_column(const yasf_plan* plan, int n_particles, const double* positions, double k,
                     const double* tmat, const double* x, double* y, int precision, int mode,
-                    void* workspace, size_t workspace_bytes, cudaStream_t stream) {
+                    void* workspace, size_t workspace_bytes, cudaStream_t stream, double cutoff2) {
   const CouplingLayout lay = coupling_layout(plan, n_particles, precision);
   if (!workspace || workspace_bytes < lay.total) return YASF_ERR_WORKSPACE;
   if (!aligned16(workspace)) return YASF_ERR_ALIGNMENT;
@@ -160,6 +160,7 @@ int coupling_column(const yasf_plan* plan, int n_particles, const double* positi
   }
   ca.partial = partial;
   ca.err = err;
+  ca.cutoff2 = cutoff2;
   ca.poll_limit = stall_hook().contract_polls;
   ca.stall = stall_hook().role == YASF_STALL_CONTRACT ? 1 : 0;
   int st = dispatch_contract(plan->lmax, precision, regular, ca, lay.tiles, lay.chunks,
@@ -513,7 +514,7 @@ extern "C" int yasf_coupling_workspace_size(const yasf_plan* plan, int n_particl
 static int matvec_common(const yasf_plan* plan, int n_particles, const double* positions,
                          double k, const double* tmat, const double* x, double* y, int nrhs,
                          long long ld, int precision, int mode, void* workspace,
-                         size_t workspace_bytes, void* stream) {
+                         size_t workspace_bytes, void* stream, double cutoff2 = -1.0) {
   int st = validate_coupling(plan, n_particles, positions, k, precision);
   if (st != YASF_OK) return st;
   if (!x || !y || nrhs <= 0) return YASF_ERR_INVALID_ARGUMENT;
@@ -525,10 +526,20 @@ static int matvec_common(const yasf_plan* plan, int n_particles, const double* p
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   for (int c = 0; c < nrhs; ++c) {
     st = coupling_column(plan, n_particles, positions, k, tmat, x + 2 * ld * c, y + 2 * ld * c,
-                         precision, mode, workspace, workspace_bytes, s);
+                         precision, mode, workspace, workspace_bytes, s, cutoff2);
     if (st != YASF_OK) return st;
   }
   return YASF_OK;
+}
+
+extern "C" int yasf_coupling_matvec_nearfield(const yasf_plan* plan, int n_particles,
+                                              const double* positions, double k_medium,
+                                              double near_field_radius, const double* x, double* y,
+                                              int nrhs, long long ld, int precision, void* workspace,
+                                              size_t workspace_bytes, void* stream) {
+  if (!(near_field_radius >= 0.0) || !std::isfinite(near_field_radius)) return YASF_ERR_INVALID_ARGUMENT;
+  return matvec_common(plan, n_particles, positions, k_medium, nullptr, x, y, nrhs, ld, precision, 0,
+                       workspace, workspace_bytes, stream, near_field_radius * near_field_radius);
 }
 
 extern "C" int yasf_coupling_matvec(const yasf_plan* plan, int n_particles,

@@ -72,9 +72,11 @@ CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int preci
 
 // Launch the full coupling pipeline for one column (vbuild, contract, reduce).
 // mode: 0 -> y = W x, 1 -> y = x - T (.) W x, 2 -> block sums of conj(x) (.) W_reg x.
+// cutoff2 >= 0 keeps only the pairs within sqrt(cutoff2) of each other (near-field variant).
 int coupling_column(const yasf_plan* plan, int n_particles, const double* positions, double k,
                     const double* tmat, const double* x, double* y, int precision, int mode,
-                    void* workspace, size_t workspace_bytes, cudaStream_t stream);
+                    void* workspace, size_t workspace_bytes, cudaStream_t stream,
+                    double cutoff2 = -1.0);
 
 int dispatch_contract(int lmax, int precision, bool regular, const ContractArgs& a, int tiles,
                       int chunks, int threads, cudaStream_t stream);

@@ -156,6 +156,7 @@ struct ContractArgs {
   int bundle_len[8];             // padded stream length per source
   void* partial;                 // (chunks, N, nmax) Real2 partial sums
   int* err;                      // set to 1 if a shared-memory stage wait timed out
+  double cutoff2;                // >= 0: only pairs with |pos[s1] - pos[s2]|^2 <= cutoff2 (near field)
   int poll_limit;                // polls of one stage wait before it gives up (2^22 normally)
   int stall;                     // test hook: 1 = the first stage copy of every block is never
                                  // issued, so its wait runs out (0 normally)
@@ -269,8 +270,9 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     const double dz = z1 - __ldg(a.pos + 3 * s2 + 2);
     const double r2 = dx * dx + dy * dy + dz * dz;
     const bool self = (s2 == s1c);
-    // Regular form keeps self pairs (r = 0: cos theta = 0, phi = 0, j_p(0) = delta_p0).
-    const bool use = active && (REGULAR ? true : !self);
+    // Regular form keeps self pairs (r = 0: cos theta = 0, phi = 0, j_p(0) = delta_p0). With a
+    // near-field cutoff only the pairs within it contribute (the others are masked like self pairs).
+    const bool use = active && (REGULAR ? true : !self) && (a.cutoff2 < 0.0 || r2 <= a.cutoff2);
     double r = sqrt(r2);
     double ct = (r > 0.0) ? dz / r : 0.0;
     ct = fmin(1.0, fmax(-1.0, ct));
@@ -307,6 +309,12 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
       last_it = it;
       if (threadIdx.x == 0) atomicExch(a.err, 1);
       break;
+    }
+    // with a cutoff, a source that no receiver of the block is near is skipped as a whole
+    // (a.cutoff2 is uniform, so is the extra barrier)
+    if (a.cutoff2 >= 0.0 && !__syncthreads_or(use)) {
+      __syncthreads();
+      continue;
     }
     const VE* vp = cur ? stage1 : stage0;
     const Real ctR = (Real)ct, stR = (Real)st;

@@ -129,6 +129,20 @@ class CouplingDevice:
         """W x for x of shape (n,) or (R, n) stored row-major as R columns (see ``columns``)."""
         return self._apply("yasf_coupling_matvec", None, x, precision, out)
 
+    def coupling_nearfield(self, x: torch.Tensor, radius: float, precision: int = YASF_C128,
+                           out: torch.Tensor | None = None):
+        """W x restricted to the pairs at most ``radius`` apart (near-field variant)."""
+        cols = x.reshape(-1, self.n) if x.dim() > 1 else x.reshape(1, self.n)
+        if x.dtype != torch.complex128 or x.device != self.device:
+            raise ValueError("vectors must be complex128 tensors on the plan's device")
+        cols = cols.contiguous()
+        y = out if out is not None else torch.empty_like(cols)
+        wsb = self.coupling_ws_bytes(precision)
+        ws = self.ws.get(wsb)
+        call("yasf_coupling_matvec_nearfield", self.plan.handle, self.n_particles, _ptr(self.pos), self.k,
+             float(radius), _ptr(cols), _ptr(y), cols.shape[0], self.n, precision, _ptr(ws), wsb, _stream_ptr())
+        return y.reshape(x.shape)
+
     def master(self, x: torch.Tensor, tmat: torch.Tensor, precision: int = YASF_C128,
                out: torch.Tensor | None = None):
         """x - T (.) W x."""

@@ -17,7 +17,7 @@ import os
 import numpy as np
 import torch
 
-from yasf_b200.coupling import B200CouplingBackend
+from yasf_b200.coupling import B200CouplingBackend, B200NearFieldCouplingBackend
 from yasf_b200.device import CouplingDevice
 from yasf_b200.incident import compute_initial_field_coefficients
 from yasf_b200.mie import compute_mie_coefficients
@@ -52,10 +52,12 @@ class Simulation:
         backend_name = str(getattr(self.numerics, "coupling_backend", "b200")).lower()
         if backend_name in {"b200"}:
             self.coupling_backend = B200CouplingBackend(self)
+        elif backend_name in {"nearfar", "near_far", "near-far"}:
+            self.coupling_backend = B200NearFieldCouplingBackend(self)
         else:
             raise ValueError(
-                f"Unsupported coupling backend: {backend_name!r}. Expected 'b200' "
-                "(the reference's 'dense', 'tiled_dense' and 'nearfar' backends live in yasfpy)."
+                f"Unsupported coupling backend: {backend_name!r}. Expected 'b200' or 'nearfar' "
+                "(the reference's 'dense' and 'tiled_dense' backends compute what 'b200' computes)."
             )
         if device is None:
             if not torch.cuda.is_available():
@@ -127,6 +129,9 @@ class Simulation:
         solver: Solver = self.numerics.solver
         if solver is None:
             raise ValueError("numerics.solver is not set")
+        if isinstance(self.coupling_backend, B200NearFieldCouplingBackend):
+            raise NotImplementedError("the device solve applies the exact coupling operator; the near-field "
+                                      "backend provides coupling products (coupling_matrix_multiply)")
         W = self.parameters.wavelengths_number
         self.scattered_field_coefficients = np.zeros_like(self.initial_field_coefficients)
         self.scattered_field_err_codes = np.zeros(W)
