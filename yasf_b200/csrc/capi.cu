@@ -57,6 +57,33 @@ static int sm_count_of(int device) {
   return cached[device];
 }
 
+template <int L>
+int contract_resident_blocks(int precision, int threads);
+
+// Resident contraction blocks per SM for (lmax, precision, threads), from the occupancy query
+// (cached per device state of this process).
+static int resident_blocks(int lmax, int precision, int threads) {
+  static std::mutex mu;
+  static int cache[YASF_LMAX_MAX + 1][2][5] = {};
+  const int pi = precision == YASF_C64 ? 1 : 0, wi = std::min(4, std::max(1, threads / 32));
+  std::lock_guard<std::mutex> lock(mu);
+  int& c = cache[lmax][pi][wi];
+  if (c == 0) {
+    switch (lmax) {
+      case 1: c = contract_resident_blocks<1>(precision, threads); break;
+      case 2: c = contract_resident_blocks<2>(precision, threads); break;
+      case 3: c = contract_resident_blocks<3>(precision, threads); break;
+      case 4: c = contract_resident_blocks<4>(precision, threads); break;
+      case 5: c = contract_resident_blocks<5>(precision, threads); break;
+      case 6: c = contract_resident_blocks<6>(precision, threads); break;
+      case 7: c = contract_resident_blocks<7>(precision, threads); break;
+      case 8: c = contract_resident_blocks<8>(precision, threads); break;
+      default: c = 2;
+    }
+  }
+  return c;
+}
+
 CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int precision) {
   CouplingLayout lay;
   // partial sums: complex at the kernel's precision; V stream: 16-byte entries at both precisions
@@ -64,13 +91,14 @@ CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int preci
   const size_t csize = (precision == YASF_C64) ? sizeof(float2) : sizeof(double2);
   const size_t vsize = (precision == YASF_C64) ? sizeof(float4) : sizeof(double2);
   const int N = n_particles;
-  // Receivers per block: whole warps, at most 4.
-  const int warps = std::min(4, std::max(1, (N + 31) / 32));
+  // Receivers per block: whole warps, at most 4, one receiver per thread (two in complex64).
+  const int rpt = precision == YASF_C64 ? 2 : 1;
+  const int warps = std::min(4, std::max(1, (N + 32 * rpt - 1) / (32 * rpt)));
   lay.threads = 32 * warps;
-  lay.tiles = (N + lay.threads - 1) / lay.threads;
+  lay.tiles = (N + lay.threads * rpt - 1) / (lay.threads * rpt);
   const int sms = sm_count_of(plan->device);
-  // Enough blocks for ~4 resident blocks per SM; split the source loop to get there.
-  const long long want = 4LL * sms;
+  // Two full waves of resident blocks; the source loop is split into chunks to get there.
+  const long long want = 2LL * resident_blocks(plan->lmax, precision, lay.threads) * sms;
   const long long base = (long long)lay.tiles * plan->n_bundles;
   int chunks = (int)std::max<long long>(1, (want + base - 1) / base);
   chunks = std::min(chunks, N);

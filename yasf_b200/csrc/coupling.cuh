@@ -203,9 +203,15 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   return false;
 }
 
+// One (receiver tile, source chunk) of bundle BID. The two stage barriers are initialised by the
+// caller; `uses` (every thread, uniform) counts the phases of each stage consumed so far and
+// `issued` (thread 0) the copies issued into each, both carried across calls, so a persistent
+// block can process many work items with the same barriers. Returns false when a stage wait ran
+// out (the error word is set, the copies in flight are drained, the block must stop).
 template <int L, int BID, typename Real, bool REGULAR>
-__device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
-                                              unsigned long long* bars) {
+__device__ __forceinline__ bool contract_body(const ContractArgs& a, int tile, int chunk, char* smem,
+                                              unsigned long long* bars, unsigned (&uses)[2],
+                                              unsigned (&issued)[2]) {
   using C = typename Cplx<Real>::T;
   using VE = typename VEntry<Real>::T;
   constexpr bool F64 = sizeof(Real) == 8;
@@ -213,7 +219,7 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
   constexpr int NR = bi.rows;
   constexpr int PMAX = 2 * L;
 
-  const int s1 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s1 = tile * blockDim.x + threadIdx.x;
   const bool active = s1 < a.n_particles;
   const int s1c = active ? s1 : 0;
   const double x1 = __ldg(a.pos + 3 * s1c + 0);
@@ -229,7 +235,7 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     else yc[r] = make_float2(0.f, 0.f);
   }
 
-  const int c = blockIdx.y;
+  const int c = chunk;
   const int sb = c * a.sources_per_chunk;
   const int se = min(a.n_particles, sb + a.sources_per_chunk);
   const VE* vbase = reinterpret_cast<const VE*>(a.v) + (size_t)a.bundle_begin[BID] * a.n_particles;
@@ -237,21 +243,13 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
   const unsigned stage_bytes = (unsigned)(vstride * sizeof(VE));
   VE* const stage0 = reinterpret_cast<VE*>(smem);
   VE* const stage1 = stage0 + vstride;
-  if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  // Thread 0 issues every stage copy and remembers, per stage, the iteration whose copy it issued
-  // last (-1: none), so that a block that gives up drains exactly the copies still in flight.
-  int issued_it[2] = {-1, -1};
+  // Thread 0 issues every stage copy and counts them per stage, so that a block that gives up
+  // drains exactly the copies still in flight (issued[b] > uses[b]).
   if (threadIdx.x == 0 && sb < se && !a.stall) {
     bulk_load(stage0, vbase + (size_t)sb * vstride, stage_bytes, &bars[0]);
-    issued_it[0] = 0;
+    ++issued[0];
   }
   bool timed_out = false;
-  int last_it = 0;
 
 #pragma unroll 1
   for (int s2 = sb; s2 < se; ++s2) {
@@ -262,7 +260,7 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     if (threadIdx.x == 0 && s2 + 1 < se) {
       bulk_load(cur ? stage0 : stage1, vbase + (size_t)(s2 + 1) * vstride, stage_bytes,
                 &bars[cur ^ 1]);
-      issued_it[cur ^ 1] = it + 1;
+      ++issued[cur ^ 1];
     }
     // ---- pair geometry: d = pos[s1] - pos[s2] (yasfpy/functions/misc.py:149-166) ----
     const double dx = x1 - __ldg(a.pos + 3 * s2 + 0);
@@ -303,13 +301,13 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     }
 
     // block-uniform decision: every thread polls (bounded), then all agree before using the stage
-    const bool ok = mbar_wait(&bars[cur], (unsigned)((it >> 1) & 1), a.poll_limit);
+    const bool ok = mbar_wait(&bars[cur], uses[cur] & 1u, a.poll_limit);
     if (__syncthreads_or(!ok)) {
       timed_out = true;
-      last_it = it;
       if (threadIdx.x == 0) atomicExch(a.err, 1);
       break;
     }
+    ++uses[cur];
     // with a cutoff, a source that no receiver of the block is near is skipped as a whole
     // (a.cutoff2 is uniform, so is the extra barrier)
     if (a.cutoff2 >= 0.0 && !__syncthreads_or(use)) {
@@ -414,18 +412,17 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
     __syncthreads();  // every warp is done with this stage before it is refilled
   }
   if (timed_out) {
-    // No copy may still be landing in shared memory when the block exits. Iterations before
-    // last_it consumed their stages, so a copy is outstanding exactly where thread 0 issued one
-    // for iteration last_it or later; wait (bounded) for each of those. Should a drain itself run
-    // out, the block exits with that copy's state undefined; the error word is already set and the
+    // No copy may still be landing in shared memory when the block exits: a stage holds one
+    // exactly when thread 0 issued more copies into it than the block consumed, and that copy
+    // completes the stage's next phase; wait (bounded) for each. Should a drain itself run out,
+    // the block exits with that copy's state undefined; the error word is already set and the
     // result is poisoned.
     if (threadIdx.x == 0) {
 #pragma unroll
       for (int b = 0; b < 2; ++b)
-        if (issued_it[b] >= last_it)
-          (void)mbar_wait(&bars[b], (unsigned)((issued_it[b] >> 1) & 1));
+        if (issued[b] > uses[b]) (void)mbar_wait(&bars[b], uses[b] & 1u);
     }
-    return;
+    return false;
   }
 
   if (active) {
@@ -449,27 +446,58 @@ __device__ __forceinline__ void contract_body(const ContractArgs& a, char* smem,
       }
     }
   }
+  return true;
+}
+
+#include "coupling_c64.cuh"
+
+// Receivers per thread of the contraction: two for the complex64 (Hankel) kernel, else one.
+template <typename Real, bool REGULAR>
+__host__ __device__ constexpr int receivers_per_thread() {
+  return (sizeof(Real) == 4 && !REGULAR) ? kC64Receivers : 1;
 }
 
 template <int L, typename Real, bool REGULAR, int B>
 struct BundleDispatch {
-  __device__ static __forceinline__ void run(const ContractArgs& a, int b, char* smem,
-                                             unsigned long long* bars) {
-    if (b == B - 1) contract_body<L, B - 1, Real, REGULAR>(a, smem, bars);
-    else BundleDispatch<L, Real, REGULAR, B - 1>::run(a, b, smem, bars);
+  __device__ static __forceinline__ bool run(const ContractArgs& a, int b, int tile, int chunk,
+                                             char* smem, unsigned long long* bars,
+                                             unsigned (&uses)[2], unsigned (&issued)[2]) {
+    if (b == B - 1) {
+      if constexpr (sizeof(Real) == 4 && !REGULAR)
+        return contract_body_c64<L, B - 1>(a, tile, chunk, smem, bars, uses, issued);
+      else
+        return contract_body<L, B - 1, Real, REGULAR>(a, tile, chunk, smem, bars, uses, issued);
+    }
+    return BundleDispatch<L, Real, REGULAR, B - 1>::run(a, b, tile, chunk, smem, bars, uses, issued);
   }
 };
 template <int L, typename Real, bool REGULAR>
 struct BundleDispatch<L, Real, REGULAR, 0> {
-  __device__ static __forceinline__ void run(const ContractArgs&, int, char*, unsigned long long*) {}
+  __device__ static __forceinline__ bool run(const ContractArgs&, int, int, int, char*,
+                                             unsigned long long*, unsigned (&)[2], unsigned (&)[2]) {
+    return true;
+  }
 };
 
+__device__ __forceinline__ void stage_barriers_init(unsigned long long* bars) {
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+}
+
 // Dynamic shared memory: two stages of the largest bundle stream (16-byte aligned).
+// blockIdx.x = receiver tile, blockIdx.y = source chunk, blockIdx.z = bundle.
 template <int L, typename Real, bool REGULAR>
 __global__ void __launch_bounds__(128) contract_kernel(ContractArgs a) {
   extern __shared__ __align__(128) char smem[];
   __shared__ __align__(8) unsigned long long bars[2];
-  BundleDispatch<L, Real, REGULAR, num_bundles(L)>::run(a, blockIdx.z, smem, bars);
+  stage_barriers_init(bars);
+  unsigned uses[2] = {0u, 0u}, issued[2] = {0u, 0u};
+  (void)BundleDispatch<L, Real, REGULAR, num_bundles(L)>::run(a, blockIdx.z, blockIdx.x, blockIdx.y, smem, bars,
+                                                              uses, issued);
 }
 
 template <int L>
@@ -561,5 +589,8 @@ __global__ void __launch_bounds__(256) reduce_dot_kernel(long long n_elems, int 
 template <int L>
 cudaError_t launch_contract(int precision, bool regular, const ContractArgs& a, int tiles,
                             int chunks, int threads, cudaStream_t stream);
+// Blocks of the (non-regular) contraction kernel resident per SM at `threads` threads.
+template <int L>
+int contract_resident_blocks(int precision, int threads);
 
 }  // namespace yasf

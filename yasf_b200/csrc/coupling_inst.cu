@@ -36,4 +36,22 @@ cudaError_t launch_contract<YASF_INST_L>(int precision, bool regular, const Cont
   return cudaGetLastError();
 }
 
+template <>
+int contract_resident_blocks<YASF_INST_L>(int precision, int threads) {
+  constexpr int L = YASF_INST_L;
+  const size_t stage = 2 * (size_t)max_bundle_stream<L>() * (precision == YASF_C64 ? sizeof(float4) : sizeof(double2));
+  int blocks = 0;
+  cudaError_t e;
+  if (precision == YASF_C64) {
+    e = cudaFuncSetAttribute(contract_kernel<L, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, contract_kernel<L, float, false>, threads, stage);
+  } else {
+    e = cudaFuncSetAttribute(contract_kernel<L, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, contract_kernel<L, double, false>, threads, stage);
+  }
+  return (e == cudaSuccess && blocks > 0) ? blocks : 2;
+}
+
 }  // namespace yasf

@@ -78,7 +78,8 @@ __global__ void mdot_final_kernel(int nvec, int nblk, const double2* partial, do
   }
   if (threadIdx.x == 0) {
     if (norm_out) {
-      norm_out[0] = sqrt(fmax(sr[0], 0.0));
+      // a NaN sum stays NaN (fmax alone would turn it into 0, a converged-looking norm)
+      norm_out[0] = (isnan(sr[0]) ? sr[0] : sqrt(fmax(sr[0], 0.0)));
     } else if (accumulate) {
       out[k].x += sr[0];
       out[k].y += si[0];

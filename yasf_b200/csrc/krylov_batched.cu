@@ -88,7 +88,8 @@ __global__ void bfinal_kernel(int nvec, int nblk, const double2* partial, double
   }
   if (threadIdx.x == 0) {
     if (norm) {
-      norm[c] = sqrt(fmax(sr[0], 0.0));
+      // a NaN sum stays NaN (fmax alone would turn it into 0, a converged-looking norm)
+      norm[c] = (isnan(sr[0]) ? sr[0] : sqrt(fmax(sr[0], 0.0)));
     } else if (accumulate) {
       double2* o = out + (size_t)c * out_col + k;
       o->x += sr[0];
