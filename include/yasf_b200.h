@@ -197,6 +197,36 @@ int yasf_plane_wave_rhs(int lmax, int n_particles, const double* positions, int 
                         const double* kvec, const double* coef, const double* focal_point,
                         const double* tmat, double* a, double* b, long long ld, void* stream);
 
+/* ---- grouped solve: right-hand sides of several aggregates at once -------------------------------
+ * No single reference counterpart: the reference solves one aggregate and one incidence per
+ * Simulation (yasfpy/scattered_field_coefficients.py:95-144, yasfpy/solver.py:108-121). Here the
+ * columns of several aggregates of one lmax (each its own spheres, positions, wavenumber, T and
+ * right-hand sides) are solved together by lockstep float64-refined GMRES, every column with its own
+ * Krylov basis: each operator application is three launches for all live columns of all aggregates,
+ * the middle one a persistent work-queue contraction (resident blocks take (column, receiver tile,
+ * source chunk, bundle) items from a device counter), so small aggregates share launches instead of
+ * each running its own. Inner operator at inner_precision (YASF_C64 or YASF_C128), float64
+ * residuals, X0 = 0, columns leave at ||b - A x|| <= rtol ||b||; no preconditioner.
+ * stats (host, may be NULL): [0] lockstep inner steps, [1] inner operator applications (all columns
+ * each), [2] float64 applications, [3] worst relative residual, [4] unconverged columns,
+ * [5] refinement steps, [6] columns, [7] work items per application. column_residuals (host, may be
+ * NULL): final relative residual of every column, aggregate by aggregate. Synchronous. */
+typedef struct {
+  int n_particles;
+  const double* positions;   /* device (N, 3) */
+  double k_medium;
+  const double* tmat;        /* device (N*nmax) complex128 */
+  const double* b;           /* device, nrhs columns of N*nmax */
+  double* x;                 /* device, nrhs columns of N*nmax (output) */
+  int nrhs;
+} yasf_problem;
+int yasf_grouped_workspace_size(const yasf_plan* plan, int n_problems, const yasf_problem* problems,
+                                int restart, size_t* bytes);
+int yasf_grouped_solve(const yasf_plan* plan, int n_problems, const yasf_problem* problems, double rtol,
+                       int restart, int max_refine, double inner_rtol, int inner_precision,
+                       void* workspace, size_t workspace_bytes, double* stats, double* column_residuals,
+                       void* stream);
+
 /* ---- cross sections (yasfpy/optics.py:55-156) ------------------------------------------------
  * out[0..1] (device) <- sum_{s,n} conj(b) (W_reg b), the bilinear form of
  * compute_scattering_cross_section (yasfpy/functions/cpu_numba.py:410-457): regular spherical

@@ -12,7 +12,7 @@ from conftest import rel_err
 from yasf_b200.device import CouplingDevice
 from yasf_b200.incident import plane_wave_block
 from yasf_b200.mie import mie_tmatrix_per_sphere
-from yasf_b200.serve import ServeConfig, Server, solve_request, summarize
+from yasf_b200.serve import ServeConfig, Server, groupable, solve_group, solve_request, summarize
 from yasf_b200.wigner import translation_table_ab5
 from yasf_b200.workloads import Aggregate, Request, incidences, rsa_cube
 
@@ -41,7 +41,10 @@ def test_results_same_alone_and_in_the_mix(cuda_device):
     mixed = Server(cfg, device=cuda_device).run(reqs, realtime=False)
     for r in mixed:
         assert r.error is None, r.error
-    alone = [solve_request(q, cfg, cuda_device) for q in reqs]
+    # a small complex64-inner request is solved by a grouped solve in the mix: alone it is a group
+    # of one; every column's trajectory is its own, so the results agree bit for bit
+    alone = [solve_group([q], cfg, cuda_device)[0] if groupable(q, cfg) else solve_request(q, cfg, cuda_device)
+             for q in reqs]
     for m, a in zip(mixed, alone):
         assert m.rid == a.rid
         assert rel_err(m.x, a.x) <= 1e-12
@@ -86,3 +89,26 @@ def test_admission_footprint_covers_the_device_memory_of_a_request(cuda_device):
         peak = torch.cuda.max_memory_allocated(cuda_device) - base
         assert peak <= fp, (req.rid, peak, fp)
         assert fp <= 2 * peak + (16 << 20), (req.rid, peak, fp)
+
+
+def test_small_requests_grouped_equal_alone(cuda_device):
+    """Five small requests of one lmax arriving together are served by one grouped solve; each
+    result equals that request solved alone (a group of one), and the float64 solve within 1e-6."""
+    reqs = []
+    for i, (n, R) in enumerate([(30, 1), (80, 2), (12, 1), (55, 2), (41, 1)]):
+        rng = np.random.default_rng(700 + i)
+        radii = rng.uniform(0.05, 0.12, size=n)
+        pos = rsa_cube(radii, 0.15, rng)
+        agg = Aggregate(f"g{i}", pos, radii, complex(1.45 + 0.02 * i, 0.01), 0.5 + 0.02 * i, 4, i)
+        polar, azim, pol = incidences(1)
+        reqs.append(Request(i, 0.0, agg, polar[:R], azim[:R], pol[:R]))
+    cfg = ServeConfig(max_slots=2, rtol=1e-8, keep_solutions=True)
+    assert all(groupable(q, cfg) for q in reqs)
+    mixed = Server(cfg, device=cuda_device).run(reqs, realtime=False)
+    sizes = {r.stats.get("group_size") for r in mixed}
+    assert max(sizes) > 1  # at least one group of several requests
+    for r, q in zip(mixed, reqs):
+        assert r.error is None, r.error
+        alone = solve_group([q], cfg, cuda_device)[0]
+        assert rel_err(r.x, alone.x) <= 1e-12
+        assert np.allclose(r.c_ext, alone.c_ext, rtol=1e-12, atol=0)

@@ -59,6 +59,8 @@ SIGNATURES = {
     "yasf_last_cuda_error": [],
     "yasf_kernel_launches": [],
     "yasf_test_stall": [_i, _i, _d],
+    "yasf_grouped_workspace_size": [_vp, _i, _vp, _i, _c.POINTER(_sz)],
+    "yasf_grouped_solve": [_vp, _i, _vp, _d, _i, _i, _d, _i, _vp, _sz, _dp, _dp, _vp],
     "yasf_plane_wave_rhs": [_i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _vp],
     "yasf_plan_create": [_i, _vp, _c.POINTER(_vp)],
     "yasf_plan_destroy": [_vp],
@@ -147,3 +149,10 @@ def test_stall(role: int, contract_polls: int = 0, panel_wait_seconds: float = 0
     one producer role from delivering, with shortened wait bounds. ``YASF_STALL_NONE`` restores
     normal launches."""
     call("yasf_test_stall", int(role), int(contract_polls), float(panel_wait_seconds))
+
+
+class YasfProblem(_c.Structure):
+    """``yasf_problem`` of include/yasf_b200.h: one aggregate of a grouped solve."""
+
+    _fields_ = [("n_particles", _i), ("positions", _vp), ("k_medium", _d), ("tmat", _vp), ("b", _vp),
+                ("x", _vp), ("nrhs", _i)]

@@ -62,7 +62,7 @@ int contract_resident_blocks(int precision, int threads);
 
 // Resident contraction blocks per SM for (lmax, precision, threads), from the occupancy query
 // (cached per device state of this process).
-static int resident_blocks(int lmax, int precision, int threads) {
+int resident_blocks(int lmax, int precision, int threads) {
   static std::mutex mu;
   static int cache[YASF_LMAX_MAX + 1][2][5] = {};
   const int pi = precision == YASF_C64 ? 1 : 0, wi = std::min(4, std::max(1, threads / 32));

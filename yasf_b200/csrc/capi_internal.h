@@ -81,6 +81,9 @@ int coupling_column(const yasf_plan* plan, int n_particles, const double* positi
 int dispatch_contract(int lmax, int precision, bool regular, const ContractArgs& a, int tiles,
                       int chunks, int threads, cudaStream_t stream);
 
+// Resident blocks per SM of the contraction kernel for (lmax, precision, threads per block).
+int resident_blocks(int lmax, int precision, int threads);
+
 int validate_coupling(const yasf_plan* plan, int n_particles, const double* positions,
                       double k, int precision);
 

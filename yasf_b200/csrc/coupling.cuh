@@ -500,6 +500,94 @@ __global__ void __launch_bounds__(128) contract_kernel(ContractArgs a) {
                                                               uses, issued);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Persistent work-queue contraction over many right-hand sides of different aggregates.
+// Every column (one right-hand side of one aggregate; all of one lmax) contributes
+// tiles x chunks x bundles work items, numbered by item_pre. Resident blocks take items from a
+// device counter until none is left, so aggregates of very different sizes share one launch and
+// one set of resident blocks; a column whose live flag is 0 is skipped. The stage barriers are
+// initialised once per block and their phases carried from item to item.
+struct GroupColumn {
+  const double* pos;      // positions of the column's aggregate (N, 3)
+  const double2* tmat;    // T of the column's aggregate (master epilogue; unused by the contraction)
+  const void* v;          // the column's V stream (VEntry), bundle-major
+  void* partial;          // the column's partial sums (chunks, N, nmax)
+  double k;
+  int n_particles;
+  int tiles;
+  int chunks;
+  int sources_per_chunk;
+};
+
+struct GroupedContractArgs {
+  const GroupColumn* cols;
+  const int* live;
+  const long long* item_pre;     // [n_cols + 1]
+  int n_cols;
+  long long total_items;
+  unsigned long long* counter;   // work-queue head, zero at launch
+  const LegendreTables* leg;
+  int nmax;
+  int n_bundles;
+  int bundle_begin[8];
+  int bundle_len[8];
+  int* err;
+  int poll_limit;
+  int stall;
+};
+
+template <int L, typename Real>
+__global__ void __launch_bounds__(128) grouped_contract_kernel(GroupedContractArgs g) {
+  extern __shared__ __align__(128) char smem[];
+  __shared__ __align__(8) unsigned long long bars[2];
+  __shared__ long long item_s;
+  stage_barriers_init(bars);
+  unsigned uses[2] = {0u, 0u}, issued[2] = {0u, 0u};
+  ContractArgs a{};
+  a.nmax = g.nmax;
+  a.leg = g.leg;
+  for (int b = 0; b < 8; ++b) {
+    a.bundle_begin[b] = g.bundle_begin[b];
+    a.bundle_len[b] = g.bundle_len[b];
+  }
+  a.err = g.err;
+  a.cutoff2 = -1.0;
+  a.poll_limit = g.poll_limit;
+  a.stall = g.stall;
+#pragma unroll 1
+  for (;;) {
+    if (threadIdx.x == 0) item_s = (long long)atomicAdd(g.counter, 1ull);
+    __syncthreads();
+    const long long item = item_s;
+    __syncthreads();  // every thread has the item before thread 0 takes the next one
+    if (item >= g.total_items) break;
+    int lo = 0, hi = g.n_cols;  // item_pre[lo] <= item < item_pre[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (g.item_pre[mid] <= item) lo = mid; else hi = mid;
+    }
+    if (!g.live[lo]) continue;
+    const GroupColumn col = g.cols[lo];
+    long long r = item - g.item_pre[lo];
+    const int bundle = (int)(r % g.n_bundles);
+    r /= g.n_bundles;
+    const int chunk = (int)(r % col.chunks);
+    const int tile = (int)(r / col.chunks);
+    a.n_particles = col.n_particles;
+    a.sources_per_chunk = col.sources_per_chunk;
+    a.k = col.k;
+    a.pos = col.pos;
+    a.v = col.v;
+    a.partial = col.partial;
+    if (!BundleDispatch<L, Real, false, num_bundles(L)>::run(a, bundle, tile, chunk, smem, bars, uses, issued))
+      break;  // a stage wait ran out: this block stops (the error word is set)
+  }
+}
+
+template <int L>
+cudaError_t launch_grouped_contract(int precision, const GroupedContractArgs& g, int blocks,
+                                    cudaStream_t stream);
+
 template <int L>
 constexpr int max_bundle_stream(int b = 0) {
   return b >= num_bundles(L) ? 0

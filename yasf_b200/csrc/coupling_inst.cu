@@ -37,6 +37,26 @@ cudaError_t launch_contract<YASF_INST_L>(int precision, bool regular, const Cont
 }
 
 template <>
+cudaError_t launch_grouped_contract<YASF_INST_L>(int precision, const GroupedContractArgs& g, int blocks,
+                                                 cudaStream_t stream) {
+  constexpr int L = YASF_INST_L;
+  const size_t stage = 2 * (size_t)max_bundle_stream<L>() * (precision == YASF_C64 ? sizeof(float4) : sizeof(double2));
+  cudaError_t e;
+  if (precision == YASF_C64) {
+    e = cudaFuncSetAttribute(grouped_contract_kernel<L, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stage);
+    if (e != cudaSuccess) return e;
+    YASF_COUNTED(grouped_contract_kernel<L, float><<<blocks, 128, stage, stream>>>(g));
+  } else {
+    e = cudaFuncSetAttribute(grouped_contract_kernel<L, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)stage);
+    if (e != cudaSuccess) return e;
+    YASF_COUNTED(grouped_contract_kernel<L, double><<<blocks, 128, stage, stream>>>(g));
+  }
+  return cudaGetLastError();
+}
+
+template <>
 int contract_resident_blocks<YASF_INST_L>(int precision, int threads) {
   constexpr int L = YASF_INST_L;
   const size_t stage = 2 * (size_t)max_bundle_stream<L>() * (precision == YASF_C64 ? sizeof(float4) : sizeof(double2));

@@ -561,3 +561,621 @@ extern "C" int yasf_batched_solve(const yasf_plan* plan, int n_particles, const 
   YASF_CUDA_TRY(cudaStreamSynchronize(s));
   return YASF_OK;
 }
+
+// =============================================================================================
+// Grouped solve: the right-hand sides of several aggregates of one lmax (different sphere counts,
+// positions, wavenumbers, T) in one lockstep refined GMRES. Column c (one right-hand side of one
+// aggregate) has n[c] = N_p nmax unknowns; the solver's vectors are ragged panels (column c at
+// offset voff[c], its Krylov basis at qoff[c]). Each operator application is three launches for
+// all live columns together: the source-side streams (grouped_vbuild_kernel), the persistent
+// work-queue contraction (grouped_contract_kernel) and the reduction with the master epilogue
+// (grouped_reduce_kernel). Float64 refinement as in yasf_batched_solve; no preconditioner.
+namespace yasf {
+
+namespace {
+
+constexpr int kGroupThreads = 128;   // threads per contraction block
+constexpr int kGroupSpc = 64;        // sources per chunk of a grouped column
+
+__device__ __forceinline__ int ragged_find(const long long* pre, int n, long long v) {
+  int lo = 0, hi = n;  // pre[lo] <= v < pre[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= v) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// partial[c][blk][k] = sum conj(Q_c[k]) w_c over the block's slice (live columns).
+__global__ void __launch_bounds__(256) gmdot_kernel(const long long* n, const long long* qoff, int nvec,
+                                                    const double2* Q, const double2* w, const long long* woff,
+                                                    const int* live, double2* partial) {
+  const int c = blockIdx.y;
+  if (!live[c]) return;
+  __shared__ double sr[8], si[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long nc = n[c];
+  const double2* wc = w + woff[c];
+  for (int k = 0; k < nvec; ++k) {
+    const double2* q = Q + qoff[c] + (size_t)k * nc;
+    double re = 0.0, im = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc; i += (long long)gridDim.x * blockDim.x) {
+      const double2 a = q[i], b = wc[i];
+      re += a.x * b.x + a.y * b.y;
+      im += a.x * b.y - a.y * b.x;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      re += __shfl_down_sync(0xffffffffu, re, off);
+      im += __shfl_down_sync(0xffffffffu, im, off);
+    }
+    if (lane == 0) { sr[wid] = re; si[wid] = im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tr = 0.0, ti = 0.0;
+      for (int t = 0; t < (int)(blockDim.x >> 5); ++t) { tr += sr[t]; ti += si[t]; }
+      partial[((size_t)c * gridDim.x + blockIdx.x) * nvec + k] = make_double2(tr, ti);
+    }
+    __syncthreads();
+  }
+}
+
+// w_c += sign * sum_k h_c[k] Q_c[k] (live columns; h_c at h + c * h_col).
+__global__ void __launch_bounds__(256) gupdate_kernel(const long long* n, const long long* qoff, int nvec,
+                                                      const double2* Q, const double2* h, long long h_col,
+                                                      double sign, double2* w, const long long* woff,
+                                                      const int* live) {
+  const int c = blockIdx.y;
+  if (!live[c]) return;
+  __shared__ double2 sh[512];
+  for (int k = threadIdx.x; k < nvec && k < 512; k += blockDim.x) sh[k] = h[(size_t)c * h_col + k];
+  __syncthreads();
+  const long long nc = n[c];
+  double2* wc = w + woff[c];
+  const double2* qc = Q + qoff[c];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc; i += (long long)gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < nvec; ++k) {
+      const double2 q = qc[(size_t)k * nc + i];
+      const double2 cc = sh[k];
+      re += cc.x * q.x - cc.y * q.y;
+      im += cc.x * q.y + cc.y * q.x;
+    }
+    double2 v = wc[i];
+    v.x += sign * re;
+    v.y += sign * im;
+    wc[i] = v;
+  }
+}
+
+// out_c (at out_off[c] + out_j n[c]) = in_c (at in_off[c]) / norm[c] for live columns, else zero.
+__global__ void gscale_kernel(const long long* n, const double2* in, const long long* in_off, const double* norm,
+                              double2* out, const long long* out_off, long long out_j, const int* live) {
+  const int c = blockIdx.y;
+  const double nv = norm[c];
+  const bool on = live[c] && nv > 0.0;
+  const double f = on ? 1.0 / nv : 0.0;
+  const long long nc = n[c];
+  const double2* ic = in + in_off[c];
+  double2* oc = out + out_off[c] + out_j * nc;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc; i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = on ? ic[i] : make_double2(0.0, 0.0);
+    oc[i] = make_double2(v.x * f, v.y * f);
+  }
+}
+
+// Ragged elementwise (columns with mask): mode 0: out = a - b ; 1: out += a ; 2: out = a.
+// Column c of a / b / out sits at ptr + off[c] (the same offsets for all three).
+__global__ void gax_kernel(const long long* n, const long long* off, int mode, const double2* a, const double2* b,
+                           double2* out, const int* mask) {
+  const int c = blockIdx.y;
+  if (mask && !mask[c]) return;
+  const long long nc = n[c];
+  const size_t base = off[c];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc; i += (long long)gridDim.x * blockDim.x) {
+    const double2 av = a[base + i];
+    if (mode == 0) {
+      const double2 bv = b[base + i];
+      out[base + i] = make_double2(av.x - bv.x, av.y - bv.y);
+    } else if (mode == 1) {
+      double2 o = out[base + i];
+      o.x += av.x;
+      o.y += av.y;
+      out[base + i] = o;
+    } else {
+      out[base + i] = av;
+    }
+  }
+}
+
+// Source-side streams of every live column: V_c[bundle][s][entry] from the column's input x_c at
+// in + in_off[c] + in_j n[c] (the stream layout of vbuild_kernel).
+struct GroupedVBuildArgs {
+  const GroupColumn* cols;
+  const int* live;
+  const long long* src_pre;   // [n_cols + 1] prefix of the columns' sphere counts
+  const long long* in_off;
+  const long long* n;
+  const double2* in;
+  long long in_j;
+  int n_cols;
+  long long total_src;
+  int nmax, total_entries, n_bundles;
+  int bundle_begin[8], bundle_len[8];
+  const int* entry_ptr;
+  const int* term_n2;
+  const double2* term_coef;
+};
+
+template <typename Real>
+__global__ void __launch_bounds__(256) grouped_vbuild_kernel(GroupedVBuildArgs a) {
+  using C = typename VEntry<Real>::T;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= a.total_entries) return;
+  int b = 0;
+  while (b + 1 < a.n_bundles && g >= a.bundle_begin[b + 1]) ++b;
+  const int t0 = __ldg(a.entry_ptr + g), t1 = __ldg(a.entry_ptr + g + 1);
+  for (long long gs = blockIdx.y; gs < a.total_src; gs += gridDim.y) {
+    const int c = ragged_find(a.src_pre, a.n_cols, gs);
+    if (!a.live[c]) continue;
+    const int s = (int)(gs - a.src_pre[c]);
+    const GroupColumn& col = a.cols[c];
+    const double2* xs = a.in + a.in_off[c] + a.in_j * a.n[c] + (size_t)s * a.nmax;
+    double re = 0.0, im = 0.0;
+    for (int t = t0; t < t1; ++t) {
+      const double2 cf = __ldg(a.term_coef + t);
+      const double2 xv = xs[__ldg(a.term_n2 + t)];
+      re = fma(cf.x, xv.x, re);
+      re = fma(-cf.y, xv.y, re);
+      im = fma(cf.x, xv.y, im);
+      im = fma(cf.y, xv.x, im);
+    }
+    C* out = reinterpret_cast<C*>(const_cast<void*>(col.v)) + (size_t)a.bundle_begin[b] * col.n_particles +
+             (size_t)s * a.bundle_len[b] + (g - a.bundle_begin[b]);
+    if constexpr (sizeof(Real) == 8) *out = make_double2(re, im);
+    else *out = make_float4((float)re, (float)im, -(float)im, (float)re);
+  }
+}
+
+// out_c = x_c - T_c (.) sum over chunks of the partials (live columns), NaN if a wait ran out.
+template <typename Real>
+__global__ void __launch_bounds__(256) grouped_reduce_kernel(const GroupColumn* cols, const int* live,
+                                                             const long long* elem_pre, int n_cols,
+                                                             long long total, int nmax, const double2* in,
+                                                             const long long* in_off, const long long* n,
+                                                             long long in_j, double2* out,
+                                                             const long long* out_off, const int* err) {
+  using Cx = typename Cplx<Real>::T;
+  const bool bad = *err != 0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int c = ragged_find(elem_pre, n_cols, e);
+    if (!live[c]) continue;
+    const long long i = e - elem_pre[c];
+    const GroupColumn& col = cols[c];
+    const long long nc = n[c];
+    double2 o;
+    if (bad) {
+      o = make_double2(nan(""), nan(""));
+    } else {
+      const Cx* pp = reinterpret_cast<const Cx*>(col.partial);
+      double re = 0.0, im = 0.0;
+      for (int ch = 0; ch < col.chunks; ++ch) {
+        const Cx v = pp[(size_t)ch * nc + i];
+        re += (double)v.x;
+        im += (double)v.y;
+      }
+      const double2 t = col.tmat[i];
+      const double2 xv = in[in_off[c] + in_j * nc + i];
+      o = make_double2(xv.x - (t.x * re - t.y * im), xv.y - (t.x * im + t.y * re));
+    }
+    out[out_off[c] + i] = o;
+  }
+}
+
+struct GroupWs {
+  int C = 0;
+  long long sum_n = 0, sum_q = 0, total_src = 0, items[2] = {0, 0};
+  size_t o_col64 = 0, o_col32 = 0, o_ipre64 = 0, o_ipre32 = 0, o_spre = 0, o_epre = 0, o_n = 0, o_voff = 0,
+         o_qoff = 0;
+  size_t o_V = 0, o_P = 0, o_X = 0, o_B = 0, o_W = 0, o_Z = 0, o_R = 0, o_D = 0, o_Q = 0, o_H = 0, o_gc = 0,
+         o_gs = 0, o_S = 0, o_y = 0, o_part = 0, o_vec = 0, o_int = 0, o_cnt = 0, total = 0;
+  std::vector<long long> n, voff, qoff, src_pre, elem_pre, ipre64, ipre32, vsoff, psoff;
+  std::vector<int> prob, chunks, tiles64, tiles32;
+};
+
+GroupWs group_layout(const yasf_plan* plan, int P, const yasf_problem* pr, int m) {
+  GroupWs L;
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const int nmax = plan->nmax;
+  for (int p = 0; p < P; ++p)
+    for (int j = 0; j < pr[p].nrhs; ++j) L.prob.push_back(p);
+  const int C = L.C = (int)L.prob.size();
+  long long vs = 0, ps = 0;
+  L.src_pre.push_back(0);
+  L.elem_pre.push_back(0);
+  L.ipre64.push_back(0);
+  L.ipre32.push_back(0);
+  for (int c = 0; c < C; ++c) {
+    const int N = pr[L.prob[c]].n_particles;
+    const long long nc = (long long)N * nmax;
+    L.n.push_back(nc);
+    L.voff.push_back(L.sum_n);
+    L.qoff.push_back(L.sum_q);
+    L.sum_n += nc;
+    L.sum_q += (long long)(m + 1) * nc;
+    const int spc = std::min(N, kGroupSpc);
+    const int ch = (N + spc - 1) / spc;
+    L.chunks.push_back(ch);
+    L.tiles64.push_back((N + kGroupThreads - 1) / kGroupThreads);
+    L.tiles32.push_back((N + 2 * kGroupThreads - 1) / (2 * kGroupThreads));
+    L.src_pre.push_back(L.src_pre.back() + N);
+    L.elem_pre.push_back(L.elem_pre.back() + nc);
+    L.ipre64.push_back(L.ipre64.back() + (long long)L.tiles64.back() * ch * plan->n_bundles);
+    L.ipre32.push_back(L.ipre32.back() + (long long)L.tiles32.back() * ch * plan->n_bundles);
+    L.vsoff.push_back(vs);
+    L.psoff.push_back(ps);
+    vs += up((size_t)N * plan->total_entries * 16);
+    ps += up((size_t)ch * nc * 16);
+  }
+  L.total_src = L.src_pre.back();
+  L.items[0] = L.ipre64.back();
+  L.items[1] = L.ipre32.back();
+  size_t o = 0;
+  const size_t cz = std::max(C, 1);
+  L.o_col64 = o; o += up(cz * sizeof(GroupColumn));
+  L.o_col32 = o; o += up(cz * sizeof(GroupColumn));
+  L.o_ipre64 = o; o += up((cz + 1) * 8);
+  L.o_ipre32 = o; o += up((cz + 1) * 8);
+  L.o_spre = o; o += up((cz + 1) * 8);
+  L.o_epre = o; o += up((cz + 1) * 8);
+  L.o_n = o; o += up(cz * 8);
+  L.o_voff = o; o += up(cz * 8);
+  L.o_qoff = o; o += up(cz * 8);
+  L.o_V = o; o += (size_t)vs;
+  L.o_P = o; o += (size_t)ps;
+  const size_t vb = up((size_t)L.sum_n * 16);
+  L.o_X = o; o += vb;
+  L.o_B = o; o += vb;
+  L.o_W = o; o += vb;
+  L.o_Z = o; o += vb;
+  L.o_R = o; o += vb;
+  L.o_D = o; o += vb;
+  L.o_Q = o; o += up((size_t)L.sum_q * 16);
+  L.o_H = o; o += up(cz * m * (m + 1) * 16);
+  L.o_gc = o; o += up(cz * m * 8);
+  L.o_gs = o; o += up(cz * m * 16);
+  L.o_S = o; o += up(cz * (m + 1) * 16);
+  L.o_y = o; o += up(cz * (m + 1) * 16);
+  L.o_part = o; o += up(cz * kBDot * (m + 1) * 16);
+  L.o_vec = o; o += up(cz * 8 * 8);
+  L.o_int = o; o += up(cz * 4 * 4);
+  L.o_cnt = o; o += 256;  // work-queue counter and error word
+  L.total = o;
+  return L;
+}
+
+int group_check(const yasf_plan* plan, int P, const yasf_problem* pr) {
+  if (!plan || P <= 0 || !pr) return YASF_ERR_INVALID_ARGUMENT;
+  for (int p = 0; p < P; ++p) {
+    const yasf_problem& q = pr[p];
+    int st = validate_coupling(plan, q.n_particles, q.positions, q.k_medium, YASF_C128);
+    if (st != YASF_OK) return st;
+    if (q.nrhs <= 0 || !q.tmat || !q.b || !q.x) return YASF_ERR_INVALID_ARGUMENT;
+    if (!aligned16(q.tmat) || !aligned16(q.b) || !aligned16(q.x)) return YASF_ERR_ALIGNMENT;
+  }
+  return YASF_OK;
+}
+
+}  // namespace
+
+int dispatch_grouped_contract(int lmax, int precision, const GroupedContractArgs& g, int blocks, cudaStream_t s) {
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (lmax) {
+    case 1: e = launch_grouped_contract<1>(precision, g, blocks, s); break;
+    case 2: e = launch_grouped_contract<2>(precision, g, blocks, s); break;
+    case 3: e = launch_grouped_contract<3>(precision, g, blocks, s); break;
+    case 4: e = launch_grouped_contract<4>(precision, g, blocks, s); break;
+    case 5: e = launch_grouped_contract<5>(precision, g, blocks, s); break;
+    case 6: e = launch_grouped_contract<6>(precision, g, blocks, s); break;
+    case 7: e = launch_grouped_contract<7>(precision, g, blocks, s); break;
+    case 8: e = launch_grouped_contract<8>(precision, g, blocks, s); break;
+    default: return YASF_ERR_UNSUPPORTED;
+  }
+  YASF_CUDA_TRY(e);
+  return YASF_OK;
+}
+
+}  // namespace yasf
+
+extern "C" int yasf_grouped_workspace_size(const yasf_plan* plan, int n_problems, const yasf_problem* problems,
+                                           int restart, size_t* bytes) {
+  if (!bytes || restart <= 0 || restart > 512) return YASF_ERR_INVALID_ARGUMENT;
+  if (int st = group_check(plan, n_problems, problems)) return st;
+  *bytes = group_layout(plan, n_problems, problems, restart).total;
+  return YASF_OK;
+}
+
+extern "C" int yasf_grouped_solve(const yasf_plan* plan, int n_problems, const yasf_problem* problems,
+                                  double rtol, int restart, int max_refine, double inner_rtol, int inner_precision,
+                                  void* workspace, size_t workspace_bytes, double* stats, double* column_residuals,
+                                  void* stream) {
+  if (int st = group_check(plan, n_problems, problems)) return st;
+  if (restart <= 0 || restart > 512 || max_refine < 1 || !(rtol >= 0.0) || !(inner_rtol > 0.0) ||
+      (inner_precision != YASF_C64 && inner_precision != YASF_C128))
+    return YASF_ERR_INVALID_ARGUMENT;
+  const int m = restart;
+  const GroupWs L = group_layout(plan, n_problems, problems, m);
+  if (!workspace || workspace_bytes < L.total) return YASF_ERR_WORKSPACE;
+  if (!aligned16(workspace)) return YASF_ERR_ALIGNMENT;
+  const int C = L.C;
+  const int nmax = plan->nmax;
+  char* ws = static_cast<char*>(workspace);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  auto dv = [&](size_t o) { return reinterpret_cast<double2*>(ws + o); };
+  const long long* d_n = reinterpret_cast<const long long*>(ws + L.o_n);
+  const long long* d_voff = reinterpret_cast<const long long*>(ws + L.o_voff);
+  const long long* d_qoff = reinterpret_cast<const long long*>(ws + L.o_qoff);
+  double2 *X = dv(L.o_X), *Bp = dv(L.o_B), *W = dv(L.o_W), *Z = dv(L.o_Z), *Rr = dv(L.o_R), *D = dv(L.o_D),
+          *Q = dv(L.o_Q), *H = dv(L.o_H), *gs = dv(L.o_gs), *S = dv(L.o_S), *yv = dv(L.o_y), *part = dv(L.o_part);
+  double* gc = reinterpret_cast<double*>(ws + L.o_gc);
+  double* vec = reinterpret_cast<double*>(ws + L.o_vec);
+  double *d_bnorm = vec, *d_beta = vec + C, *d_h0 = vec + 2 * C, *d_h1 = vec + 3 * C, *d_presid = vec + 4 * C,
+         *d_rnorm = vec + 5 * C;
+  int* ints = reinterpret_cast<int*>(ws + L.o_int);
+  int *d_live = ints, *d_brk = ints + C, *d_stop = ints + 2 * C, *d_active = ints + 3 * C;
+  unsigned long long* d_counter = reinterpret_cast<unsigned long long*>(ws + L.o_cnt);
+  int* d_err = reinterpret_cast<int*>(ws + L.o_cnt + 8);
+
+  // ---- tables: columns (per precision: tiles differ), prefixes, lengths, offsets ---------------
+  {
+    std::vector<GroupColumn> c64(C), c32(C);
+    for (int c = 0; c < C; ++c) {
+      const yasf_problem& q = problems[L.prob[c]];
+      GroupColumn g{};
+      g.pos = q.positions;
+      g.tmat = reinterpret_cast<const double2*>(q.tmat);
+      g.v = ws + L.o_V + L.vsoff[c];
+      g.partial = ws + L.o_P + L.psoff[c];
+      g.k = q.k_medium;
+      g.n_particles = q.n_particles;
+      g.chunks = L.chunks[c];
+      g.sources_per_chunk = std::min(q.n_particles, kGroupSpc);
+      g.tiles = L.tiles64[c];
+      c64[c] = g;
+      g.tiles = L.tiles32[c];
+      c32[c] = g;
+    }
+    auto put = [&](size_t off, const void* src, size_t bytes) -> int {
+      YASF_CUDA_TRY(cudaMemcpyAsync(ws + off, src, bytes, cudaMemcpyHostToDevice, s));
+      return YASF_OK;
+    };
+    int st = YASF_OK;
+    if ((st = put(L.o_col64, c64.data(), C * sizeof(GroupColumn))) ||
+        (st = put(L.o_col32, c32.data(), C * sizeof(GroupColumn))) ||
+        (st = put(L.o_ipre64, L.ipre64.data(), (C + 1) * 8)) || (st = put(L.o_ipre32, L.ipre32.data(), (C + 1) * 8)) ||
+        (st = put(L.o_spre, L.src_pre.data(), (C + 1) * 8)) || (st = put(L.o_epre, L.elem_pre.data(), (C + 1) * 8)) ||
+        (st = put(L.o_n, L.n.data(), C * 8)) || (st = put(L.o_voff, L.voff.data(), C * 8)) ||
+        (st = put(L.o_qoff, L.qoff.data(), C * 8)))
+      return st;
+    // the caller's right-hand sides into the packed panel
+    for (int c = 0, first = 0; c < C; ++c) {
+      const yasf_problem& q = problems[L.prob[c]];
+      if (c > 0 && L.prob[c] != L.prob[c - 1]) first = c;
+      const double* src = q.b + 2 * (size_t)(c - first) * L.n[c];
+      YASF_CUDA_TRY(cudaMemcpyAsync(Bp + L.voff[c], src, L.n[c] * 16, cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  YASF_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+  int sms = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  // operator application A at `prec` on the live columns: in_c at in + in_off[c] + in_j n[c],
+  // out_c at out + voff[c]
+  long long mv_inner = 0, mv64 = 0;
+  auto apply = [&](int prec, const double2* in, const long long* in_off, long long in_j, double2* out,
+                   const int* live) -> int {
+    GroupedVBuildArgs va{};
+    va.cols = reinterpret_cast<const GroupColumn*>(ws + (prec == YASF_C64 ? L.o_col32 : L.o_col64));
+    va.live = live;
+    va.src_pre = reinterpret_cast<const long long*>(ws + L.o_spre);
+    va.in_off = in_off;
+    va.n = d_n;
+    va.in = in;
+    va.in_j = in_j;
+    va.n_cols = C;
+    va.total_src = L.total_src;
+    va.nmax = nmax;
+    va.total_entries = plan->total_entries;
+    va.n_bundles = plan->n_bundles;
+    for (int b = 0; b < 8; ++b) {
+      va.bundle_begin[b] = plan->bundle_begin[b];
+      va.bundle_len[b] = plan->bundle_len[b];
+    }
+    va.entry_ptr = plan->d_entry_ptr;
+    va.term_n2 = plan->d_term_n2;
+    va.term_coef = plan->d_term_coef;
+    const dim3 vgrid((plan->total_entries + 255) / 256, (unsigned)std::min<long long>(L.total_src, 65535));
+    if (prec == YASF_C64) YASF_COUNTED(grouped_vbuild_kernel<float><<<vgrid, 256, 0, s>>>(va));
+    else YASF_COUNTED(grouped_vbuild_kernel<double><<<vgrid, 256, 0, s>>>(va));
+    YASF_CUDA_TRY(cudaGetLastError());
+    GroupedContractArgs ga{};
+    ga.cols = va.cols;
+    ga.live = live;
+    ga.item_pre = reinterpret_cast<const long long*>(ws + (prec == YASF_C64 ? L.o_ipre32 : L.o_ipre64));
+    ga.n_cols = C;
+    ga.total_items = L.items[prec == YASF_C64 ? 1 : 0];
+    ga.counter = d_counter;
+    ga.leg = plan->d_leg;
+    ga.nmax = nmax;
+    ga.n_bundles = plan->n_bundles;
+    for (int b = 0; b < 8; ++b) {
+      ga.bundle_begin[b] = plan->bundle_begin[b];
+      ga.bundle_len[b] = plan->bundle_len[b];
+    }
+    ga.err = d_err;
+    ga.poll_limit = stall_hook().contract_polls;
+    ga.stall = stall_hook().role == YASF_STALL_CONTRACT ? 1 : 0;
+    YASF_CUDA_TRY(cudaMemsetAsync(d_counter, 0, sizeof(unsigned long long), s));
+    const int resident = std::max(1, resident_blocks(plan->lmax, prec, kGroupThreads));
+    const int blocks = (int)std::min<long long>(ga.total_items, (long long)resident * sms);
+    if (int st = dispatch_grouped_contract(plan->lmax, prec, ga, std::max(1, blocks), s)) return st;
+    const int rblocks = (int)std::min<long long>((L.sum_n + 255) / 256, 8192);
+    if (prec == YASF_C64)
+      YASF_COUNTED(grouped_reduce_kernel<float><<<rblocks, 256, 0, s>>>(
+          va.cols, live, reinterpret_cast<const long long*>(ws + L.o_epre), C, L.sum_n, nmax, in, in_off, d_n,
+          in_j, out, d_voff, d_err));
+    else
+      YASF_COUNTED(grouped_reduce_kernel<double><<<rblocks, 256, 0, s>>>(
+          va.cols, live, reinterpret_cast<const long long*>(ws + L.o_epre), C, L.sum_n, nmax, in, in_off, d_n,
+          in_j, out, d_voff, d_err));
+    YASF_CUDA_TRY(cudaGetLastError());
+    return YASF_OK;
+  };
+  const dim3 pgrid(256, C);
+  std::vector<int> h_live(C), h_active(C), h_stop(C), h_brk(C);
+  auto to_host_d = [&](const double* src, double* dst, int count) -> int {
+    YASF_CUDA_TRY(cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyDeviceToHost, s));
+    YASF_CUDA_TRY(cudaStreamSynchronize(s));
+    return YASF_OK;
+  };
+  auto to_dev_i = [&](int* dst, const int* src) -> int {
+    YASF_CUDA_TRY(cudaMemcpyAsync(dst, src, C * sizeof(int), cudaMemcpyHostToDevice, s));
+    return YASF_OK;
+  };
+  auto norms = [&](const double2* V, const long long* off, double* dst, const int* mask) -> int {
+    YASF_COUNTED(gmdot_kernel<<<dim3(kBDot, C), 256, 0, s>>>(d_n, off, 1, V, V, off, mask, part));
+    YASF_COUNTED(bfinal_kernel<<<dim3(1, C), 64, 0, s>>>(1, kBDot, part, nullptr, 0, 0, dst, mask));
+    YASF_CUDA_TRY(cudaGetLastError());
+    return YASF_OK;
+  };
+  const double eps = 2.220446049250313e-16;
+  int st = YASF_OK;
+  for (int c = 0; c < C; ++c) h_active[c] = 1;
+  if ((st = to_dev_i(d_active, h_active.data()))) return st;
+  if ((st = norms(Bp, d_voff, d_bnorm, d_active))) return st;
+  std::vector<double> bnorm(C);
+  if ((st = to_host_d(d_bnorm, bnorm.data(), C))) return st;
+  for (int c = 0; c < C; ++c)
+    if (!std::isfinite(bnorm[c])) return YASF_ERR_NOT_FINITE;
+  YASF_CUDA_TRY(cudaMemsetAsync(X, 0, (size_t)L.sum_n * 16, s));
+  YASF_COUNTED(gax_kernel<<<pgrid, 256, 0, s>>>(d_n, d_voff, 2, Bp, nullptr, Rr, nullptr));
+  std::vector<double> rnorm(bnorm);
+  int refine = 0;
+  long long inner_steps = 0;
+  for (int c = 0; c < C; ++c) h_active[c] = rnorm[c] > rtol * bnorm[c];
+  for (refine = 0; refine < max_refine; ++refine) {
+    bool any = false;
+    for (int c = 0; c < C; ++c) any |= h_active[c] != 0;
+    if (!any) break;
+    h_live = h_active;
+    if ((st = to_dev_i(d_live, h_live.data()))) return st;
+    if ((st = norms(Rr, d_voff, d_beta, d_live))) return st;
+    YASF_COUNTED(gscale_kernel<<<pgrid, 256, 0, s>>>(d_n, Rr, d_voff, d_beta, Q, d_qoff, 0, d_live));
+    YASF_COUNTED(bstart_kernel<<<(C + 63) / 64, 64, 0, s>>>(C, m, d_beta, S, d_live));
+    YASF_CUDA_TRY(cudaGetLastError());
+    std::vector<double> beta(C);
+    if ((st = to_host_d(d_beta, beta.data(), C))) return st;
+    for (int c = 0; c < C; ++c) h_stop[c] = -1;
+    for (int j = 0; j < m; ++j) {
+      if ((st = apply(inner_precision, Q, d_qoff, j, W, d_live))) return st;
+      ++mv_inner;
+      if ((st = norms(W, d_voff, d_h0, d_live))) return st;
+      double2* hcol = H + (size_t)j * (m + 1);
+      for (int pass = 0; pass < 2; ++pass) {
+        YASF_COUNTED(gmdot_kernel<<<dim3(kBDot, C), 256, 0, s>>>(d_n, d_qoff, j + 1, Q, W, d_voff, d_live, part));
+        if (pass == 0) {
+          YASF_COUNTED(bfinal_kernel<<<dim3(j + 1, C), 64, 0, s>>>(j + 1, kBDot, part, hcol, (long long)m * (m + 1), 0,
+                                                                 nullptr, d_live));
+          YASF_COUNTED(gupdate_kernel<<<pgrid, 256, 0, s>>>(d_n, d_qoff, j + 1, Q, hcol, (long long)m * (m + 1), -1.0,
+                                                          W, d_voff, d_live));
+        } else {
+          YASF_COUNTED(bfinal_kernel<<<dim3(j + 1, C), 64, 0, s>>>(j + 1, kBDot, part, yv, m + 1, 0, nullptr, d_live));
+          YASF_COUNTED(gupdate_kernel<<<pgrid, 256, 0, s>>>(d_n, d_qoff, j + 1, Q, yv, m + 1, -1.0, W, d_voff, d_live));
+          YASF_COUNTED(bfinal_kernel<<<dim3(j + 1, C), 64, 0, s>>>(j + 1, kBDot, part, hcol, (long long)m * (m + 1), 1,
+                                                                 nullptr, d_live));
+        }
+        YASF_CUDA_TRY(cudaGetLastError());
+      }
+      if ((st = norms(W, d_voff, d_h1, d_live))) return st;
+      YASF_COUNTED(gscale_kernel<<<pgrid, 256, 0, s>>>(d_n, W, d_voff, d_h1, Q, d_qoff, j + 1, d_live));
+      YASF_COUNTED(bgivens_kernel<<<(C + 63) / 64, 64, 0, s>>>(C, j, m, H, gc, gs, S, d_h0, d_h1, d_presid, d_brk,
+                                                             d_live, eps));
+      YASF_CUDA_TRY(cudaGetLastError());
+      std::vector<double> presid(C);
+      if ((st = to_host_d(d_presid, presid.data(), C))) return st;
+      YASF_CUDA_TRY(cudaMemcpyAsync(h_brk.data(), d_brk, C * sizeof(int), cudaMemcpyDeviceToHost, s));
+      YASF_CUDA_TRY(cudaStreamSynchronize(s));
+      inner_steps++;
+      bool any_live = false;
+      for (int c = 0; c < C; ++c) {
+        if (!h_live[c]) continue;
+        if (!std::isfinite(presid[c])) return YASF_ERR_NOT_FINITE;
+        if (presid[c] <= inner_rtol * beta[c] || h_brk[c] || j == m - 1) {
+          h_stop[c] = j;
+          h_live[c] = 0;
+        } else {
+          any_live = true;
+        }
+      }
+      if ((st = to_dev_i(d_live, h_live.data()))) return st;
+      if (!any_live) break;
+    }
+    // ---- D_c = Q_c y_c ; X += D ------------------------------------------------------------------
+    if ((st = to_dev_i(d_stop, h_stop.data()))) return st;
+    YASF_COUNTED(bbacksolve_kernel<<<(C + 63) / 64, 64, 0, s>>>(C, m, d_stop, H, S, yv));
+    YASF_CUDA_TRY(cudaMemsetAsync(D, 0, (size_t)L.sum_n * 16, s));
+    std::vector<int> has(C);
+    int maxstop = -1;
+    for (int c = 0; c < C; ++c) {
+      has[c] = h_stop[c] >= 0;
+      maxstop = std::max(maxstop, h_stop[c]);
+    }
+    if ((st = to_dev_i(d_live, has.data()))) return st;
+    if (maxstop >= 0)
+      YASF_COUNTED(gupdate_kernel<<<pgrid, 256, 0, s>>>(d_n, d_qoff, maxstop + 1, Q, yv, m + 1, 1.0, D, d_voff, d_live));
+    YASF_COUNTED(gax_kernel<<<pgrid, 256, 0, s>>>(d_n, d_voff, 1, D, nullptr, X, d_live));
+    YASF_CUDA_TRY(cudaGetLastError());
+    // ---- float64 residual of the active columns ----------------------------------------------
+    if ((st = to_dev_i(d_active, h_active.data()))) return st;
+    if ((st = apply(YASF_C128, X, d_voff, 0, W, d_active))) return st;
+    ++mv64;
+    YASF_COUNTED(gax_kernel<<<pgrid, 256, 0, s>>>(d_n, d_voff, 0, Bp, W, Rr, d_active));
+    if ((st = norms(Rr, d_voff, d_rnorm, d_active))) return st;
+    std::vector<double> rn(C);
+    if ((st = to_host_d(d_rnorm, rn.data(), C))) return st;
+    for (int c = 0; c < C; ++c) {
+      if (!h_active[c]) continue;
+      if (!std::isfinite(rn[c])) return YASF_ERR_NOT_FINITE;
+      rnorm[c] = rn[c];
+      if (rnorm[c] <= rtol * bnorm[c]) h_active[c] = 0;
+    }
+  }
+  // solutions back into the caller's columns
+  for (int c = 0, first = 0; c < C; ++c) {
+    const yasf_problem& q = problems[L.prob[c]];
+    if (c > 0 && L.prob[c] != L.prob[c - 1]) first = c;
+    YASF_CUDA_TRY(cudaMemcpyAsync(q.x + 2 * (size_t)(c - first) * L.n[c], X + L.voff[c], L.n[c] * 16,
+                                  cudaMemcpyDeviceToDevice, s));
+  }
+  double worst = 0.0;
+  int unconverged = 0;
+  for (int c = 0; c < C; ++c) {
+    const double rel = bnorm[c] > 0.0 ? rnorm[c] / bnorm[c] : 0.0;
+    worst = std::max(worst, rel);
+    unconverged += rnorm[c] > rtol * bnorm[c];
+    if (column_residuals) column_residuals[c] = rel;
+  }
+  if (stats) {
+    stats[0] = (double)inner_steps;
+    stats[1] = (double)mv_inner;
+    stats[2] = (double)mv64;
+    stats[3] = worst;
+    stats[4] = (double)unconverged;
+    stats[5] = (double)refine;
+    stats[6] = (double)C;
+    stats[7] = (double)L.items[inner_precision == YASF_C64 ? 1 : 0];
+  }
+  YASF_CUDA_TRY(cudaStreamSynchronize(s));
+  return YASF_OK;
+}

@@ -278,6 +278,45 @@ class CouplingDevice:
         }
 
 
+def grouped_solve(items, rtol: float, restart: int = 30, max_refine: int = 8, inner_rtol: float = 1e-3,
+                  inner: str = "c64") -> tuple[list[torch.Tensor], dict]:
+    """Solve the right-hand sides of several aggregates of one lmax together (yasf_grouped_solve).
+
+    items: list of (CouplingDevice, tmat (n,), B (R, n)) on one device, sharing one translation
+    plan. Returns the solutions (one (R, n) tensor per item, in order) and the solve statistics;
+    the column residuals are listed aggregate by aggregate."""
+    if not items:
+        return [], {}
+    dev0 = items[0][0]
+    plan = dev0.plan
+    probs = (_lib.YasfProblem * len(items))()
+    outs, keep = [], []
+    for i, (dev, tmat, B) in enumerate(items):
+        if dev.plan is not plan:
+            raise ValueError("a grouped solve needs one translation plan (one lmax, one table, one device)")
+        cols = B.reshape(-1, dev.n).contiguous()
+        X = torch.empty_like(cols)
+        keep += [cols, tmat]
+        outs.append(X)
+        probs[i] = _lib.YasfProblem(dev.n_particles, dev.pos.data_ptr(), dev.k, tmat.data_ptr(), cols.data_ptr(),
+                                    X.data_ptr(), cols.shape[0])
+    restart = int(max(1, min(restart, 512)))
+    nb = ctypes.c_size_t()
+    call("yasf_grouped_workspace_size", plan.handle, len(items), probs, restart, ctypes.byref(nb))
+    ws = dev0.ws.get(nb.value)
+    C = sum(int(x.shape[0]) for x in outs)
+    stats = (ctypes.c_double * 8)()
+    colres = (ctypes.c_double * C)()
+    call("yasf_grouped_solve", plan.handle, len(items), probs, float(rtol), restart, int(max_refine),
+         float(inner_rtol), PRECISIONS[inner], _ptr(ws), nb.value, stats, colres, _stream_ptr())
+    info = {"inner_steps": int(stats[0]), "inner_applications": int(stats[1]), "applications_f64": int(stats[2]),
+            "worst_relative_residual": float(stats[3]), "unconverged": int(stats[4]),
+            "refinement_steps": int(stats[5]), "columns": int(stats[6]), "work_items": int(stats[7]),
+            "column_residuals": list(colres)}
+    del keep
+    return outs, info
+
+
 class DevicePreconditioner:
     """Block-Jacobi factors of (I - T W) on the device (C-ABI handle + block inversion)."""
 

@@ -9,10 +9,14 @@ incidences (directions x polarisations = R right-hand sides). The loop:
 - runs every admitted request on its own CUDA stream, so the kernels of in-flight solves
   interleave on the device while their GMRES state stays resident there;
 - solves in mixed precision: the batched refined solve (yasf_batched_solve) with the tensor-core
-  TF32 panel as the inner operator (complex64 coupling kernel for one or two columns; with ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for
-  the request's (lmax, N, R)), float64 residuals,
-  stopping at rtol (1e-6 by default, which keeps the extinction cross section well inside 1e-6 of
-  the float64 solution);
+  TF32 panel as the inner operator (complex64 coupling kernel for one or two columns; with
+  ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for the request's
+  (lmax, N, R)), float64 residuals, stopping at rtol (1e-6 by default, which keeps the extinction
+  cross section well inside 1e-6 of the float64 solution);
+- packs the small requests whose inner operator is the complex64 kernel (up to
+  ``group_max_spheres`` spheres) that have arrived, with the same lmax, into one grouped solve
+  (yasf_grouped_solve): every operator application of the group is one persistent work-queue
+  contraction for all of them, instead of a launch sequence per request;
 - reports per-request latency (completion - arrival, queueing included), p50/p99 and solves/s.
 
 The kernels are deterministic (no atomics in any reduction), so a request's result does not depend
@@ -47,6 +51,9 @@ class ServeConfig:
     inner_rtol: float = 1e-3
     keep_solutions: bool = False
     tuner: object | None = None           # an autotune.Autotuner: inner operator by measurement
+    group_small: bool = True              # small complex64-inner requests share one grouped solve
+    group_max_spheres: int = 600          # a request joins a group up to this many spheres
+    group_max_requests: int = 16          # requests per group
 
 
 @dataclass
@@ -141,6 +148,49 @@ def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> Reque
     return res
 
 
+def groupable(req: Request, cfg: ServeConfig) -> bool:
+    """A request joins a grouped solve when its inner operator is the complex64 kernel (few
+    columns: the tensor-core panel does not pay) and it is small enough that launches, not
+    arithmetic, dominate its own solve."""
+    agg = req.aggregate
+    return (cfg.group_small and cfg.tuner is None and agg.n <= cfg.group_max_spheres
+            and inner_kind(agg.lmax, len(req.pol)) == "c64")
+
+
+def solve_group(reqs: list[Request], cfg: ServeConfig, device: torch.device) -> list[RequestResult]:
+    """Several small requests of one lmax in one grouped solve (yasf_grouped_solve): every
+    operator application of the group is one persistent work-queue contraction for all of them."""
+    from yasf_b200.device import grouped_solve
+
+    items, As, out = [], [], []
+    for req in reqs:
+        agg = req.aggregate
+        tm = mie_tmatrix_per_sphere(agg.lmax, agg.k, agg.radii, agg.refractive_index)
+        dev = CouplingDevice(agg.lmax, cached_translation_table(agg.lmax), agg.positions, agg.k, device)
+        tmat = torch.from_numpy(tm).to(device)
+        A, B = dev.plane_wave_rhs(tmat, req.polar, req.azimuthal, req.pol)
+        items.append((dev, tmat, B))
+        As.append(A)
+    Xs, st = grouped_solve(items, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
+                           inner_rtol=cfg.inner_rtol, inner="c64")
+    colres = st.pop("column_residuals")
+    c0 = 0
+    for req, A, X in zip(reqs, As, Xs):
+        agg = req.aggregate
+        R = len(req.pol)
+        res = RequestResult(req.rid, agg.n, agg.lmax, R)
+        res.c_ext = (-torch.real((A.conj() * X).sum(dim=1)) / agg.k**2 * np.pi).cpu().numpy()
+        res.stats = dict(st, inner="c64 grouped", group_size=len(reqs),
+                         worst_relative_residual=max(colres[c0:c0 + R]))
+        if max(colres[c0:c0 + R]) > cfg.rtol:
+            res.error = f"not converged: relative residual {max(colres[c0:c0 + R]):.3e}"
+        if cfg.keep_solutions:
+            res.x = X.cpu().numpy()
+        out.append(res)
+        c0 += R
+    return out
+
+
 class Server:
     """Continuous-batching loop over a request stream on one GPU."""
 
@@ -178,6 +228,23 @@ class Server:
         res.finished = time.perf_counter() - t0
         return res
 
+    def _worker_group(self, reqs: list[Request], t0: float) -> list[RequestResult]:
+        stream = getattr(self._tls, "stream", None)
+        if stream is None:
+            stream = torch.cuda.Stream(device=self.device)
+            self._tls.stream = stream
+        with torch.cuda.device(self.device), torch.cuda.stream(stream):
+            try:
+                out = solve_group(reqs, self.cfg, self.device)
+            except Exception as e:  # the group's requests report the error, the loop goes on
+                out = [RequestResult(q.rid, q.aggregate.n, q.aggregate.lmax, len(q.pol),
+                                     error=f"{type(e).__name__}: {e}") for q in reqs]
+            stream.synchronize()
+        fin = time.perf_counter() - t0
+        for r in out:
+            r.finished = fin
+        return out
+
     def run(self, requests: list[Request], realtime: bool = True) -> list[RequestResult]:
         """Serve the requests (arrival times in seconds from the start); returns results by rid."""
         for lmax in sorted({r.aggregate.lmax for r in requests}):
@@ -206,6 +273,26 @@ class Server:
                     if used + fp > budget:
                         break  # wait for memory to free up
                     pending.popleft()
+                    if self.device.type == "cuda" and groupable(req, self.cfg):
+                        # gather the arrived small requests of the same lmax into one grouped solve
+                        group, gfp = [req], fp
+                        for other in list(pending):
+                            if realtime and other.arrival > now:
+                                break
+                            if len(group) >= self.cfg.group_max_requests:
+                                break
+                            if other.aggregate.lmax != req.aggregate.lmax or not groupable(other, self.cfg):
+                                continue
+                            ofp = self._footprint(other, self.cfg)
+                            if used + gfp + ofp > budget:
+                                continue
+                            pending.remove(other)
+                            group.append(other)
+                            gfp += ofp
+                        used += gfp
+                        fut = pool.submit(self._worker_group, group, t0)
+                        inflight[fut] = (group, gfp, now)
+                        continue
                     used += fp
                     fut = pool.submit(self._worker, req, t0)
                     inflight[fut] = (req, fp, now)
@@ -220,10 +307,12 @@ class Server:
                 for f in done:
                     req, fp, admitted = inflight.pop(f)
                     used -= fp
-                    r = f.result()
-                    r.arrival = req.arrival if realtime else 0.0
-                    r.admitted = admitted
-                    results.append(r)
+                    got = f.result()
+                    reqs = req if isinstance(req, list) else [req]
+                    for q, r in zip(reqs, got if isinstance(got, list) else [got]):
+                        r.arrival = q.arrival if realtime else 0.0
+                        r.admitted = admitted
+                        results.append(r)
         return sorted(results, key=lambda r: r.rid)
 
 
