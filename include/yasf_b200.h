@@ -51,6 +51,15 @@ const char* yasf_last_cuda_error(void);
  * per-operator matvec_calls / uploads counters of yasfpy/coupling/cuda_dense.py:102-105. */
 unsigned long long yasf_kernel_launches(void);
 
+/* Tile shapes for the next launches and workspace-size queries FROM THIS HOST THREAD (0 keeps the
+ * built-in rule): contract_waves in {1, 2, 4, 8} sizes the coupling contraction's source chunks for
+ * that many waves of resident blocks (rule: 2); dpanel_cols in {32, 64} is the float64 dense panel's
+ * column tile (rule: 64 from 64 columns, else 32); panel_groups in {1, 2} is the tensor-core panel's
+ * column groups of 64 per block (rule: 2 when there are two, up to lmax 7). Set it before the size
+ * query of a solve and keep it for the solve. Chosen per (lmax, N, R) by yasf_b200.autotune; no
+ * reference counterpart. */
+int yasf_set_tiles(int contract_waves, int dpanel_cols, int panel_groups);
+
 /* Test hook for failure detection; no counterpart in the reference. Every wait inside a kernel of
  * this library is bounded: when it runs out, the kernel records an error word, writes NaN outputs,
  * frees what it holds and returns, so the CUDA context stays usable and the host sees

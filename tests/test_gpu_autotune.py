@@ -25,8 +25,41 @@ def test_tuned_choice_by_columns(cuda_device):
     tmat = torch.from_numpy(0.2 * (rng.normal(size=dev.n) + 1j * rng.normal(size=dev.n))).to(cuda_device)
     t = Autotuner()
     d1, d64 = t.decide(dev, tmat, 1), t.decide(dev, tmat, 64)
-    assert set(d64.ms_per_step) == {"c64", "tf32"} and all(v > 0 for v in d64.ms_per_step.values())
+    # every candidate (inner operator x tile shape) timed: contraction waves, panel, dense-panel tiles
+    assert {"c64/w1", "c64/w2", "c64/w4", "tf32/g0", "f64/c32", "f64/c64"} == set(d64.ms_per_step)
+    assert all(v > 0 for v in d64.ms_per_step.values())
     assert d64.inner == "tf32" and d1.inner == "c64"
+    assert d1.tiles.get("contract_waves") in (1, 2, 4) and d64.tiles.get("dpanel_cols") in (32, 64)
+
+
+def test_tile_shapes_give_the_same_products(cuda_device):
+    """Tile shapes change only how the work is split: every shape gives the same coupling product
+    (float64: identical partial-sum layout per chunk count, so agreement to rounding), the same
+    dense-panel result and the same tensor-core panel result."""
+    from conftest import rel_err
+
+    from yasf_b200._lib import set_tiles
+
+    rng = np.random.default_rng(3)
+    radii = rng.uniform(0.05, 0.12, size=150)
+    pos = rsa_cube(radii, 0.15, rng)
+    dev = CouplingDevice(4, translation_table_ab5(4), pos, 2 * np.pi / 0.55, cuda_device)
+    x = torch.from_numpy(rng.normal(size=(130, dev.n)) + 1j * rng.normal(size=(130, dev.n))).to(cuda_device)
+    ref = dev.coupling(x[0]).cpu().numpy()
+    refd = dev.dpanel(x[:40]).cpu().numpy()
+    refp = dev.panel(x).cpu().numpy()
+    try:
+        for w in (1, 2, 4, 8):
+            set_tiles(w, 0, 0)
+            assert rel_err(dev.coupling(x[0]).cpu().numpy(), ref) < 1e-13
+        for c in (32, 64):
+            set_tiles(0, c, 0)
+            assert rel_err(dev.dpanel(x[:40]).cpu().numpy(), refd) < 1e-13
+        for g in (1, 2):
+            set_tiles(0, 0, g)
+            assert rel_err(dev.panel(x).cpu().numpy(), refp) < 1e-6
+    finally:
+        set_tiles(0, 0, 0)
 
 
 def test_tuned_request_matches_rule(cuda_device):

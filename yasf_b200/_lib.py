@@ -59,6 +59,7 @@ SIGNATURES = {
     "yasf_last_cuda_error": [],
     "yasf_kernel_launches": [],
     "yasf_test_stall": [_i, _i, _d],
+    "yasf_set_tiles": [_i, _i, _i],
     "yasf_grouped_workspace_size": [_vp, _i, _vp, _i, _c.POINTER(_sz)],
     "yasf_grouped_solve": [_vp, _i, _vp, _d, _i, _i, _d, _i, _vp, _sz, _dp, _dp, _vp],
     "yasf_plane_wave_rhs": [_i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _vp],
@@ -156,3 +157,8 @@ class YasfProblem(_c.Structure):
 
     _fields_ = [("n_particles", _i), ("positions", _vp), ("k_medium", _d), ("tmat", _vp), ("b", _vp),
                 ("x", _vp), ("nrhs", _i)]
+
+
+def set_tiles(contract_waves: int = 0, dpanel_cols: int = 0, panel_groups: int = 0) -> None:
+    """Tile shapes of this host thread's next launches (yasf_set_tiles); zeros restore the rules."""
+    call("yasf_set_tiles", int(contract_waves), int(dpanel_cols), int(panel_groups))

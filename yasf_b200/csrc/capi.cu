@@ -13,8 +13,10 @@ namespace yasf {
 static thread_local std::string g_last_error;
 static std::atomic<unsigned long long> g_launches{0};
 static thread_local StallHook g_stall;
+static thread_local TileConfig g_tiles;
 
 const StallHook& stall_hook() { return g_stall; }
+const TileConfig& tile_config() { return g_tiles; }
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -97,8 +99,10 @@ CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int preci
   lay.threads = 32 * warps;
   lay.tiles = (N + lay.threads * rpt - 1) / (lay.threads * rpt);
   const int sms = sm_count_of(plan->device);
-  // Two full waves of resident blocks; the source loop is split into chunks to get there.
-  const long long want = 2LL * resident_blocks(plan->lmax, precision, lay.threads) * sms;
+  // Two full waves of resident blocks (or the thread's tile configuration); the source loop is
+  // split into chunks to get there.
+  const int waves = tile_config().contract_waves > 0 ? tile_config().contract_waves : 2;
+  const long long want = (long long)waves * resident_blocks(plan->lmax, precision, lay.threads) * sms;
   const long long base = (long long)lay.tiles * plan->n_bundles;
   int chunks = (int)std::max<long long>(1, (want + base - 1) / base);
   chunks = std::min(chunks, N);
@@ -286,6 +290,18 @@ extern "C" const char* yasf_status_string(int status) {
 }
 
 extern "C" const char* yasf_last_cuda_error(void) { return g_last_error.c_str(); }
+
+extern "C" int yasf_set_tiles(int contract_waves, int dpanel_cols, int panel_groups) {
+  const bool ok_w = contract_waves == 0 || contract_waves == 1 || contract_waves == 2 || contract_waves == 4 ||
+                    contract_waves == 8;
+  const bool ok_c = dpanel_cols == 0 || dpanel_cols == 32 || dpanel_cols == 64;
+  const bool ok_g = panel_groups == 0 || panel_groups == 1 || panel_groups == 2;
+  if (!ok_w || !ok_c || !ok_g) return YASF_ERR_INVALID_ARGUMENT;
+  g_tiles.contract_waves = contract_waves;
+  g_tiles.dpanel_cols = dpanel_cols;
+  g_tiles.panel_groups = panel_groups;
+  return YASF_OK;
+}
 
 extern "C" int yasf_test_stall(int role, int contract_polls, double panel_wait_seconds) {
   if (role < YASF_STALL_NONE || role > YASF_STALL_DPANEL) return YASF_ERR_INVALID_ARGUMENT;

@@ -100,6 +100,17 @@ struct StallHook {
 };
 const StallHook& stall_hook();
 
+// Tile shapes of the next launches and workspace queries from this host thread (set by
+// yasf_set_tiles; 0 = the built-in rule): waves of resident blocks the contraction's source chunks
+// are sized for, columns per tile of the float64 dense panel, column groups per tensor-core panel
+// block.
+struct TileConfig {
+  int contract_waves = 0;
+  int dpanel_cols = 0;
+  int panel_groups = 0;
+};
+const TileConfig& tile_config();
+
 int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::vector<unsigned>& goff,
                       std::vector<unsigned>& dst);
 int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std::vector<int2>& items,

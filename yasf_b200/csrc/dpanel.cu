@@ -511,7 +511,10 @@ int dpanel_build_items(int L, const double* ab5, std::vector<int4>& chunks, std:
 }
 
 // Column tile width for nrhs columns: 64 once there are 64 or more.
-static int dpanel_cols(int nrhs) { return nrhs >= 64 ? 64 : 32; }
+static int dpanel_cols(int nrhs) {
+  if (tile_config().dpanel_cols) return tile_config().dpanel_cols;
+  return nrhs >= 64 ? 64 : 32;
+}
 
 template <int L, int CT>
 static int launch_dpanel_ct(const DpArgs& da, cudaStream_t s) {

@@ -182,7 +182,10 @@ int panel_build_terms(int L, const double* ab5, std::vector<float>& coef, std::v
 // Right-hand-side groups of 64 per panel block: two as soon as there are two (each W_ij is then
 // generated once for 128 columns), padded to an even count whose extra columns are zero.
 // lmax 8 keeps one group per block: two groups' accumulators would exceed tensor memory.
-static int panel_groups_per_block(int groups, int lmax) { return groups >= 2 && lmax <= 7 ? 2 : 1; }
+static int panel_groups_per_block(int groups, int lmax) {
+  if (tile_config().panel_groups == 1) return 1;
+  return groups >= 2 && lmax <= 7 ? 2 : 1;
+}
 static int panel_padded_groups(int groups, int lmax) {
   const int ng = panel_groups_per_block(groups, lmax);
   return (groups + ng - 1) / ng * ng;

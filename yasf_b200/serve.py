@@ -136,12 +136,23 @@ def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> Reque
     tmat = torch.from_numpy(tm).to(device)
     # incident coefficients and right-hand sides of the R incidences, formed on the device
     A, Bt = dev.plane_wave_rhs(tmat, req.polar, req.azimuthal, req.pol)
-    inner = cfg.tuner.decide(dev, tmat, R).inner if cfg.tuner is not None else inner_kind(agg.lmax, R)
-    X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
-                              inner_rtol=cfg.inner_rtol, inner=inner)
+    decision = cfg.tuner.decide(dev, tmat, R) if cfg.tuner is not None else None
+    inner = decision.inner if decision is not None else inner_kind(agg.lmax, R)
+    if decision is not None:
+        decision.apply_tiles()  # tile shapes for this thread's launches
+    try:
+        X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
+                                  inner_rtol=cfg.inner_rtol, inner=inner)
+    finally:
+        if decision is not None:
+            from yasf_b200._lib import set_tiles
+
+            set_tiles(0, 0, 0)
     res.c_ext = (-torch.real((A.conj() * X).sum(dim=1)) / agg.k**2 * np.pi).cpu().numpy()
     st.pop("column_residuals", None)
     st["inner"] = inner
+    if decision is not None:
+        st["tiles"] = dict(decision.tiles)
     res.stats = st
     if cfg.keep_solutions:
         res.x = X.cpu().numpy()
