@@ -208,7 +208,12 @@ def run_reference(args, rank: int, world: int) -> None:
         "data": "synthetic (seeded RSA aggregate)",
         "config": {"workload": agg.name, "n_spheres": agg.n, "lmax": agg.lmax,
                    "unknowns": agg.n * 2 * agg.lmax * (agg.lmax + 2), "rtol": 1e-8,
-                   "parallelism": "host threads"},
+                   "parallelism": "host threads",
+                   "solve_model": "matvec time x the b200 solve's float64 matvec count; no preconditioner "
+                                  "cost: the reference's own block-Jacobi prepare cannot factor cells of two "
+                                  "or more spheres (yasfpy/preconditioner.py:408-423), and without it GMRES "
+                                  "needs more iterations, so this understates the reference's solve time",
+                   "translation_table": "the reference's own Numerics.translation_ab5 (committed fixture)"},
         "matvec_per_s": 1.0 / t_mv,
         "cpu_baseline": {
             "value": value, "unit": UNIT, "cores": threads, "kind": "port",
