@@ -652,6 +652,11 @@ def run_serve(args, rank: int, world: int) -> None:
     torch.cuda.synchronize()
     launches = lib.yasf_kernel_launches() - launches0
     summ = summarize(results)
+    grouped = [r for r in results if r.error is None and r.stats.get("group_size", 0) >= 1]
+    summ["grouped_requests"] = len(grouped)
+    summ["mean_group_size"] = (sum(r.stats["group_size"] for r in grouped) / len(grouped)) if grouped else None
+    summ["inner_operators"] = {k: sum(1 for r in results if r.error is None and r.stats.get("inner") == k)
+                               for k in ("tf32", "c64", "c64 grouped")}
     flat = gather_records([(r.rid, r.nrhs, r.latency, r.finished, r.error) for r in results])
     tot = serving_totals(flat, min(r.arrival for r in stream))
 
