@@ -283,9 +283,10 @@ int yasf_precond_finalize(yasf_precond* pc, void* stream);
 /* Replaces BlockDiagonalPreconditioner.apply (yasfpy/preconditioner.py:177-219, the unit-lower and
  * upper triangular solves of :470-519): gather with the pivots, a forward sweep with L and a
  * backward sweep with U over tile rows (one launch per tile row, float64 arithmetic on the complex64
- * factors, or the complex128 ones when kept and precision is YASF_C128), scatter. The first apply with
- * more columns than any before allocates the preconditioner's sweep buffer; applies of ONE
- * preconditioner on different streams at the same time race on that buffer. */
+ * factors, or the complex128 ones when kept and precision is YASF_C128), scatter. The sweeps are
+ * captured once per column count as a CUDA graph (on a private stream) and replayed on `stream`. The
+ * first apply with more columns than any before allocates the preconditioner's sweep buffer; applies
+ * of ONE preconditioner on different streams at the same time race on that buffer. */
 int yasf_precond_apply(const yasf_precond* pc, const double* x, double* y, int nrhs, long long ld,
                        int precision, void* stream);
 /* Device bytes held by the factors. */

@@ -51,6 +51,16 @@ struct yasf_precond {
   double2* d_dinv64 = nullptr;
   double2* d_z = nullptr;
   int z_cols = 0;
+  // the sweep launches of an apply, captured once per (columns, factor precision) as a CUDA graph
+  // on a private stream and replayed on the caller's stream
+  struct SweepGraph {
+    int nrhs;
+    bool f64;
+    int launches;
+    cudaGraphExec_t exec;
+  };
+  std::vector<SweepGraph> graphs;
+  cudaStream_t capture_stream = nullptr;
 };
 
 namespace yasf {
@@ -360,6 +370,8 @@ extern "C" int yasf_precond_destroy(yasf_precond* pc) {
   cudaFree(pc->d_dinv);
   cudaFree(pc->d_dinv64);
   cudaFree(pc->d_z);
+  for (auto& g : pc->graphs) cudaGraphExecDestroy(g.exec);
+  if (pc->capture_stream) cudaStreamDestroy(pc->capture_stream);
   delete pc;
   return YASF_OK;
 }
@@ -525,6 +537,8 @@ extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
       pc->d_mat = nullptr;
     }
   }
+  for (auto& gr : pc->graphs) cudaGraphExecDestroy(gr.exec);  // captured the previous factors
+  pc->graphs.clear();
   pc->prepared = true;
   return YASF_OK;
 }
@@ -552,27 +566,64 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
       }
       YASF_CUDA_TRY(cudaStreamSynchronize(s));
       cudaFree(pc->d_z);
-      const_cast<yasf_precond*>(pc)->d_z = z;
-      const_cast<yasf_precond*>(pc)->z_cols = nrhs;
+      yasf_precond* mpc = const_cast<yasf_precond*>(pc);
+      mpc->d_z = z;
+      mpc->z_cols = nrhs;
+      for (auto& gr : mpc->graphs) cudaGraphExecDestroy(gr.exec);  // they captured the old buffer
+      mpc->graphs.clear();
     }
+    yasf_precond* mpc = const_cast<yasf_precond*>(pc);
     const int gb = (int)std::min<long long>(((long long)pc->total_rows * nrhs + 255) / 256, 8192);
     YASF_COUNTED(lu_gather_kernel<<<gb, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld, pc->d_row_block,
                                                      pc->d_row_local, pc->d_block_ptr, pc->d_particles,
                                                      pc->d_row0, pc->d_piv, reinterpret_cast<const double2*>(x),
                                                      pc->d_z));
     const LuGeom g = lu_geom(pc);
-    for (int upper = 0; upper < 2; ++upper)
-      for (int step = 0; step < pc->lu_steps; ++step) {
-        int n = 0;
-        const int* pre = lu_pre(pc, 3, step, &n);
-        if (!n) continue;
-        if (f64)
-          YASF_COUNTED(lu_sweep_kernel<double2><<<n, 256, 0, s>>>(g, pre, step, upper, pc->d_mat, pc->d_dinv64,
-                                                                  nrhs, pc->total_rows, pc->d_z));
-        else
-          YASF_COUNTED(lu_sweep_kernel<float2><<<n, 256, 0, s>>>(g, pre, step, upper, pc->d_mat32, pc->d_dinv,
-                                                                 nrhs, pc->total_rows, pc->d_z));
+    // the forward and backward sweeps (one launch per tile row) into stream `ss`
+    auto sweeps = [&](cudaStream_t ss) -> int {
+      int launched = 0;
+      for (int upper = 0; upper < 2; ++upper)
+        for (int step = 0; step < pc->lu_steps; ++step) {
+          int n = 0;
+          const int* pre = lu_pre(pc, 3, step, &n);
+          if (!n) continue;
+          if (f64)
+            lu_sweep_kernel<double2><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat, pc->d_dinv64, nrhs,
+                                                        pc->total_rows, pc->d_z);
+          else
+            lu_sweep_kernel<float2><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat32, pc->d_dinv, nrhs,
+                                                       pc->total_rows, pc->d_z);
+          ++launched;
+        }
+      return launched;
+    };
+    const yasf_precond::SweepGraph* graph = nullptr;
+    for (const auto& gr : pc->graphs)
+      if (gr.nrhs == nrhs && gr.f64 == f64) graph = &gr;
+    if (!graph) {  // capture once on the private stream; a failed capture falls back to launches
+      if (!mpc->capture_stream) YASF_CUDA_TRY(cudaStreamCreateWithFlags(&mpc->capture_stream, cudaStreamNonBlocking));
+      cudaGraph_t gr = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      int launched = 0;
+      if (cudaStreamBeginCapture(mpc->capture_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        launched = sweeps(mpc->capture_stream);
+        if (cudaStreamEndCapture(mpc->capture_stream, &gr) == cudaSuccess && gr &&
+            cudaGraphInstantiate(&exec, gr, 0) == cudaSuccess) {
+          mpc->graphs.push_back({nrhs, f64, launched, exec});
+          graph = &mpc->graphs.back();
+        }
+        if (gr) cudaGraphDestroy(gr);
       }
+      (void)cudaGetLastError();  // a refused capture leaves no sticky error
+    }
+    if (graph) {
+      YASF_CUDA_TRY(cudaGraphLaunch(graph->exec, s));
+      for (int i = 0; i < graph->launches; ++i) count_launch();
+    } else {
+      const int launched = sweeps(s);
+      for (int i = 0; i < launched; ++i) count_launch();
+      YASF_CUDA_TRY(cudaGetLastError());
+    }
     YASF_COUNTED(lu_scatter_kernel<<<gb, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld, pc->d_row_block,
                                                       pc->d_row_local, pc->d_block_ptr, pc->d_particles, pc->d_z,
                                                       reinterpret_cast<double2*>(y)));
