@@ -639,7 +639,7 @@ def run_serve(args, rank: int, world: int) -> None:
     from yasf_b200.autotune import Autotuner
 
     tuner = Autotuner() if args.autotune else None
-    cfg = ServeConfig(max_slots=args.slots, rtol=args.serve_rtol, tuner=tuner)
+    cfg = ServeConfig(max_slots=args.slots, rtol=args.serve_rtol, tuner=tuner, group_small=not args.no_group)
     server = Server(cfg, device=device)
     server.run(warm, realtime=False)
     torch.cuda.synchronize()
@@ -692,6 +692,10 @@ def run_serve(args, rank: int, world: int) -> None:
         "latency_s": {"p50": tot["latency_p50_s"], "p99": tot["latency_p99_s"]},
         "requests_completed": tot["completed"], "requests_failed": tot["failed"],
         "rhs_solves": tot["rhs_solves"], "makespan_s": tot["makespan_s"], "rank0_summary": summ,
+        "requests": [{"rid": r.rid, "n": r.n_spheres, "lmax": r.lmax, "nrhs": r.nrhs,
+                      "inner": r.stats.get("inner"), "group": r.stats.get("group_size"),
+                      "inner_steps": r.stats.get("inner_steps"), "admitted_s": round(r.admitted, 3),
+                      "latency_s": round(r.latency, 3), "error": r.error} for r in results],
         "c_ext_error_vs_fp64": {"max": max((e["c_ext_rel_err"] for e in errs), default=None),
                                 "samples": errs},
         "autotune": None if tuner is None else {
@@ -914,6 +918,8 @@ def main() -> None:
                     help="serve: choose each request's inner operator with the (lmax, N, R) autotuner "
                          "(timed inside the run) instead of the fixed rule")
     ap.add_argument("--serve-rtol", type=float, default=1e-6, help="serving refinement tolerance")
+    ap.add_argument("--no-group", action="store_true",
+                    help="serve: solve every request on its own (no grouped solves of small requests)")
     ap.add_argument("--error-samples", type=int, default=3, help="float64 check solves (serve)")
     ap.add_argument("--no-column-errors", action="store_true",
                     help="skip the float64 reference solves behind the batched block's per-column errors")

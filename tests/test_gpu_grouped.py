@@ -31,7 +31,7 @@ def _aggregates(device, lmax, specs):
         k = 2 * np.pi / wl
         dev = CouplingDevice(lmax, cached_translation_table(lmax), pos, k, device)
         tmat = torch.from_numpy(mie_tmatrix_per_sphere(lmax, k, radii, m)).to(device)
-        polar, azim, pol = incidences(max(1, R // 2))
+        polar, azim, pol = incidences((R + 1) // 2)  # R columns: ceil(R / 2) directions x TE/TM
         A, B = dev.plane_wave_rhs(tmat, polar[:R], azim[:R], pol[:R])
         out.append((dev, tmat, B, A))
     return out

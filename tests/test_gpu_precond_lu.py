@@ -3,8 +3,10 @@ triangular-sweep apply, against dense solves of the same assembled blocks.
 
 Block orders are multiples of nmax (48 at lmax 4, 96 at lmax 6), so most are not multiples of the
 64-row tiles: the ragged last tile, several tiles per block and blocks of very different orders in
-one factorisation are all exercised. Tolerances: 1e-10 relative (max-norm) with the complex128
-factors kept, 1e-5 with the complex64 factors the solves stream.
+one factorisation are all exercised. Tolerances: forward error 1e-10 relative (max-norm) with the
+complex128 factors kept; with the complex64 factors the solves stream, the residual of the block
+system below 1e-5 of the right-hand side (backward error; the forward error is bounded by it times
+the blocks' condition number).
 """
 
 from __future__ import annotations
@@ -58,8 +60,11 @@ def test_block_lu_apply_inverts_the_blocks(cuda_device, lmax, n, phi, cells):
     My = torch.from_numpy(_block_product(dev, mats, blocks, y)).to(cuda_device)
     out = pc.apply(My, YASF_C128).cpu().numpy()
     assert rel_err(out, y) < 1e-10
+    # complex64 factors: a backward-stable solve with them leaves a small residual of the block
+    # system (its forward error grows with the blocks' condition number, ~1e5 at lmax 6)
     out64 = pc.apply(My, YASF_C64).cpu().numpy()
-    assert rel_err(out64, y) < 1e-5
+    resid = _block_product(dev, mats, blocks, out64) - My.cpu().numpy()
+    assert np.linalg.norm(resid) < 1e-5 * np.linalg.norm(My.cpu().numpy())
     # several right-hand sides in one apply equal the one-column applies
     X = torch.from_numpy(rng.normal(size=(3, dev.n)) + 1j * rng.normal(size=(3, dev.n))).to(cuda_device)
     Y = pc.apply(X, YASF_C64).cpu().numpy()

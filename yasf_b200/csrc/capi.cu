@@ -94,7 +94,7 @@ CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int preci
   const size_t vsize = (precision == YASF_C64) ? sizeof(float4) : sizeof(double2);
   const int N = n_particles;
   // Receivers per block: whole warps, at most 4, one receiver per thread (two in complex64).
-  const int rpt = precision == YASF_C64 ? 2 : 1;
+  const int rpt = precision == YASF_C64 ? kC64Receivers : 1;
   const int warps = std::min(4, std::max(1, (N + 32 * rpt - 1) / (32 * rpt)));
   lay.threads = 32 * warps;
   lay.tiles = (N + lay.threads * rpt - 1) / (lay.threads * rpt);

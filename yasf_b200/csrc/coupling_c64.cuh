@@ -13,7 +13,15 @@
 // Included by coupling.cuh inside namespace yasf, after contract_body (it uses the stage helpers).
 #pragma once
 
-constexpr int kC64Receivers = 2;  // receivers per thread of the complex64 contraction
+// Receivers per thread and whether the order-p loop is unrolled: build-time choices (defaults 2, 1),
+// the host layout follows kC64Receivers.
+#ifndef YASF_C64_RECEIVERS
+#define YASF_C64_RECEIVERS 2
+#endif
+#ifndef YASF_C64_UNROLL_P
+#define YASF_C64_UNROLL_P 1
+#endif
+constexpr int kC64Receivers = YASF_C64_RECEIVERS;  // receivers per thread of the complex64 contraction
 
 template <int L, int BID>
 __device__ __forceinline__ bool contract_body_c64(const ContractArgs& a, int tile, int chunk, char* smem,
@@ -139,8 +147,13 @@ __device__ __forceinline__ bool contract_body_c64(const ContractArgs& a, int til
           ha_r[q] = hb_r[q]; ha_i[q] = hb_i[q]; hb_r[q] = nr; hb_i[q] = ni;
         }
       }
-#pragma unroll 1
-      for (int p = d; p <= PMAX; ++p) {
+      // The order-p loop is unrolled (d is a warp-uniform runtime value, p < d is skipped): the
+      // valid row count of every (m1, p) is a compile-time constant, so the row loops below are
+      // straight-line code without predicated-off row slots taking issue slots.
+      constexpr int kPU = YASF_C64_UNROLL_P ? PMAX + 1 : 1;
+#pragma unroll kPU
+      for (int p = YASF_C64_UNROLL_P ? 0 : d; p <= PMAX; ++p) {
+        if (p < d) continue;
         float2 gpr2[Q], gpi2[Q], gmr2[Q], gmi2[Q];
 #pragma unroll
         for (int q = 0; q < Q; ++q) {

@@ -806,7 +806,7 @@ GroupWs group_layout(const yasf_plan* plan, int P, const yasf_problem* pr, int m
     const int ch = (N + spc - 1) / spc;
     L.chunks.push_back(ch);
     L.tiles64.push_back((N + kGroupThreads - 1) / kGroupThreads);
-    L.tiles32.push_back((N + 2 * kGroupThreads - 1) / (2 * kGroupThreads));
+    L.tiles32.push_back((N + kC64Receivers * kGroupThreads - 1) / (kC64Receivers * kGroupThreads));
     L.src_pre.push_back(L.src_pre.back() + N);
     L.elem_pre.push_back(L.elem_pre.back() + nc);
     L.ipre64.push_back(L.ipre64.back() + (long long)L.tiles64.back() * ch * plan->n_bundles);
