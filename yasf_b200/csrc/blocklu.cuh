@@ -377,16 +377,18 @@ __global__ void lu_scatter_kernel(int total_rows, int nmax, int nrhs, long long 
 // One step of a sweep. Forward (upper = 0), launch s: tile rows i = s .. nt-1 of every block with
 // s < nt: z_i -= L_{i,s-1} z_{s-1} (s > 0), then z_s = L_ss^{-1} z_s. Backward (upper = 1), launch
 // t, s = nt - 1 - t: tile rows i = 0 .. s: z_i -= U_{i,s+1} z_{s+1} (t > 0), then z_s = U_ss^{-1} z_s.
-// 256 threads: thread (row = tid >> 2, part = tid & 3) sums 16 of the 64 products of its row; the
-// four parts are combined by shuffles. Right-hand sides are processed kLuCols at a time.
+// 256 threads: thread (row = tid >> 2, part = tid & 3) owns 16 of the 64 products of its row, all of
+// whose factor loads are issued at once (the loop is fully unrolled, predicated only on the ragged
+// edge); the four parts are combined by shuffles. Two blocks per SM. Right-hand sides are processed
+// NC at a time (NC = 1 for a single column, else kLuCols).
 // FT: float2 (the complex64 factors the solves stream) or double2 (complex128 factors, when kept).
 constexpr int kLuCols = 8;
-template <typename FT>
-__global__ void __launch_bounds__(256) lu_sweep_kernel(LuGeom g, const int* pre, int step, int upper,
-                                                       const FT* lu, const FT* dinv, int nrhs,
-                                                       int total_rows, double2* z) {
-  __shared__ double2 zin[kLuCols][kLuT];   // z of the eliminated tile row
-  __shared__ double2 zacc[kLuCols][kLuT];  // the diagonal tile row before its inverse is applied
+template <typename FT, int NC>
+__global__ void __launch_bounds__(256, 2) lu_sweep_kernel(LuGeom g, const int* pre, int step, int upper,
+                                                          const FT* lu, const FT* dinv, int nrhs,
+                                                          int total_rows, double2* z) {
+  __shared__ double2 zin[NC][kLuT];   // z of the eliminated tile row
+  __shared__ double2 zacc[NC][kLuT];  // the diagonal tile row before its inverse is applied
   const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
   const int item = blockIdx.x - pre[b];
   const int dim = g.dim[b];
@@ -400,26 +402,34 @@ __global__ void __launch_bounds__(256) lu_sweep_kernel(LuGeom g, const int* pre,
   const FT* M = lu + g.mat_off[b];
   const int tid = threadIdx.x, row = tid >> 2, part = tid & 3;
   const size_t zb = g.row0[b];
-  for (int c0 = 0; c0 < nrhs; c0 += kLuCols) {
-    const int nc = min(kLuCols, nrhs - c0);
+  const bool diag = i == s;
+  // this thread's 16 factor entries of the eliminated tile
+  FT m[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const int q = part + 4 * k;
+    m[k] = (has_e && row < vi && q < ve) ? M[(size_t)(i0 + row) * dim + e0 + q] : FT{};
+  }
+  const FT* inv = dinv + ((size_t)(g.tile0[b] + s) * 2 + (upper ? 1 : 0)) * kLuT * kLuT + (size_t)row * kLuT;
+  for (int c0 = 0; c0 < nrhs; c0 += NC) {
+    const int nc = min(NC, nrhs - c0);
     __syncthreads();
     if (has_e)
-      for (int e = tid; e < kLuCols * kLuT; e += blockDim.x) {
+      for (int e = tid; e < NC * kLuT; e += blockDim.x) {
         const int cc = e / kLuT, r = e % kLuT;
         zin[cc][r] = (cc < nc && r < ve) ? z[(size_t)(c0 + cc) * total_rows + zb + e0 + r] : make_double2(0.0, 0.0);
       }
     __syncthreads();
-    double2 acc[kLuCols];
+    double2 acc[NC];
 #pragma unroll
-    for (int cc = 0; cc < kLuCols; ++cc) acc[cc] = make_double2(0.0, 0.0);
-    if (has_e && row < vi) {
-      const FT* mr = M + (size_t)(i0 + row) * dim + e0;
-#pragma unroll 4
-      for (int q = part; q < ve; q += 4) {
-        const FT m = mr[q];
-        const double mx = m.x, my = m.y;
+    for (int cc = 0; cc < NC; ++cc) acc[cc] = make_double2(0.0, 0.0);
+    if (has_e) {
 #pragma unroll
-        for (int cc = 0; cc < kLuCols; ++cc) {
+      for (int k = 0; k < 16; ++k) {
+        const double mx = m[k].x, my = m[k].y;
+        const int q = part + 4 * k;
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
           const double2 zv = zin[cc][q];
           acc[cc].x = fma(mx, zv.x, fma(-my, zv.y, acc[cc].x));
           acc[cc].y = fma(mx, zv.y, fma(my, zv.x, acc[cc].y));
@@ -427,13 +437,13 @@ __global__ void __launch_bounds__(256) lu_sweep_kernel(LuGeom g, const int* pre,
       }
     }
 #pragma unroll
-    for (int cc = 0; cc < kLuCols; ++cc) {
+    for (int cc = 0; cc < NC; ++cc) {
       acc[cc].x += __shfl_xor_sync(0xffffffffu, acc[cc].x, 1);
       acc[cc].y += __shfl_xor_sync(0xffffffffu, acc[cc].y, 1);
       acc[cc].x += __shfl_xor_sync(0xffffffffu, acc[cc].x, 2);
       acc[cc].y += __shfl_xor_sync(0xffffffffu, acc[cc].y, 2);
     }
-    if (i != s) {
+    if (!diag) {
       if (part == 0 && row < vi)
         for (int cc = 0; cc < nc; ++cc) {
           double2* zp = z + (size_t)(c0 + cc) * total_rows + zb + i0 + row;
@@ -444,29 +454,29 @@ __global__ void __launch_bounds__(256) lu_sweep_kernel(LuGeom g, const int* pre,
     }
     // diagonal tile row: r = z_s - (eliminated part), then z_s = inverse(diagonal tile) r
     if (part == 0)
-      for (int cc = 0; cc < kLuCols; ++cc) {
+      for (int cc = 0; cc < NC; ++cc) {
         double2 o = make_double2(0.0, 0.0);
         if (row < vi && cc < nc) o = z[(size_t)(c0 + cc) * total_rows + zb + i0 + row];
         zacc[cc][row] = make_double2(o.x - acc[cc].x, o.y - acc[cc].y);
       }
     __syncthreads();
-    const FT* inv = dinv + ((size_t)(g.tile0[b] + s) * 2 + (upper ? 1 : 0)) * kLuT * kLuT + (size_t)row * kLuT;
-    double2 out[kLuCols];
+    double2 out[NC];
 #pragma unroll
-    for (int cc = 0; cc < kLuCols; ++cc) out[cc] = make_double2(0.0, 0.0);
-#pragma unroll 4
-    for (int q = part; q < kLuT; q += 4) {
-      const FT m = inv[q];
-      const double mx = m.x, my = m.y;
+    for (int cc = 0; cc < NC; ++cc) out[cc] = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int cc = 0; cc < kLuCols; ++cc) {
+    for (int k = 0; k < 16; ++k) {
+      const FT wv = inv[part + 4 * k];
+      const double mx = wv.x, my = wv.y;
+      const int q = part + 4 * k;
+#pragma unroll
+      for (int cc = 0; cc < NC; ++cc) {
         const double2 zv = zacc[cc][q];
         out[cc].x = fma(mx, zv.x, fma(-my, zv.y, out[cc].x));
         out[cc].y = fma(mx, zv.y, fma(my, zv.x, out[cc].y));
       }
     }
 #pragma unroll
-    for (int cc = 0; cc < kLuCols; ++cc) {
+    for (int cc = 0; cc < NC; ++cc) {
       out[cc].x += __shfl_xor_sync(0xffffffffu, out[cc].x, 1);
       out[cc].y += __shfl_xor_sync(0xffffffffu, out[cc].y, 1);
       out[cc].x += __shfl_xor_sync(0xffffffffu, out[cc].x, 2);

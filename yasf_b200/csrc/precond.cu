@@ -587,12 +587,18 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
           int n = 0;
           const int* pre = lu_pre(pc, 3, step, &n);
           if (!n) continue;
-          if (f64)
-            lu_sweep_kernel<double2><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat, pc->d_dinv64, nrhs,
-                                                        pc->total_rows, pc->d_z);
+          if (f64 && nrhs == 1)
+            lu_sweep_kernel<double2, 1><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat, pc->d_dinv64, nrhs,
+                                                           pc->total_rows, pc->d_z);
+          else if (f64)
+            lu_sweep_kernel<double2, kLuCols><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat, pc->d_dinv64,
+                                                                 nrhs, pc->total_rows, pc->d_z);
+          else if (nrhs == 1)
+            lu_sweep_kernel<float2, 1><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat32, pc->d_dinv, nrhs,
+                                                          pc->total_rows, pc->d_z);
           else
-            lu_sweep_kernel<float2><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat32, pc->d_dinv, nrhs,
-                                                       pc->total_rows, pc->d_z);
+            lu_sweep_kernel<float2, kLuCols><<<n, 256, 0, ss>>>(g, pre, step, upper, pc->d_mat32, pc->d_dinv,
+                                                                nrhs, pc->total_rows, pc->d_z);
           ++launched;
         }
       return launched;
