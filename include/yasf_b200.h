@@ -66,16 +66,19 @@ int yasf_set_tiles(int contract_waves, int dpanel_cols, int panel_groups);
  * YASF_ERR_NOT_FINITE from a solve. This call makes such a wait run out on purpose for the next
  * launches FROM THIS HOST THREAD: `role` names one producer that never delivers (the first stage
  * copy of every block of the coupling contraction; the pair-table warps of the tensor-core panel;
- * the helper warp of the float64 dense panel), `contract_polls` (> 0) replaces the contraction's
- * poll limit per stage wait (2^22) and `panel_wait_seconds` (> 0, <= 10) the panels' wait bound
- * (1 s). 0 keeps a default. YASF_STALL_NONE restores normal launches. The error word a kernel
- * sets is the int at byte offset (required workspace bytes - 256) of the call's workspace, for
- * the coupling, panel and dense-panel entry points alike (0: every wait completed). */
+ * the helper warp of the float64 dense panel; the first tile row of a one-column preconditioner
+ * apply, whose sweeps then wait on it and write NaN), `contract_polls` (> 0) replaces the contraction's
+ * poll limit per stage wait (2^22) and `panel_wait_seconds` (> 0, <= 10) the wait bound of the
+ * panels and of the preconditioner sweeps (1 s). 0 keeps a default. YASF_STALL_NONE restores
+ * normal launches. The error word a kernel sets is the int at byte offset (required workspace
+ * bytes - 256) of the call's workspace, for the coupling, panel and dense-panel entry points alike
+ * (0: every wait completed); a preconditioner apply whose wait ran out leaves NaN in its output. */
 enum yasf_stall_role {
   YASF_STALL_NONE = 0,
   YASF_STALL_CONTRACT = 1,
   YASF_STALL_PANEL = 2,
-  YASF_STALL_DPANEL = 3
+  YASF_STALL_DPANEL = 3,
+  YASF_STALL_PRECOND = 4
 };
 int yasf_test_stall(int role, int contract_polls, double panel_wait_seconds);
 

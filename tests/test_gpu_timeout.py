@@ -1,7 +1,7 @@
 """Failure detection on the device: bounded waits that run out.
 
 Every wait inside the library's kernels is bounded (the coupling contraction by a poll count, the
-tensor-core and float64 dense panels by %globaltimer). When a wait runs out the kernel sets the
+tensor-core and float64 dense panels and the preconditioner's one-launch sweeps by %globaltimer). When a wait runs out the kernel sets the
 call's error word, writes NaN outputs, frees what it holds and returns, so the CUDA context stays
 usable. The test hook ``yasf_test_stall`` keeps one producer role from ever delivering (a flag that
 nothing sets) and shortens the bound, so each wait below runs out in milliseconds; nothing faults,
@@ -18,8 +18,8 @@ from conftest import rel_err
 
 from oracle import restate as R
 from yasf_b200 import _lib
-from yasf_b200._lib import (YASF_STALL_CONTRACT, YASF_STALL_DPANEL, YASF_STALL_NONE, YASF_STALL_PANEL,
-                            YasfError)
+from yasf_b200._lib import (YASF_C64, YASF_STALL_CONTRACT, YASF_STALL_DPANEL, YASF_STALL_NONE, YASF_STALL_PANEL,
+                            YASF_STALL_PRECOND, YasfError)
 from yasf_b200.device import CouplingDevice
 from yasf_b200.wigner import translation_table_ab5
 
@@ -112,6 +112,36 @@ def test_dense_panel_wait_runs_out(cuda_device):
     assert _error_word(dev, nb) == 0
     ref = dev.coupling(X)
     assert rel_err(y2.cpu().numpy(), ref.cpu().numpy()) < 1e-12
+
+
+def test_preconditioner_sweep_wait_runs_out(cuda_device):
+    from yasf_b200.device import DevicePreconditioner
+    from yasf_b200.mie import mie_tmatrix_per_sphere
+    from yasf_b200.workloads import rsa_cube
+
+    rng = np.random.default_rng(6)
+    lmax = 4
+    radii = rng.uniform(0.06, 0.1, size=60)
+    pos = rsa_cube(radii, 0.2, rng, largest_first=True)
+    dev = CouplingDevice(lmax, translation_table_ab5(lmax), pos, 2 * np.pi / 0.55, cuda_device)
+    tmat = torch.from_numpy(mie_tmatrix_per_sphere(lmax, dev.k, radii, 1.5 + 0.01j)).to(cuda_device)
+    ext = pos.max(axis=0) - pos.min(axis=0)
+    from yasf_b200.preconditioner import make_particle_partition
+
+    pc = DevicePreconditioner(dev, make_particle_partition(pos, (ext + 2.0) / 2))
+    pc.prepare(tmat)
+    x = torch.from_numpy(rng.normal(size=dev.n) + 1j * rng.normal(size=dev.n)).to(cuda_device)
+    good = pc.apply(x, YASF_C64)
+    try:
+        # the first tile row never delivers: the rows that wait on it give up after 50 ms
+        _lib.test_stall(YASF_STALL_PRECOND, 0, 0.05)
+        y = pc.apply(x, YASF_C64)
+        torch.cuda.synchronize()
+    finally:
+        _lib.test_stall(YASF_STALL_NONE)
+    assert torch.isnan(y.real).any()
+    # the context is still usable and the next apply equals the one before the stall
+    assert torch.equal(pc.apply(x, YASF_C64), good)
 
 
 def dev_panel_bytes(dev, R_):

@@ -143,6 +143,7 @@ YASF_STALL_NONE = 0
 YASF_STALL_CONTRACT = 1
 YASF_STALL_PANEL = 2
 YASF_STALL_DPANEL = 3
+YASF_STALL_PRECOND = 4
 
 
 def test_stall(role: int, contract_polls: int = 0, panel_wait_seconds: float = 0.0) -> None:

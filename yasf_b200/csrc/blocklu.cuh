@@ -19,11 +19,13 @@
 //
 // Apply (finalize keeps only a complex64 copy of the factors plus the complex64 inverses of the
 // diagonal tiles of L and U, and frees the complex128 matrices): z = P x gathered from the
-// particle-major vector, forward sweep with L, backward sweep with U, scattered back. Sweep step
-// s of the forward pass: every tile row i >= s subtracts L_{i,s-1} z_{s-1} (z_{s-1} was finished
-// by the previous launch), and tile row s then multiplies by L_ss^{-1}; the backward pass mirrors
-// it. One launch per step, no inter-CTA waits, no atomics: every element is written by one CTA per
-// launch in a fixed order, so the apply is deterministic. Arithmetic is float64 throughout.
+// particle-major vector, forward sweep with L, backward sweep with U, scattered back. One column
+// (every Krylov step): both sweeps in ONE launch whose CTAs take tile rows in ticket order and wait
+// on per-block finished-row counters (lu_solve_kernel). Several columns: one launch per sweep
+// step; step s of the forward pass: every tile row i >= s subtracts L_{i,s-1} z_{s-1} (finished by
+// the previous launch), and tile row s then multiplies by L_ss^{-1}; the backward pass mirrors it.
+// Both forms sum every row in a fixed order, so applies are deterministic. Arithmetic is float64
+// throughout.
 #pragma once
 
 #include "capi_internal.h"
@@ -485,6 +487,229 @@ __global__ void __launch_bounds__(256, 2) lu_sweep_kernel(LuGeom g, const int* p
     if (part == 0 && row < vi)
       for (int cc = 0; cc < nc; ++cc) z[(size_t)(c0 + cc) * total_rows + zb + i0 + row] = out[cc];
   }
+}
+
+// ---- both sweeps of a one-column apply in ONE launch ------------------------------------------
+// Each CTA takes a ticket from a global counter when it starts; ticket t names one tile row: the
+// forward sweep's rows first (ordered by tile row, then block), then the backward sweep's rows
+// (ordered by distance from the block's last tile row, then block). The CTA computes its whole row,
+// z_i = D_i^{-1} (z_i - sum_j F_ij z_j) over the finished rows j (forward: j < i, F = L; backward:
+// j > i, F = U; D_i^{-1} the inverse of the diagonal tile), consuming the rows as its block's
+// finished-row counter announces them, then publishes row i by raising that counter. Rows of one
+// block finish strictly in order (row i needs row i-1), so one counter per block and sweep carries
+// every dependency, and a backward row starts once its block's forward counter reaches nt. Every
+// row a CTA waits for has a smaller ticket, held by a CTA that is already running, so the launch
+// progresses whatever order the hardware schedules CTAs in. The factor streams once, as in the
+// step-per-launch sweep, but without one launch (and one tail) per tile row.
+// Waits are bounded in time; a wait that runs out raises the abort word, after which every CTA
+// writes NaN for its row and publishes at once, so the launch ends quickly and the solve reports a
+// non-finite result. Arithmetic is float64 (the factor entries are widened as they are read); the
+// sum over j runs in the order of the sweep, not the step-per-launch order, so results differ from
+// that kernel's only by rounding.
+struct LuSolveArgs {
+  LuGeom g;
+  const int2* order;  // [2 * n_tiles]: (block, tile row) of each ticket
+  int n_tiles;
+  double2* z;
+  int* sync;  // [0] ticket, [1] abort, [2, 2 + n_blocks) forward rows done, then backward rows done
+  unsigned long long wait_ns;
+  int stall;  // test hook: the CTA of ticket 0 never delivers its row
+};
+constexpr int kLuBatch = 32;     // finished tile rows whose z is staged in shared memory at once
+constexpr int kLuInvS = kLuT + 4;  // row stride of the staged inverse (conflict-free 8/16 B reads)
+template <typename FT>
+constexpr size_t lu_solve_smem() {
+  return (size_t)kLuT * kLuInvS * sizeof(FT) + (size_t)(kLuBatch + 1) * kLuT * sizeof(double2);
+}
+
+__device__ __forceinline__ int lu_ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long lu_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits until *done > need and returns the count seen, or returns -1 once the abort word is set or
+// `bound_ns` has passed (raising the abort word).
+__device__ int lu_wait_rows(const int* done, int need, int* abort_word, unsigned long long bound_ns) {
+  unsigned long long t0 = 0;
+#pragma unroll 1
+  for (unsigned spin = 0;; ++spin) {
+    const int v = lu_ld_acquire(done);
+    if (v > need) return v;
+    if (lu_ld_acquire(abort_word)) return -1;
+    if (spin == 0) {
+      t0 = lu_ns();
+    } else if ((spin & 15) == 0 && lu_ns() - t0 > bound_ns) {
+      atomicExch(abort_word, 1);
+      return -1;
+    }
+    __nanosleep(64);
+  }
+}
+
+template <typename FT>
+__device__ __forceinline__ void lu_row_products(const FT (&m)[16], const double2* zt, int part, double& ax,
+                                                double& ay) {
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    const double mx = m[k].x, my = m[k].y;
+    const double2 zv = zt[part + 4 * k];
+    ax = fma(mx, zv.x, fma(-my, zv.y, ax));
+    ay = fma(mx, zv.y, fma(my, zv.x, ay));
+  }
+}
+
+// entries 2 (part + 4k) and 2 (part + 4k) + 1 of a complex64 tile row, as float4 pairs
+__device__ __forceinline__ void lu_pair_products(const float4 (&m)[8], const double2* zt, int part, double& ax,
+                                                 double& ay) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int q = 2 * (part + 4 * k);
+    const double2 z0 = zt[q], z1 = zt[q + 1];
+    const double m0x = m[k].x, m0y = m[k].y, m1x = m[k].z, m1y = m[k].w;
+    ax = fma(m0x, z0.x, fma(-m0y, z0.y, ax));
+    ay = fma(m0x, z0.y, fma(m0y, z0.x, ay));
+    ax = fma(m1x, z1.x, fma(-m1y, z1.y, ax));
+    ay = fma(m1x, z1.y, fma(m1y, z1.x, ay));
+  }
+}
+
+template <typename FT>
+__global__ void __launch_bounds__(256, 2) lu_solve_kernel(LuSolveArgs a, const FT* lu, const FT* dinv) {
+  extern __shared__ __align__(16) unsigned char lu_solve_raw[];
+  FT* winv = reinterpret_cast<FT*>(lu_solve_raw);  // [64][kLuInvS] the diagonal tile's inverse
+  double2* zs = reinterpret_cast<double2*>(lu_solve_raw + (size_t)kLuT * kLuInvS * sizeof(FT));  // [kLuBatch][64]
+  double2* zrow = zs + kLuBatch * kLuT;  // [64] this row's right-hand side
+  __shared__ int s_ticket, s_avail;
+  const int tid = threadIdx.x, row = tid >> 2, part = tid & 3;
+  if (tid == 0) s_ticket = atomicAdd(a.sync, 1);
+  __syncthreads();
+  const int t = s_ticket;
+  if (t >= 2 * a.n_tiles || (a.stall && t == 0)) return;
+  const bool upper = t >= a.n_tiles;
+  const int2 bi = a.order[t];
+  const int b = bi.x, i = bi.y;
+  const int dim = a.g.dim[b], nt = lu_tiles(dim);
+  const int i0 = i * kLuT, vi = min(kLuT, dim - i0);
+  // this thread's factor row (rows past a ragged edge re-read the last row; never stored)
+  const FT* M = lu + a.g.mat_off[b] + (size_t)(i0 + min(row, vi - 1)) * dim;
+  double2* zb = a.z + a.g.row0[b];
+  int* abort_word = a.sync + 1;
+  int* done = a.sync + 2 + (upper ? a.g.n_blocks : 0) + b;
+  {
+    const FT* inv = dinv + ((size_t)(a.g.tile0[b] + i) * 2 + (upper ? 1 : 0)) * kLuT * kLuT;
+    for (int e = tid; e < kLuT * kLuT; e += blockDim.x) winv[(e >> 6) * kLuInvS + (e & 63)] = inv[e];
+  }
+  const int ndep = upper ? nt - 1 - i : i;
+  bool ok = true;
+  if (upper) {  // the backward sweep reads the block's finished forward sweep
+    if (tid == 0) s_avail = lu_wait_rows(a.sync + 2 + b, nt - 1, abort_word, a.wait_ns);
+    __syncthreads();
+    ok = s_avail >= 0;
+    __syncthreads();
+  }
+  double ax = 0.0, ay = 0.0;
+  int c = 0;  // finished rows consumed
+  while (ok && c < ndep) {
+    if (tid == 0) s_avail = lu_wait_rows(done, c, abort_word, a.wait_ns);
+    __syncthreads();
+    if (s_avail < 0) {
+      ok = false;
+      break;
+    }
+    const int avail = min(ndep, s_avail);
+    for (int c0 = c; c0 < avail; c0 += kLuBatch) {
+      const int nb = min(kLuBatch, avail - c0);
+      for (int e = tid; e < nb * kLuT; e += blockDim.x) {
+        const int cc = c0 + (e >> 6);
+        const int r = (upper ? nt - 1 - cc : cc) * kLuT + (e & 63);
+        zs[e] = r < dim ? __ldcg(zb + r) : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+      if constexpr (sizeof(FT) == 8) {
+        // complex64 factors as pairs (float4): thread part owns entries 2 (part + 4k) and +1; two
+        // tiles' loads in flight. Block orders are even, so a pair never straddles the edge.
+        const float4* M4 = reinterpret_cast<const float4*>(M);
+        int u = 0;
+#pragma unroll 1
+        for (; u + 1 < nb; u += 2) {
+          const int ja = (upper ? nt - 1 - (c0 + u) : c0 + u) * kLuT;
+          const int jb = (upper ? nt - 2 - (c0 + u) : c0 + u + 1) * kLuT;
+          const int va = min(kLuT, dim - ja), vb = min(kLuT, dim - jb);
+          float4 m0[8], m1[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int q = 2 * (part + 4 * k);
+            m0[k] = q < va ? M4[(ja + q) >> 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+            m1[k] = q < vb ? M4[(jb + q) >> 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+          lu_pair_products(m0, zs + u * kLuT, part, ax, ay);
+          lu_pair_products(m1, zs + (u + 1) * kLuT, part, ax, ay);
+        }
+        if (u < nb) {
+          const int j0 = (upper ? nt - 1 - (c0 + u) : c0 + u) * kLuT;
+          const int vj = min(kLuT, dim - j0);
+          float4 m0[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int q = 2 * (part + 4 * k);
+            m0[k] = q < vj ? M4[(j0 + q) >> 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+          lu_pair_products(m0, zs + u * kLuT, part, ax, ay);
+        }
+      } else {
+#pragma unroll 1
+        for (int u = 0; u < nb; ++u) {
+          const int j0 = (upper ? nt - 1 - (c0 + u) : c0 + u) * kLuT;
+          const int vj = min(kLuT, dim - j0);
+          FT m0[16];
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const int q = part + 4 * k;
+            m0[k] = q < vj ? M[j0 + q] : FT{};
+          }
+          lu_row_products(m0, zs + u * kLuT, part, ax, ay);
+        }
+      }
+      __syncthreads();
+    }
+    c = avail;
+  }
+  ax += __shfl_xor_sync(0xffffffffu, ax, 1);
+  ay += __shfl_xor_sync(0xffffffffu, ay, 1);
+  ax += __shfl_xor_sync(0xffffffffu, ax, 2);
+  ay += __shfl_xor_sync(0xffffffffu, ay, 2);
+  if (ok) {
+    if (part == 0) {
+      const double2 o = row < vi ? __ldcg(zb + i0 + row) : make_double2(0.0, 0.0);
+      zrow[row] = make_double2(o.x - ax, o.y - ay);
+    }
+    __syncthreads();
+    double ox = 0.0, oy = 0.0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const FT w = winv[row * kLuInvS + part + 4 * k];
+      const double2 zv = zrow[part + 4 * k];
+      const double wx = w.x, wy = w.y;
+      ox = fma(wx, zv.x, fma(-wy, zv.y, ox));
+      oy = fma(wx, zv.y, fma(wy, zv.x, oy));
+    }
+    ox += __shfl_xor_sync(0xffffffffu, ox, 1);
+    oy += __shfl_xor_sync(0xffffffffu, oy, 1);
+    ox += __shfl_xor_sync(0xffffffffu, ox, 2);
+    oy += __shfl_xor_sync(0xffffffffu, oy, 2);
+    if (part == 0 && row < vi) __stcg(zb + i0 + row, make_double2(ox, oy));
+  } else if (part == 0 && row < vi) {
+    __stcg(zb + i0 + row, make_double2(__longlong_as_double(0x7ff8000000000000ll),
+                                       __longlong_as_double(0x7ff8000000000000ll)));
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) atomicMax(done, upper ? nt - i : i + 1);
 }
 
 }  // namespace yasf

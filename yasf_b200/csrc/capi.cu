@@ -304,7 +304,7 @@ extern "C" int yasf_set_tiles(int contract_waves, int dpanel_cols, int panel_gro
 }
 
 extern "C" int yasf_test_stall(int role, int contract_polls, double panel_wait_seconds) {
-  if (role < YASF_STALL_NONE || role > YASF_STALL_DPANEL) return YASF_ERR_INVALID_ARGUMENT;
+  if (role < YASF_STALL_NONE || role > YASF_STALL_PRECOND) return YASF_ERR_INVALID_ARGUMENT;
   if (contract_polls < 0 || !(panel_wait_seconds >= 0.0) || panel_wait_seconds > 10.0)
     return YASF_ERR_INVALID_ARGUMENT;
   StallHook h;

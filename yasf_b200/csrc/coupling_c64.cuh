@@ -1,22 +1,23 @@
-// Complex64 contraction body: two receivers per thread.
+// Complex64 contraction body: Q receivers per thread (build-time, one by default).
 //
 // Same factored sum, stream order, stage pipeline, cutoff and timeout behaviour as contract_body
-// (coupling.cuh), with the pair side and the accumulators in float. Every thread owns the two
-// receivers (2 tile + q) blockDim.x + threadIdx.x, q = 0, 1, so each V entry read from the stage
-// (one broadcast 16-byte shared load of (re, im, -im, re)) feeds four packed FP32 FMAs (FFMA2) in
-// two independent accumulation chains:
-//   (y_re, y_im)_q += (g_re, g_re)_q * (re, im) + (g_im, g_im)_q * (-im, re).
-// Compared with one receiver per thread this halves the shared loads per FMA and doubles the
-// independent work between dependent FMAs. Pair geometry and h_0, h_1 are evaluated in float64
-// (positions stay exact), then rounded; every recurrence runs in float.
+// (coupling.cuh), with the pair side and the accumulators in float. Thread q-slot j owns receiver
+// (Q tile + j) blockDim.x + threadIdx.x; each V entry read from the stage (one broadcast 16-byte
+// shared load of (re, im, -im, re)) feeds two packed FP32 FMAs (FFMA2) per receiver:
+//   (y_re, y_im) += (g_re, g_re) * (re, im) + (g_im, g_im) * (-im, re).
+// The order-p loop is unrolled so every (m1, p) has a compile-time row count. Measured on B200
+// (2000 spheres, lmax 6): one receiver per thread 15.4 ms, two 22.3 ms (the second receiver's
+// pair-side registers push the kernel to fewer resident blocks), against 24.5 ms for float64.
+// Pair geometry and h_0, h_1 are evaluated in float64 (positions stay exact), then rounded; every
+// recurrence runs in float.
 //
 // Included by coupling.cuh inside namespace yasf, after contract_body (it uses the stage helpers).
 #pragma once
 
-// Receivers per thread and whether the order-p loop is unrolled: build-time choices (defaults 2, 1),
+// Receivers per thread and whether the order-p loop is unrolled: build-time choices (defaults 1, 1),
 // the host layout follows kC64Receivers.
 #ifndef YASF_C64_RECEIVERS
-#define YASF_C64_RECEIVERS 2
+#define YASF_C64_RECEIVERS 1
 #endif
 #ifndef YASF_C64_UNROLL_P
 #define YASF_C64_UNROLL_P 1

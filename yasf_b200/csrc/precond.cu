@@ -51,6 +51,10 @@ struct yasf_precond {
   double2* d_dinv64 = nullptr;
   double2* d_z = nullptr;
   int z_cols = 0;
+  // one-column applies: ticket order of the tile rows (forward sweep, then backward) and the
+  // ticket / abort / finished-row words of the single-launch solve
+  int2* d_order = nullptr;
+  int* d_sync = nullptr;
   // the sweep launches of an apply, captured once per (columns, factor precision) as a CUDA graph
   // on a private stream and replayed on the caller's stream
   struct SweepGraph {
@@ -337,6 +341,17 @@ extern "C" int yasf_precond_create(const yasf_plan* plan, int n_particles, int n
     up(&pc->d_row0, row0.data(), row0.size());
     up(&pc->d_tile0, tile0.data(), tile0.size());
     up(&pc->d_pre, pre.data(), pre.size());
+    std::vector<int2> order;
+    order.reserve(2 * (size_t)tiles);
+    for (int upper = 0; upper < 2; ++upper)
+      for (int c = 0; c < steps; ++c)
+        for (int b = 0; b < n_blocks; ++b) {
+          const int nt = (dims[b] + kLuT - 1) / kLuT;
+          if (c < nt) order.push_back(make_int2(b, upper ? nt - 1 - c : c));
+        }
+    up(&pc->d_order, order.data(), order.size());
+    if (e == cudaSuccess)
+      e = cudaMalloc(reinterpret_cast<void**>(&pc->d_sync), (2 + 2 * (size_t)n_blocks) * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&pc->d_piv), std::max(1, rows) * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&pc->d_err), sizeof(int));
   }
@@ -370,6 +385,8 @@ extern "C" int yasf_precond_destroy(yasf_precond* pc) {
   cudaFree(pc->d_dinv);
   cudaFree(pc->d_dinv64);
   cudaFree(pc->d_z);
+  cudaFree(pc->d_order);
+  cudaFree(pc->d_sync);
   for (auto& g : pc->graphs) cudaGraphExecDestroy(g.exec);
   if (pc->capture_stream) cudaStreamDestroy(pc->capture_stream);
   delete pc;
@@ -403,6 +420,10 @@ int lu_smem_attributes() {
                                      2 * one));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)yasf::kLuUpdateSmem));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_solve_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)yasf::lu_solve_smem<float2>()));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_solve_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)yasf::lu_solve_smem<double2>()));
   done = 1;
   return YASF_OK;
 }
@@ -579,7 +600,30 @@ extern "C" int yasf_precond_apply(const yasf_precond* pc, const double* x, doubl
                                                      pc->d_row0, pc->d_piv, reinterpret_cast<const double2*>(x),
                                                      pc->d_z));
     const LuGeom g = lu_geom(pc);
-    // the forward and backward sweeps (one launch per tile row) into stream `ss`
+    if (nrhs == 1) {  // both sweeps in one launch, rows ordered by tickets
+      if (int st = lu_smem_attributes()) return st;
+      LuSolveArgs sa;
+      sa.g = g;
+      sa.order = pc->d_order;
+      sa.n_tiles = pc->n_tiles;
+      sa.z = pc->d_z;
+      sa.sync = pc->d_sync;
+      sa.wait_ns = stall_hook().panel_wait_ns;
+      sa.stall = stall_hook().role == YASF_STALL_PRECOND ? 1 : 0;
+      YASF_CUDA_TRY(cudaMemsetAsync(pc->d_sync, 0, (2 + 2 * (size_t)pc->n_blocks) * sizeof(int), s));
+      if (f64)
+        YASF_COUNTED(lu_solve_kernel<double2><<<2 * pc->n_tiles, 256, lu_solve_smem<double2>(), s>>>(
+            sa, pc->d_mat, pc->d_dinv64));
+      else
+        YASF_COUNTED(lu_solve_kernel<float2><<<2 * pc->n_tiles, 256, lu_solve_smem<float2>(), s>>>(
+            sa, pc->d_mat32, pc->d_dinv));
+      YASF_COUNTED(lu_scatter_kernel<<<gb, 256, 0, s>>>(pc->total_rows, pc->plan->nmax, nrhs, ld, pc->d_row_block,
+                                                        pc->d_row_local, pc->d_block_ptr, pc->d_particles, pc->d_z,
+                                                        reinterpret_cast<double2*>(y)));
+      YASF_CUDA_TRY(cudaGetLastError());
+      return YASF_OK;
+    }
+    // several columns: the forward and backward sweeps (one launch per tile row) into stream `ss`
     auto sweeps = [&](cudaStream_t ss) -> int {
       int launched = 0;
       for (int upper = 0; upper < 2; ++upper)

@@ -49,8 +49,11 @@ __host__ __device__ constexpr int valid_rows(int L, int m1, int p) {
 // whole bundle in registers while the pair-side factors (Hankel, Legendre, azimuthal phase)
 // are generated once per bundle. Bundles are a snake deal of m1 sorted by |m1|, which
 // balances both the row count and the stream length.
+#ifndef YASF_BUNDLES_L6
+#define YASF_BUNDLES_L6 4
+#endif
 __host__ __device__ constexpr int num_bundles(int L) {
-  return L <= 3 ? 1 : (L == 4 ? 2 : (L == 5 ? 3 : (L == 6 ? 4 : (L == 7 ? 6 : 8))));
+  return L <= 3 ? 1 : (L == 4 ? 2 : (L == 5 ? 3 : (L == 6 ? YASF_BUNDLES_L6 : (L == 7 ? 6 : 8))));
 }
 
 // The i-th m1 in the order 0, 1, -1, 2, -2, ...
