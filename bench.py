@@ -694,7 +694,10 @@ def run_serve(args, rank: int, world: int) -> None:
         "rhs_solves": tot["rhs_solves"], "makespan_s": tot["makespan_s"], "rank0_summary": summ,
         "requests": [{"rid": r.rid, "n": r.n_spheres, "lmax": r.lmax, "nrhs": r.nrhs,
                       "inner": r.stats.get("inner"), "group": r.stats.get("group_size"),
-                      "inner_steps": r.stats.get("inner_steps"), "admitted_s": round(r.admitted, 3),
+                      "inner_steps": r.stats.get("inner_steps"),
+                      "restart": r.stats.get("restart"),
+                      "relative_residual": r.stats.get("worst_relative_residual"),
+                      "admitted_s": round(r.admitted, 3),
                       "latency_s": round(r.latency, 3), "error": r.error} for r in results],
         "c_ext_error_vs_fp64": {"max": max((e["c_ext_rel_err"] for e in errs), default=None),
                                 "samples": errs},
@@ -887,6 +890,52 @@ def matvec_probe(args) -> None:
                       "ms": e0.elapsed_time(e1) / 3, "max_abs": float(y.abs().max())}))
 
 
+def precond_probe(args) -> None:
+    """Block-Jacobi preconditioner on the first N spheres of the C2 aggregate (4x4x4 cells of the
+    aggregate's extent, as in the default bench line): prepare (assemble, batched LU, finalize),
+    then one warm-up and five timed one-column complex64 applies, and one 16-column apply."""
+    import torch
+
+    from yasf_b200.device import PRECISIONS, CouplingDevice, DevicePreconditioner
+    from yasf_b200.mie import mie_tmatrix_per_sphere
+    from yasf_b200.numerics import cached_translation_table
+    from yasf_b200.preconditioner import make_particle_partition
+
+    agg, _, _ = workload("c2")
+    n = min(args.precond_probe, agg.n)
+    pos = agg.positions[:n]
+    dev0 = torch.device("cuda", 0)
+    dev = CouplingDevice(agg.lmax, cached_translation_table(agg.lmax), pos, agg.k, dev0)
+    tmat = torch.from_numpy(mie_tmatrix_per_sphere(agg.lmax, agg.k, agg.radii[:n], agg.refractive_index)).to(dev0)
+    ext = agg.positions.max(axis=0) - agg.positions.min(axis=0)
+    blocks = make_particle_partition(pos, (ext + 2.0) / 4)
+    pc = DevicePreconditioner(dev, blocks)
+    phases = pc.prepare(tmat)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(dev.n, dtype=torch.complex128, device=dev0, generator=g)
+    X = torch.randn(16, dev.n, dtype=torch.complex128, device=dev0, generator=g)
+    y = pc.apply(x, PRECISIONS["c64"])
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        y = pc.apply(x, PRECISIONS["c64"])
+    e1.record()
+    e1.synchronize()
+    one = e0.elapsed_time(e1) / 5
+    Y = pc.apply(X, PRECISIONS["c64"])
+    e0.record()
+    Y = pc.apply(X, PRECISIONS["c64"])
+    e1.record()
+    e1.synchronize()
+    dims = [len(b) * dev.nmax for b in blocks]
+    factor_bytes = sum(d * d for d in dims) * 8  # complex64 L and U, streamed once per apply
+    print(json.dumps({"probe": "precond", "n": n, "blocks": len(blocks), "max_dim": max(dims),
+                      "prepare_s": phases, "factor_bytes": factor_bytes, "apply_c64_ms": one,
+                      "apply_c64_gbs": factor_bytes / one / 1e6, "apply_c64_16cols_ms": e0.elapsed_time(e1),
+                      "finite": bool(torch.isfinite(y).all() and torch.isfinite(Y).all())}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -907,6 +956,9 @@ def main() -> None:
     ap.add_argument("--panel-probe", type=int, default=0, metavar="N",
                     help="profiling aid: run 4 TF32 panel matvecs on the first N spheres and exit")
     ap.add_argument("--nrhs", type=int, default=128, help="columns of --panel-probe")
+    ap.add_argument("--precond-probe", type=int, default=0, metavar="N",
+                    help="profiling aid: prepare the block-Jacobi preconditioner on the first N spheres, "
+                         "time its applies and exit")
     ap.add_argument("--float64-panel", action="store_true",
                     help="--panel-probe times the float64 dense multi-column coupling instead")
     ap.add_argument("--restart-batched", type=int, default=50, help="inner GMRES cycle length (c3)")
@@ -929,6 +981,9 @@ def main() -> None:
         return
     if args.panel_probe:
         panel_probe(args)
+        return
+    if args.precond_probe:
+        precond_probe(args)
         return
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)

@@ -222,7 +222,9 @@ int yasf_plane_wave_rhs(int lmax, int n_particles, const double* positions, int 
  * stats (host, may be NULL): [0] lockstep inner steps, [1] inner operator applications (all columns
  * each), [2] float64 applications, [3] worst relative residual, [4] unconverged columns,
  * [5] refinement steps, [6] columns, [7] work items per application. column_residuals (host, may be
- * NULL): final relative residual of every column, aggregate by aggregate. Synchronous. */
+ * NULL): final relative residual of every column, aggregate by aggregate. Synchronous.
+ * yasf_grouped_workspace_size reads only n_particles and nrhs of each problem (its pointers may be
+ * NULL), so a group can be sized before its buffers exist. */
 typedef struct {
   int n_particles;
   const double* positions;   /* device (N, 3) */

@@ -91,9 +91,7 @@ def test_admission_footprint_covers_the_device_memory_of_a_request(cuda_device):
         assert fp <= 2 * peak + (16 << 20), (req.rid, peak, fp)
 
 
-def test_small_requests_grouped_equal_alone(cuda_device):
-    """Five small requests of one lmax arriving together are served by one grouped solve; each
-    result equals that request solved alone (a group of one), and the float64 solve within 1e-6."""
+def _small_requests():
     reqs = []
     for i, (n, R) in enumerate([(30, 1), (80, 2), (12, 1), (55, 2), (41, 1)]):
         rng = np.random.default_rng(700 + i)
@@ -102,6 +100,33 @@ def test_small_requests_grouped_equal_alone(cuda_device):
         agg = Aggregate(f"g{i}", pos, radii, complex(1.45 + 0.02 * i, 0.01), 0.5 + 0.02 * i, 4, i)
         polar, azim, pol = incidences(1)
         reqs.append(Request(i, 0.0, agg, polar[:R], azim[:R], pol[:R]))
+    return reqs
+
+
+def test_group_footprint_covers_the_device_memory_of_a_group(cuda_device):
+    """A group is admitted by the grouped solve's own size query plus its requests' vectors: at
+    least the device memory the grouped solve allocates."""
+    from yasf_b200.serve import group_footprint_bytes
+
+    reqs = _small_requests()
+    cfg = ServeConfig(max_slots=1, rtol=1e-6)
+    fp = group_footprint_bytes(reqs, cfg, cuda_device)
+    solve_group(reqs, cfg, cuda_device)  # plans and caches set up
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    base = torch.cuda.memory_allocated(cuda_device)
+    torch.cuda.reset_peak_memory_stats(cuda_device)
+    out = solve_group(reqs, cfg, cuda_device)
+    torch.cuda.synchronize()
+    peak = torch.cuda.max_memory_allocated(cuda_device) - base
+    assert all(r.error is None for r in out)
+    assert peak <= fp, (peak, fp)
+
+
+def test_small_requests_grouped_equal_alone(cuda_device):
+    """Five small requests of one lmax arriving together are served by one grouped solve; each
+    result equals that request solved alone (a group of one), and the float64 solve within 1e-6."""
+    reqs = _small_requests()
     cfg = ServeConfig(max_slots=2, rtol=1e-8, keep_solutions=True)
     assert all(groupable(q, cfg) for q in reqs)
     mixed = Server(cfg, device=cuda_device).run(reqs, realtime=False)

@@ -118,3 +118,29 @@ def test_admission_never_exceeds_the_budget():
     res = srv.run(reqs)
     assert all(r.error is None for r in res)
     assert state["peak"] <= budget and state["peak"] > 600  # several in flight at once
+
+
+def test_cycle_length_by_columns():
+    """Requests with few columns get long GMRES cycles (their basis is cheap), wide ones the base
+    cycle; the admission footprint is sized with the same cycle length."""
+    cfg = ServeConfig()
+    assert [cfg.restart_for(R) for R in (1, 2, 4, 5, 16, 17, 64)] == [100, 100, 100, 60, 60, 30, 30]
+    cfg = ServeConfig(restart=40, restart_few=())
+    assert cfg.restart_for(1) == 40
+
+
+def test_unconverged_request_is_an_error():
+    """A stand-in solve that reports unconverged columns is not counted as completed."""
+
+    def solve(req, cfg, device):
+        agg = req.aggregate
+        r = RequestResult(req.rid, agg.n, agg.lmax, len(req.pol), c_ext=np.zeros(len(req.pol)))
+        if req.rid == 1:
+            r.error = "not converged: 1 of 1 columns"
+        return r
+
+    srv = Server(ServeConfig(max_slots=2, hbm_budget_bytes=100), device="cpu", solve_fn=solve,
+                 footprint_fn=lambda r, c: 1)
+    out = srv.run([_req(0, 0.0), _req(1, 0.0), _req(2, 0.0)], realtime=False)
+    s = summarize(out)
+    assert s["completed"] == 2 and s["failed"] == 1 and s["rhs_solves"] == 2

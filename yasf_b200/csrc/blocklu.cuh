@@ -684,9 +684,9 @@ __global__ void __launch_bounds__(256, 2) lu_solve_kernel(LuSolveArgs a, const F
   ax += __shfl_xor_sync(0xffffffffu, ax, 2);
   ay += __shfl_xor_sync(0xffffffffu, ay, 2);
   if (ok) {
-    if (part == 0) {
+    if (part == 0) {  // rows past a ragged edge stage zero (their clamped products are not theirs)
       const double2 o = row < vi ? __ldcg(zb + i0 + row) : make_double2(0.0, 0.0);
-      zrow[row] = make_double2(o.x - ax, o.y - ay);
+      zrow[row] = row < vi ? make_double2(o.x - ax, o.y - ay) : make_double2(0.0, 0.0);
     }
     __syncthreads();
     double ox = 0.0, oy = 0.0;
@@ -709,7 +709,10 @@ __global__ void __launch_bounds__(256, 2) lu_solve_kernel(LuSolveArgs a, const F
   }
   __threadfence();
   __syncthreads();
-  if (tid == 0) atomicMax(done, upper ? nt - i : i + 1);
+  if (tid == 0) {  // release: the row's stores (ordered before the barrier) precede the count
+    __threadfence();
+    atomicMax(done, upper ? nt - i : i + 1);
+  }
 }
 
 }  // namespace yasf

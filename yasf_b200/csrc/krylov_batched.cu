@@ -889,7 +889,10 @@ int dispatch_grouped_contract(int lmax, int precision, const GroupedContractArgs
 extern "C" int yasf_grouped_workspace_size(const yasf_plan* plan, int n_problems, const yasf_problem* problems,
                                            int restart, size_t* bytes) {
   if (!bytes || restart <= 0 || restart > 512) return YASF_ERR_INVALID_ARGUMENT;
-  if (int st = group_check(plan, n_problems, problems)) return st;
+  // the size depends only on the counts: a caller may size a group before its buffers exist
+  if (!plan || n_problems <= 0 || !problems) return YASF_ERR_INVALID_ARGUMENT;
+  for (int p = 0; p < n_problems; ++p)
+    if (problems[p].n_particles <= 0 || problems[p].nrhs <= 0) return YASF_ERR_INVALID_ARGUMENT;
   *bytes = group_layout(plan, n_problems, problems, restart).total;
   return YASF_OK;
 }

@@ -12,11 +12,14 @@ incidences (directions x polarisations = R right-hand sides). The loop:
   TF32 panel as the inner operator (complex64 coupling kernel for one or two columns; with
   ``ServeConfig.tuner`` set, whichever of the two the autotuner measured cheaper for the request's
   (lmax, N, R)), float64 residuals, stopping at rtol (1e-6 by default, which keeps the extinction
-  cross section well inside 1e-6 of the float64 solution);
+  cross section well inside 1e-6 of the float64 solution); GMRES cycles of 100 steps for up to 4
+  columns, 60 up to 16, 30 beyond (``ServeConfig.restart_for``); a request whose columns do not
+  reach rtol within max_refine cycles is reported as an error, not as a completed solve;
 - packs the small requests whose inner operator is the complex64 kernel (up to
   ``group_max_spheres`` spheres) that have arrived, with the same lmax, into one grouped solve
   (yasf_grouped_solve): every operator application of the group is one persistent work-queue
-  contraction for all of them, instead of a launch sequence per request;
+  contraction for all of them, instead of a launch sequence per request; a group is admitted by
+  the grouped solve's own size query (yasf_grouped_workspace_size) plus its requests' vectors;
 - reports per-request latency (completion - arrival, queueing included), p50/p99 and solves/s.
 
 The kernels are deterministic (no atomics in any reduction), so a request's result does not depend
@@ -46,9 +49,19 @@ class ServeConfig:
     max_slots: int = 4
     hbm_budget_bytes: int | None = None   # default: 80 % of the free device memory at start
     rtol: float = 1e-6
-    restart: int = 30
+    restart: int = 30                     # GMRES cycle length of requests with many columns
+    restart_few: tuple = ((4, 100), (16, 60))  # (up to R columns, cycle length): longer cycles
     max_refine: int = 8
     inner_rtol: float = 1e-3
+
+    def restart_for(self, nrhs: int) -> int:
+        """GMRES cycle length of a request with nrhs columns. Unpreconditioned restarted GMRES
+        stagnates on dense aggregates with short cycles; a long cycle costs R (restart + 1) vectors
+        of basis, cheap for a few columns, so requests with few columns get the longer cycles."""
+        for cols, restart in self.restart_few:
+            if nrhs <= cols:
+                return int(restart)
+        return int(self.restart)
     keep_solutions: bool = False
     tuner: object | None = None           # an autotune.Autotuner: inner operator by measurement
     group_small: bool = True              # small complex64-inner requests share one grouped solve
@@ -106,7 +119,7 @@ def footprint_bytes(req: Request, cfg: ServeConfig, device: torch.device | None 
     nmax = 2 * agg.lmax * (agg.lmax + 2)
     n = agg.n * nmax
     R = len(req.pol)
-    restart = int(max(1, min(cfg.restart, 512, n)))
+    restart = int(max(1, min(cfg.restart_for(R), 512, n)))
     device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
     plan = Plan.get(agg.lmax, cached_translation_table(agg.lmax), device)
     kinds = ("tf32", "c64") if cfg.tuner is not None else (inner_kind(agg.lmax, R),)
@@ -116,13 +129,48 @@ def footprint_bytes(req: Request, cfg: ServeConfig, device: torch.device | None 
         call("yasf_batched_workspace_size", plan.handle, agg.n, R, restart,
              CouplingDevice.INNER_KINDS[kind], ctypes.byref(nb))
         ws = max(ws, nb.value)
-    gran = 2 << 20
+    return _rounded(ws) + _vector_bytes(req)
 
-    def rounded(b):
-        return (int(b) + gran - 1) // gran * gran
 
-    return (rounded(ws) + rounded(n * 16) + 3 * rounded(R * n * 16) + rounded(agg.n * 24)
-            + rounded(R * nmax * 16) + rounded(R * 24) + rounded(R * 16) + rounded(256))
+_GRAN = 2 << 20  # the caching allocator's block granularity
+
+
+def _rounded(b: int) -> int:
+    return (int(b) + _GRAN - 1) // _GRAN * _GRAN
+
+
+def _vector_bytes(req: Request) -> int:
+    """A request's device vectors besides the solve's workspace: T (n), the incident coefficients,
+    right-hand sides and solution (R n each, complex128), positions, mode factors, wave vectors."""
+    agg = req.aggregate
+    nmax = 2 * agg.lmax * (agg.lmax + 2)
+    n = agg.n * nmax
+    R = len(req.pol)
+    return (_rounded(n * 16) + 3 * _rounded(R * n * 16) + _rounded(agg.n * 24) + _rounded(R * nmax * 16)
+            + _rounded(R * 24) + _rounded(R * 16) + _rounded(256))
+
+
+def group_restart(reqs: list[Request], cfg: ServeConfig) -> int:
+    return min(cfg.restart_for(max(len(r.pol) for r in reqs)), 512)
+
+
+def group_footprint_bytes(reqs: list[Request], cfg: ServeConfig, device: torch.device | None = None) -> int:
+    """Device bytes a grouped solve of `reqs` holds: the library's yasf_grouped_workspace_size for
+    the group (which reads only the sphere and column counts), plus every request's vectors."""
+    import ctypes
+
+    from yasf_b200 import _lib
+    from yasf_b200.device import Plan
+
+    lmax = reqs[0].aggregate.lmax
+    device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+    plan = Plan.get(lmax, cached_translation_table(lmax), device)
+    probs = (_lib.YasfProblem * len(reqs))()
+    for i, req in enumerate(reqs):
+        probs[i] = _lib.YasfProblem(req.aggregate.n, None, req.aggregate.k, None, None, None, len(req.pol))
+    nb = ctypes.c_size_t()
+    call("yasf_grouped_workspace_size", plan.handle, len(reqs), probs, group_restart(reqs, cfg), ctypes.byref(nb))
+    return _rounded(nb.value) + sum(_vector_bytes(r) for r in reqs)
 
 
 def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> RequestResult:
@@ -141,8 +189,8 @@ def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> Reque
     if decision is not None:
         decision.apply_tiles()  # tile shapes for this thread's launches
     try:
-        X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
-                                  inner_rtol=cfg.inner_rtol, inner=inner)
+        X, st = dev.batched_solve(tmat, Bt, rtol=cfg.rtol, restart=min(cfg.restart_for(R), 512, dev.n),
+                                  max_refine=cfg.max_refine, inner_rtol=cfg.inner_rtol, inner=inner)
     finally:
         if decision is not None:
             from yasf_b200._lib import set_tiles
@@ -151,9 +199,13 @@ def solve_request(req: Request, cfg: ServeConfig, device: torch.device) -> Reque
     res.c_ext = (-torch.real((A.conj() * X).sum(dim=1)) / agg.k**2 * np.pi).cpu().numpy()
     st.pop("column_residuals", None)
     st["inner"] = inner
+    st["restart"] = min(cfg.restart_for(R), 512, dev.n)
     if decision is not None:
         st["tiles"] = dict(decision.tiles)
     res.stats = st
+    if st.get("unconverged", 0):
+        res.error = (f"not converged: {st['unconverged']} of {R} columns, relative residual "
+                     f"{st['worst_relative_residual']:.3e} after {st['inner_steps']} inner steps")
     if cfg.keep_solutions:
         res.x = X.cpu().numpy()
     return res
@@ -182,7 +234,7 @@ def solve_group(reqs: list[Request], cfg: ServeConfig, device: torch.device) -> 
         A, B = dev.plane_wave_rhs(tmat, req.polar, req.azimuthal, req.pol)
         items.append((dev, tmat, B))
         As.append(A)
-    Xs, st = grouped_solve(items, rtol=cfg.rtol, restart=cfg.restart, max_refine=cfg.max_refine,
+    Xs, st = grouped_solve(items, rtol=cfg.rtol, restart=group_restart(reqs, cfg), max_refine=cfg.max_refine,
                            inner_rtol=cfg.inner_rtol, inner="c64")
     colres = st.pop("column_residuals")
     c0 = 0
@@ -191,7 +243,7 @@ def solve_group(reqs: list[Request], cfg: ServeConfig, device: torch.device) -> 
         R = len(req.pol)
         res = RequestResult(req.rid, agg.n, agg.lmax, R)
         res.c_ext = (-torch.real((A.conj() * X).sum(dim=1)) / agg.k**2 * np.pi).cpu().numpy()
-        res.stats = dict(st, inner="c64 grouped", group_size=len(reqs),
+        res.stats = dict(st, inner="c64 grouped", group_size=len(reqs), restart=group_restart(reqs, cfg),
                          worst_relative_residual=max(colres[c0:c0 + R]))
         if max(colres[c0:c0 + R]) > cfg.rtol:
             res.error = f"not converged: relative residual {max(colres[c0:c0 + R]):.3e}"
@@ -286,6 +338,7 @@ class Server:
                     pending.popleft()
                     if self.device.type == "cuda" and groupable(req, self.cfg):
                         # gather the arrived small requests of the same lmax into one grouped solve
+                        # (admitted by the grouped solve's own size query)
                         group, gfp = [req], fp
                         for other in list(pending):
                             if realtime and other.arrival > now:
@@ -294,12 +347,12 @@ class Server:
                                 break
                             if other.aggregate.lmax != req.aggregate.lmax or not groupable(other, self.cfg):
                                 continue
-                            ofp = self._footprint(other, self.cfg)
-                            if used + gfp + ofp > budget:
+                            tfp = group_footprint_bytes(group + [other], self.cfg, self.device)
+                            if used + tfp > budget:
                                 continue
                             pending.remove(other)
                             group.append(other)
-                            gfp += ofp
+                            gfp = tfp
                         used += gfp
                         fut = pool.submit(self._worker_group, group, t0)
                         inflight[fut] = (group, gfp, now)
