@@ -90,7 +90,8 @@ int yasf_test_stall(int role, int contract_polls, double panel_wait_seconds);
  * current CUDA device and allocates its own device memory. */
 int yasf_plan_create(int lmax, const double* translation_ab5, yasf_plan** plan);
 int yasf_plan_destroy(yasf_plan* plan);
-/* nmax, stream entries per source particle (all bundles), source-side terms per particle. */
+/* nmax, stream entries per source particle (all bundles) and source-side terms per particle of the
+ * float64 kernels' stream layout (the complex64 kernel may split the stream into other bundles). */
 int yasf_plan_info(const yasf_plan* plan, int* nmax, long long* stream_entries,
                    long long* source_terms);
 /* Host-only check (no device, nothing allocated on a GPU): builds the generation layouts a plan

@@ -103,7 +103,8 @@ CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int preci
   // split into chunks to get there.
   const int waves = tile_config().contract_waves > 0 ? tile_config().contract_waves : 2;
   const long long want = (long long)waves * resident_blocks(plan->lmax, precision, lay.threads) * sms;
-  const long long base = (long long)lay.tiles * plan->n_bundles;
+  const yasf_stream_layout& sl = plan->layout(precision);
+  const long long base = (long long)lay.tiles * sl.n_bundles;
   int chunks = (int)std::max<long long>(1, (want + base - 1) / base);
   chunks = std::min(chunks, N);
   // Cap the partial-sum buffer at 1 GiB.
@@ -112,7 +113,7 @@ CouplingLayout coupling_layout(const yasf_plan* plan, int n_particles, int preci
   lay.sources_per_chunk = (N + chunks - 1) / chunks;
   lay.chunks = (N + lay.sources_per_chunk - 1) / lay.sources_per_chunk;
   auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-  lay.v_bytes = up((size_t)N * plan->total_entries * vsize);
+  lay.v_bytes = up((size_t)N * sl.total_entries * vsize);
   lay.partial_bytes = up(per_chunk * lay.chunks);
   lay.dot_bytes = up(1024 * sizeof(double2) + 256);  // block sums + the stage-timeout word
   lay.total = lay.v_bytes + lay.partial_bytes + lay.dot_bytes;
@@ -157,22 +158,23 @@ int coupling_column(const yasf_plan* plan, int n_particles, const double* positi
   if (regular && precision != YASF_C128) return YASF_ERR_UNSUPPORTED;
 
   // 1) source side: V streams
+  const yasf_stream_layout& sl = plan->layout(precision);
   VBuildArgs va{};
   va.n_particles = n_particles;
   va.nmax = plan->nmax;
-  va.total_entries = plan->total_entries;
-  va.n_bundles = plan->n_bundles;
+  va.total_entries = sl.total_entries;
+  va.n_bundles = sl.n_bundles;
   for (int b = 0; b < 8; ++b) {
-    va.bundle_begin[b] = plan->bundle_begin[b];
-    va.bundle_len[b] = plan->bundle_len[b];
+    va.bundle_begin[b] = sl.bundle_begin[b];
+    va.bundle_len[b] = sl.bundle_len[b];
   }
-  va.entry_ptr = plan->d_entry_ptr;
-  va.term_n2 = plan->d_term_n2;
-  va.term_coef = plan->d_term_coef;
+  va.entry_ptr = sl.d_entry_ptr;
+  va.term_n2 = sl.d_term_n2;
+  va.term_coef = sl.d_term_coef;
   va.x = reinterpret_cast<const double2*>(x);
   va.v = vbuf;
   {
-    const dim3 grid((plan->total_entries + 255) / 256, std::min(n_particles, 65535));
+    const dim3 grid((sl.total_entries + 255) / 256, std::min(n_particles, 65535));
     if (precision == YASF_C64) YASF_COUNTED(vbuild_kernel<float><<<grid, 256, 0, stream>>>(va));
     else YASF_COUNTED(vbuild_kernel<double><<<grid, 256, 0, stream>>>(va));
     YASF_CUDA_TRY(cudaGetLastError());
@@ -187,8 +189,8 @@ int coupling_column(const yasf_plan* plan, int n_particles, const double* positi
   ca.v = vbuf;
   ca.leg = plan->d_leg;
   for (int b = 0; b < 8; ++b) {
-    ca.bundle_begin[b] = plan->bundle_begin[b];
-    ca.bundle_len[b] = plan->bundle_len[b];
+    ca.bundle_begin[b] = sl.bundle_begin[b];
+    ca.bundle_len[b] = sl.bundle_len[b];
   }
   ca.partial = partial;
   ca.err = err;
@@ -320,6 +322,18 @@ extern "C" unsigned long long yasf_kernel_launches(void) {
   return g_launches.load(std::memory_order_relaxed);
 }
 
+static void free_stream_layouts(yasf_plan* plan) {
+  for (auto& lay : plan->stream) {
+    if (!lay.owns) continue;
+    cudaFree(lay.d_entry_ptr);
+    cudaFree(lay.d_term_n2);
+    cudaFree(lay.d_term_coef);
+    lay.d_entry_ptr = nullptr;
+    lay.d_term_n2 = nullptr;
+    lay.d_term_coef = nullptr;
+  }
+}
+
 // Build the bundle streams from the dense a5/b5 table. The stream order is the one the
 // contraction kernel walks (yasf_common.cuh: bundle_stream_length).
 extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
@@ -344,55 +358,63 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
     delete plan;
     return YASF_ERR_CUDA;
   }
-  plan->n_bundles = num_bundles(L);
-
-  std::vector<int> entry_ptr(1, 0), term_n2;
-  std::vector<double2> term_coef;
-  int begin = 0;
-  for (int b = 0; b < plan->n_bundles; ++b) {
-    const BundleInfo bi = make_bundle(L, b);
-    plan->bundle_begin[b] = begin;
-    int len = 0;
-    for (int d = 0; d <= 2 * L; ++d)
-      for (int p = d; p <= 2 * L; ++p)
-        for (int s = 0; s < (d == 0 ? 1 : 2); ++s) {
-          const int sg = s == 0 ? 1 : -1;
-          for (int i = 0; i < bi.count; ++i) {
-            const int m1 = bi.m1[i];
-            const int m2 = m1 + sg * d;
-            if (m2 < -L || m2 > L) continue;
-            const int nv = valid_rows(L, m1, p);
-            for (int r = 0; r < nv; ++r) {
-              const int n1 = mode_index(L, row_tau(r), row_l(L, r), m1);
-              for (int tau2 = 1; tau2 <= 2; ++tau2)
-                for (int l2 = std::max(1, std::abs(m2)); l2 <= L; ++l2) {
-                  const int n2 = mode_index(L, tau2, l2, m2);
-                  double re, im;
-                  A(n1, n2, p, &re, &im);
-                  if (re != 0.0 || im != 0.0) {
-                    term_n2.push_back(n2);
-                    term_coef.push_back(make_double2(re, im));
+  // the stream layouts of the float64 and complex64 kernels (shared when their bundle counts agree)
+  std::vector<int> entry_ptr_l[2], term_n2_l[2];
+  std::vector<double2> term_coef_l[2];
+  for (int li = 0; li < 2; ++li) {
+    yasf_stream_layout& lay = plan->stream[li];
+    lay.n_bundles = num_bundles(L, li == 1);
+    if (li == 1 && lay.n_bundles == plan->stream[0].n_bundles) continue;
+    std::vector<int>& entry_ptr = entry_ptr_l[li];
+    std::vector<int>& term_n2 = term_n2_l[li];
+    std::vector<double2>& term_coef = term_coef_l[li];
+    entry_ptr.assign(1, 0);
+    int begin = 0;
+    for (int b = 0; b < lay.n_bundles; ++b) {
+      const BundleInfo bi = make_bundle(L, b, lay.n_bundles);
+      lay.bundle_begin[b] = begin;
+      int len = 0;
+      for (int d = 0; d <= 2 * L; ++d)
+        for (int p = d; p <= 2 * L; ++p)
+          for (int s = 0; s < (d == 0 ? 1 : 2); ++s) {
+            const int sg = s == 0 ? 1 : -1;
+            for (int i = 0; i < bi.count; ++i) {
+              const int m1 = bi.m1[i];
+              const int m2 = m1 + sg * d;
+              if (m2 < -L || m2 > L) continue;
+              const int nv = valid_rows(L, m1, p);
+              for (int r = 0; r < nv; ++r) {
+                const int n1 = mode_index(L, row_tau(r), row_l(L, r), m1);
+                for (int tau2 = 1; tau2 <= 2; ++tau2)
+                  for (int l2 = std::max(1, std::abs(m2)); l2 <= L; ++l2) {
+                    const int n2 = mode_index(L, tau2, l2, m2);
+                    double re, im;
+                    A(n1, n2, p, &re, &im);
+                    if (re != 0.0 || im != 0.0) {
+                      term_n2.push_back(n2);
+                      term_coef.push_back(make_double2(re, im));
+                    }
                   }
-                }
-              entry_ptr.push_back((int)term_n2.size());
-              ++len;
+                entry_ptr.push_back((int)term_n2.size());
+                ++len;
+              }
             }
           }
-        }
-    if (len != bundle_stream_length(L, b)) {
-      delete plan;
-      set_error_text("internal: stream length mismatch");
-      return YASF_ERR_INVALID_ARGUMENT;
+      if (len != bundle_stream_length(L, b, lay.n_bundles)) {
+        delete plan;
+        set_error_text("internal: stream length mismatch");
+        return YASF_ERR_INVALID_ARGUMENT;
+      }
+      if (len & 1) {  // pad to an even entry count (32-byte aligned per-source streams)
+        entry_ptr.push_back((int)term_n2.size());
+        ++len;
+      }
+      lay.bundle_len[b] = len;
+      begin += len;
     }
-    if (len & 1) {  // pad to an even entry count (32-byte aligned per-source streams)
-      entry_ptr.push_back((int)term_n2.size());
-      ++len;
-    }
-    plan->bundle_len[b] = len;
-    begin += len;
+    lay.total_entries = begin;
+    lay.total_terms = (long long)term_n2.size();
   }
-  plan->total_entries = begin;
-  plan->total_terms = (long long)term_n2.size();
 
   // Explicit (n1, n2) term lists for block assembly.
   std::vector<int> pair_ptr(1, 0), pair_p;
@@ -449,9 +471,7 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
 
   auto fail = [&](cudaError_t e) {
     set_cuda_error(e);
-    cudaFree(plan->d_entry_ptr);
-    cudaFree(plan->d_term_n2);
-    cudaFree(plan->d_term_coef);
+    free_stream_layouts(plan);
     cudaFree(plan->d_leg);
     cudaFree(plan->d_pair_ptr);
     cudaFree(plan->d_pair_p);
@@ -475,9 +495,17 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
                         cudaMemcpyHostToDevice)) != cudaSuccess)                        \
       return fail(e);                                                                   \
   } while (0)
-  YASF_UPLOAD(plan->d_entry_ptr, entry_ptr);
-  YASF_UPLOAD(plan->d_term_n2, term_n2);
-  YASF_UPLOAD(plan->d_term_coef, term_coef);
+  for (int li = 0; li < 2; ++li) {
+    yasf_stream_layout& lay = plan->stream[li];
+    if (li == 1 && lay.n_bundles == plan->stream[0].n_bundles) {
+      lay = plan->stream[0];
+      lay.owns = false;
+      continue;
+    }
+    YASF_UPLOAD(lay.d_entry_ptr, entry_ptr_l[li]);
+    YASF_UPLOAD(lay.d_term_n2, term_n2_l[li]);
+    YASF_UPLOAD(lay.d_term_coef, term_coef_l[li]);
+  }
   YASF_UPLOAD(plan->d_pair_ptr, pair_ptr);
   YASF_UPLOAD(plan->d_pair_p, pair_p);
   YASF_UPLOAD(plan->d_pair_coef, pair_coef);
@@ -503,9 +531,7 @@ extern "C" int yasf_plan_create(int lmax, const double* ab5, yasf_plan** out) {
 
 extern "C" int yasf_plan_destroy(yasf_plan* plan) {
   if (!plan) return YASF_OK;
-  cudaFree(plan->d_entry_ptr);
-  cudaFree(plan->d_term_n2);
-  cudaFree(plan->d_term_coef);
+  free_stream_layouts(plan);
   cudaFree(plan->d_leg);
   cudaFree(plan->d_pair_ptr);
   cudaFree(plan->d_pair_p);
@@ -542,8 +568,8 @@ extern "C" int yasf_plan_info(const yasf_plan* plan, int* nmax, long long* strea
                               long long* source_terms) {
   if (!plan) return YASF_ERR_INVALID_ARGUMENT;
   if (nmax) *nmax = plan->nmax;
-  if (stream_entries) *stream_entries = plan->total_entries;
-  if (source_terms) *source_terms = plan->total_terms;
+  if (stream_entries) *stream_entries = plan->stream[0].total_entries;
+  if (source_terms) *source_terms = plan->stream[0].total_terms;
   return YASF_OK;
 }
 

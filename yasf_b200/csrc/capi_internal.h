@@ -8,19 +8,29 @@
 
 #include "coupling.cuh"
 
-struct yasf_plan {
-  int lmax = 0;
-  int nmax = 0;
-  int device = -1;
+// One V-stream layout: how a source's stream is split into bundles, and the source-side term lists
+// (CSR over the stream's entries) that vbuild evaluates.
+struct yasf_stream_layout {
   int n_bundles = 0;
   int bundle_begin[8] = {0};
   int bundle_len[8] = {0};
   int total_entries = 0;          // per source, all bundles (padded)
   long long total_terms = 0;
-  // device arrays
   int* d_entry_ptr = nullptr;
   int* d_term_n2 = nullptr;
   double2* d_term_coef = nullptr;
+  bool owns = true;               // false: the device arrays belong to the other layout
+};
+
+struct yasf_plan {
+  int lmax = 0;
+  int nmax = 0;
+  int device = -1;
+  // [0]: the float64 kernels (and the regular-Bessel C_sca kernel), [1]: the complex64 kernel;
+  // the same arrays when both use the same bundle count
+  yasf_stream_layout stream[2];
+  const yasf_stream_layout& layout(int precision) const { return stream[precision == YASF_C64 ? 1 : 0]; }
+  // device arrays
   yasf::LegendreTables* d_leg = nullptr;
   // nonzero (n1, n2, p) terms for explicit block assembly, CSR over (n1, n2)
   int* d_pair_ptr = nullptr;      // [nmax*nmax + 1]

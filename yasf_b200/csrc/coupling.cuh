@@ -208,14 +208,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 // `issued` (thread 0) the copies issued into each, both carried across calls, so a persistent
 // block can process many work items with the same barriers. Returns false when a stage wait ran
 // out (the error word is set, the copies in flight are drained, the block must stop).
-template <int L, int BID, typename Real, bool REGULAR>
+template <int L, int NB, int BID, typename Real, bool REGULAR>
 __device__ __forceinline__ bool contract_body(const ContractArgs& a, int tile, int chunk, char* smem,
                                               unsigned long long* bars, unsigned (&uses)[2],
                                               unsigned (&issued)[2]) {
   using C = typename Cplx<Real>::T;
   using VE = typename VEntry<Real>::T;
   constexpr bool F64 = sizeof(Real) == 8;
-  constexpr BundleInfo bi = make_bundle(L, BID);
+  constexpr BundleInfo bi = make_bundle(L, BID, NB);
   constexpr int NR = bi.rows;
   constexpr int PMAX = 2 * L;
 
@@ -451,28 +451,35 @@ __device__ __forceinline__ bool contract_body(const ContractArgs& a, int tile, i
 
 #include "coupling_c64.cuh"
 
-// Receivers per thread of the contraction: two for the complex64 (Hankel) kernel, else one.
+// Receivers per thread of the contraction: kC64Receivers for the complex64 (Hankel) kernel, else one.
 template <typename Real, bool REGULAR>
 __host__ __device__ constexpr int receivers_per_thread() {
   return (sizeof(Real) == 4 && !REGULAR) ? kC64Receivers : 1;
 }
 
-template <int L, typename Real, bool REGULAR, int B>
+// Bundles of the stream layout a kernel reads: the complex64 (Hankel) kernel has its own.
+template <typename Real, bool REGULAR>
+__host__ __device__ constexpr bool c64_layout() {
+  return sizeof(Real) == 4 && !REGULAR;
+}
+
+// Bundle b of NB (B counts down from NB to 0 through the recursion).
+template <int L, typename Real, bool REGULAR, int NB, int B>
 struct BundleDispatch {
   __device__ static __forceinline__ bool run(const ContractArgs& a, int b, int tile, int chunk,
                                              char* smem, unsigned long long* bars,
                                              unsigned (&uses)[2], unsigned (&issued)[2]) {
     if (b == B - 1) {
       if constexpr (sizeof(Real) == 4 && !REGULAR)
-        return contract_body_c64<L, B - 1>(a, tile, chunk, smem, bars, uses, issued);
+        return contract_body_c64<L, NB, B - 1>(a, tile, chunk, smem, bars, uses, issued);
       else
-        return contract_body<L, B - 1, Real, REGULAR>(a, tile, chunk, smem, bars, uses, issued);
+        return contract_body<L, NB, B - 1, Real, REGULAR>(a, tile, chunk, smem, bars, uses, issued);
     }
-    return BundleDispatch<L, Real, REGULAR, B - 1>::run(a, b, tile, chunk, smem, bars, uses, issued);
+    return BundleDispatch<L, Real, REGULAR, NB, B - 1>::run(a, b, tile, chunk, smem, bars, uses, issued);
   }
 };
-template <int L, typename Real, bool REGULAR>
-struct BundleDispatch<L, Real, REGULAR, 0> {
+template <int L, typename Real, bool REGULAR, int NB>
+struct BundleDispatch<L, Real, REGULAR, NB, 0> {
   __device__ static __forceinline__ bool run(const ContractArgs&, int, int, int, char*,
                                              unsigned long long*, unsigned (&)[2], unsigned (&)[2]) {
     return true;
@@ -496,8 +503,9 @@ __global__ void __launch_bounds__(128) contract_kernel(ContractArgs a) {
   __shared__ __align__(8) unsigned long long bars[2];
   stage_barriers_init(bars);
   unsigned uses[2] = {0u, 0u}, issued[2] = {0u, 0u};
-  (void)BundleDispatch<L, Real, REGULAR, num_bundles(L)>::run(a, blockIdx.z, blockIdx.x, blockIdx.y, smem, bars,
-                                                              uses, issued);
+  constexpr int NB = num_bundles(L, c64_layout<Real, REGULAR>());
+  (void)BundleDispatch<L, Real, REGULAR, NB, NB>::run(a, blockIdx.z, blockIdx.x, blockIdx.y, smem, bars, uses,
+                                                      issued);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -579,7 +587,8 @@ __global__ void __launch_bounds__(128) grouped_contract_kernel(GroupedContractAr
     a.pos = col.pos;
     a.v = col.v;
     a.partial = col.partial;
-    if (!BundleDispatch<L, Real, false, num_bundles(L)>::run(a, bundle, tile, chunk, smem, bars, uses, issued))
+    constexpr int NB = num_bundles(L, c64_layout<Real, false>());
+    if (!BundleDispatch<L, Real, false, NB, NB>::run(a, bundle, tile, chunk, smem, bars, uses, issued))
       break;  // a stage wait ran out: this block stops (the error word is set)
   }
 }
@@ -588,12 +597,13 @@ template <int L>
 cudaError_t launch_grouped_contract(int precision, const GroupedContractArgs& g, int blocks,
                                     cudaStream_t stream);
 
-template <int L>
+// Longest padded bundle stream (entries per source) of the layout with NB bundles.
+template <int L, int NB>
 constexpr int max_bundle_stream(int b = 0) {
-  return b >= num_bundles(L) ? 0
-                             : (padded_stream_length(L, b) > max_bundle_stream<L>(b + 1)
-                                    ? padded_stream_length(L, b)
-                                    : max_bundle_stream<L>(b + 1));
+  return b >= NB ? 0
+                 : (padded_stream_length(L, b, NB) > max_bundle_stream<L, NB>(b + 1)
+                        ? padded_stream_length(L, b, NB)
+                        : max_bundle_stream<L, NB>(b + 1));
 }
 
 // ---------------------------------------------------------------------------------------------

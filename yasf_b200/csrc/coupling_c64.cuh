@@ -24,13 +24,13 @@
 #endif
 constexpr int kC64Receivers = YASF_C64_RECEIVERS;  // receivers per thread of the complex64 contraction
 
-template <int L, int BID>
+template <int L, int NB, int BID>
 __device__ __forceinline__ bool contract_body_c64(const ContractArgs& a, int tile, int chunk, char* smem,
                                                   unsigned long long* bars, unsigned (&uses)[2],
                                                   unsigned (&issued)[2]) {
   using VE = float4;
   constexpr int Q = kC64Receivers;
-  constexpr BundleInfo bi = make_bundle(L, BID);
+  constexpr BundleInfo bi = make_bundle(L, BID, NB);
   constexpr int NR = bi.rows;
   constexpr int PMAX = 2 * L;
 

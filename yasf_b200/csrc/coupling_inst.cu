@@ -13,9 +13,11 @@ cudaError_t launch_contract<YASF_INST_L>(int precision, bool regular, const Cont
                                           int tiles, int chunks, int threads,
                                           cudaStream_t stream) {
   constexpr int L = YASF_INST_L;
-  const dim3 grid(tiles, chunks, num_bundles(L));
-  const size_t stage64 = 2 * (size_t)max_bundle_stream<L>() * sizeof(double2);
-  const size_t stage32 = 2 * (size_t)max_bundle_stream<L>() * sizeof(float4);
+  constexpr int NB64 = num_bundles(L, false), NB32 = num_bundles(L, true);
+  const bool c64 = precision == YASF_C64 && !regular;
+  const dim3 grid(tiles, chunks, c64 ? NB32 : NB64);
+  const size_t stage64 = 2 * (size_t)max_bundle_stream<L, NB64>() * sizeof(double2);
+  const size_t stage32 = 2 * (size_t)max_bundle_stream<L, NB32>() * sizeof(float4);
   cudaError_t e;
   if (regular) {
     e = cudaFuncSetAttribute(contract_kernel<L, double, true>,
@@ -40,7 +42,9 @@ template <>
 cudaError_t launch_grouped_contract<YASF_INST_L>(int precision, const GroupedContractArgs& g, int blocks,
                                                  cudaStream_t stream) {
   constexpr int L = YASF_INST_L;
-  const size_t stage = 2 * (size_t)max_bundle_stream<L>() * (precision == YASF_C64 ? sizeof(float4) : sizeof(double2));
+  const size_t stage = precision == YASF_C64
+                           ? 2 * (size_t)max_bundle_stream<L, num_bundles(L, true)>() * sizeof(float4)
+                           : 2 * (size_t)max_bundle_stream<L, num_bundles(L, false)>() * sizeof(double2);
   cudaError_t e;
   if (precision == YASF_C64) {
     e = cudaFuncSetAttribute(grouped_contract_kernel<L, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -59,7 +63,9 @@ cudaError_t launch_grouped_contract<YASF_INST_L>(int precision, const GroupedCon
 template <>
 int contract_resident_blocks<YASF_INST_L>(int precision, int threads) {
   constexpr int L = YASF_INST_L;
-  const size_t stage = 2 * (size_t)max_bundle_stream<L>() * (precision == YASF_C64 ? sizeof(float4) : sizeof(double2));
+  const size_t stage = precision == YASF_C64
+                           ? 2 * (size_t)max_bundle_stream<L, num_bundles(L, true)>() * sizeof(float4)
+                           : 2 * (size_t)max_bundle_stream<L, num_bundles(L, false)>() * sizeof(double2);
   int blocks = 0;
   cudaError_t e;
   if (precision == YASF_C64) {

@@ -809,11 +809,11 @@ GroupWs group_layout(const yasf_plan* plan, int P, const yasf_problem* pr, int m
     L.tiles32.push_back((N + kC64Receivers * kGroupThreads - 1) / (kC64Receivers * kGroupThreads));
     L.src_pre.push_back(L.src_pre.back() + N);
     L.elem_pre.push_back(L.elem_pre.back() + nc);
-    L.ipre64.push_back(L.ipre64.back() + (long long)L.tiles64.back() * ch * plan->n_bundles);
-    L.ipre32.push_back(L.ipre32.back() + (long long)L.tiles32.back() * ch * plan->n_bundles);
+    L.ipre64.push_back(L.ipre64.back() + (long long)L.tiles64.back() * ch * plan->stream[0].n_bundles);
+    L.ipre32.push_back(L.ipre32.back() + (long long)L.tiles32.back() * ch * plan->stream[1].n_bundles);
     L.vsoff.push_back(vs);
     L.psoff.push_back(ps);
-    vs += up((size_t)N * plan->total_entries * 16);
+    vs += up((size_t)N * std::max(plan->stream[0].total_entries, plan->stream[1].total_entries) * 16);
     ps += up((size_t)ch * nc * 16);
   }
   L.total_src = L.src_pre.back();
@@ -989,16 +989,17 @@ extern "C" int yasf_grouped_solve(const yasf_plan* plan, int n_problems, const y
     va.n_cols = C;
     va.total_src = L.total_src;
     va.nmax = nmax;
-    va.total_entries = plan->total_entries;
-    va.n_bundles = plan->n_bundles;
+    const yasf_stream_layout& sl = plan->layout(prec);
+    va.total_entries = sl.total_entries;
+    va.n_bundles = sl.n_bundles;
     for (int b = 0; b < 8; ++b) {
-      va.bundle_begin[b] = plan->bundle_begin[b];
-      va.bundle_len[b] = plan->bundle_len[b];
+      va.bundle_begin[b] = sl.bundle_begin[b];
+      va.bundle_len[b] = sl.bundle_len[b];
     }
-    va.entry_ptr = plan->d_entry_ptr;
-    va.term_n2 = plan->d_term_n2;
-    va.term_coef = plan->d_term_coef;
-    const dim3 vgrid((plan->total_entries + 255) / 256, (unsigned)std::min<long long>(L.total_src, 65535));
+    va.entry_ptr = sl.d_entry_ptr;
+    va.term_n2 = sl.d_term_n2;
+    va.term_coef = sl.d_term_coef;
+    const dim3 vgrid((sl.total_entries + 255) / 256, (unsigned)std::min<long long>(L.total_src, 65535));
     if (prec == YASF_C64) YASF_COUNTED(grouped_vbuild_kernel<float><<<vgrid, 256, 0, s>>>(va));
     else YASF_COUNTED(grouped_vbuild_kernel<double><<<vgrid, 256, 0, s>>>(va));
     YASF_CUDA_TRY(cudaGetLastError());
@@ -1011,10 +1012,10 @@ extern "C" int yasf_grouped_solve(const yasf_plan* plan, int n_problems, const y
     ga.counter = d_counter;
     ga.leg = plan->d_leg;
     ga.nmax = nmax;
-    ga.n_bundles = plan->n_bundles;
+    ga.n_bundles = sl.n_bundles;
     for (int b = 0; b < 8; ++b) {
-      ga.bundle_begin[b] = plan->bundle_begin[b];
-      ga.bundle_len[b] = plan->bundle_len[b];
+      ga.bundle_begin[b] = sl.bundle_begin[b];
+      ga.bundle_len[b] = sl.bundle_len[b];
     }
     ga.err = d_err;
     ga.poll_limit = stall_hook().contract_polls;

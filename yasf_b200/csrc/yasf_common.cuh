@@ -48,12 +48,22 @@ __host__ __device__ constexpr int valid_rows(int L, int m1, int p) {
 // Receiving orders m1 are split into bundles so that one thread keeps the accumulators of a
 // whole bundle in registers while the pair-side factors (Hankel, Legendre, azimuthal phase)
 // are generated once per bundle. Bundles are a snake deal of m1 sorted by |m1|, which
-// balances both the row count and the stream length.
-#ifndef YASF_BUNDLES_L6
-#define YASF_BUNDLES_L6 4
+// balances both the row count and the stream length. The float64 and complex64 kernels may use
+// different counts (each its own stream layout): at lmax 6 on B200 the float64 contraction runs
+// fastest with 3 bundles of 32 rows (22.3 ms per C2 matvec against 25.7 ms with 4), the complex64
+// one with 4 of 24 rows (15.3 ms against 18.9 ms with 3, whose accumulators cost occupancy).
+#ifndef YASF_BUNDLES_L6_F64
+#define YASF_BUNDLES_L6_F64 3
 #endif
-__host__ __device__ constexpr int num_bundles(int L) {
-  return L <= 3 ? 1 : (L == 4 ? 2 : (L == 5 ? 3 : (L == 6 ? YASF_BUNDLES_L6 : (L == 7 ? 6 : 8))));
+#ifndef YASF_BUNDLES_L6_C64
+#define YASF_BUNDLES_L6_C64 4
+#endif
+__host__ __device__ constexpr int num_bundles(int L, bool c64) {
+  return L <= 3 ? 1
+                : (L == 4 ? 2
+                          : (L == 5 ? 3
+                                    : (L == 6 ? (c64 ? YASF_BUNDLES_L6_C64 : YASF_BUNDLES_L6_F64)
+                                              : (L == 7 ? 6 : 8))));
 }
 
 // The i-th m1 in the order 0, 1, -1, 2, -2, ...
@@ -73,11 +83,11 @@ struct BundleInfo {
   int rows;                           // total rows (accumulators) of the bundle
 };
 
-__host__ __device__ constexpr BundleInfo make_bundle(int L, int b) {
+// Bundle b of B at lmax L.
+__host__ __device__ constexpr BundleInfo make_bundle(int L, int b, int B) {
   BundleInfo info{};
   info.count = 0;
   info.rows = 0;
-  const int B = num_bundles(L);
   for (int i = 0; i < 2 * L + 1; ++i) {
     if (bundle_of_index(i, B) == b) {
       const int m1 = m_in_abs_order(i);
@@ -95,8 +105,8 @@ __host__ __device__ constexpr BundleInfo make_bundle(int L, int b) {
 //     for m1 in bundle order with |m1 + sign*d| <= L, for r < valid_rows(m1, p).
 // Each entry (tau1,l1,m1; p; m2=m1+sign*d) holds
 //   V = sum_{tau2,l2} A[(tau1,l1,m1),(tau2,l2,m2),p] * x_source[(tau2,l2,m2)].
-__host__ __device__ constexpr int bundle_stream_length(int L, int b) {
-  const BundleInfo bi = make_bundle(L, b);
+__host__ __device__ constexpr int bundle_stream_length(int L, int b, int B) {
+  const BundleInfo bi = make_bundle(L, b, B);
   int len = 0;
   for (int d = 0; d <= 2 * L; ++d)
     for (int p = d; p <= 2 * L; ++p)
@@ -112,8 +122,8 @@ __host__ __device__ constexpr int bundle_stream_length(int L, int b) {
 }
 
 // Streams of consecutive sources start on 32-byte boundaries (even entry counts).
-__host__ __device__ constexpr int padded_stream_length(int L, int b) {
-  return (bundle_stream_length(L, b) + 1) & ~1;
+__host__ __device__ constexpr int padded_stream_length(int L, int b, int B) {
+  return (bundle_stream_length(L, b, B) + 1) & ~1;
 }
 
 }  // namespace yasf
