@@ -272,15 +272,21 @@ int yasf_precond_assemble(yasf_precond* pc, const double* positions, double k_me
                           const double* tmat, void* stream);
 /* Device pointer and order of block `block`: row-major (dim, dim) complex128, dim = n_B*nmax,
  * rows/columns in the block's particle order, particle-major inside. Available from assemble until
- * a finalize that releases the complex128 factors (YASF_ERR_NOT_PREPARED afterwards). */
+ * a complex64 factorisation (or a finalize) releases the complex128 blocks (YASF_ERR_NOT_PREPARED
+ * afterwards). */
 int yasf_precond_block(const yasf_precond* pc, int block, double** matrix, int* dim);
 /* Replaces the block LU of prepare() (yasfpy/preconditioner.py:445-468, scipy.linalg.lu on complex64
- * blocks): every block factored in place in complex128, P_B M_B = L_B U_B, by a right-looking tile LU
- * (64 x 64 tiles, partial pivoting inside each diagonal tile, so P_B permutes rows only within each
- * tile row); all blocks of the preconditioner in one sequence of launches. Asynchronous. */
+ * blocks): every block factored in place, P_B M_B = L_B U_B, by a right-looking tile LU (64 x 64
+ * tiles, partial pivoting inside each diagonal tile, so P_B permutes rows only within each tile
+ * row); all blocks of the preconditioner in one sequence of launches. By default in complex64, as
+ * the reference factors (the complex128 blocks are converted and released first; diagonal-tile
+ * steps in float64 arithmetic, trailing updates in FP32); in complex128 when
+ * yasf_precond_keep_float64(pc, 1) was called before. Synchronises the stream in complex64 mode
+ * (the release), else asynchronous. */
 int yasf_precond_factor(yasf_precond* pc, void* stream);
-/* Whether finalize keeps the complex128 factors beside the complex64 copy (default 0: released,
- * halving the resident bytes; YASF_C128 applies then also stream the complex64 factors). */
+/* Call before factor: 1 factors in complex128 and keeps those factors beside the complex64 copy
+ * after finalize (YASF_C128 applies stream them); 0 (default) factors in complex64, halving the
+ * resident bytes, and YASF_C128 applies stream the complex64 factors. */
 int yasf_precond_keep_float64(yasf_precond* pc, int keep);
 /* Call after factor (or after the caller's in-place inversion). Makes the complex64 copy and, after
  * factor, the inverses of the diagonal tiles of L and U; YASF_ERR_NOT_FINITE for a zero pivot.

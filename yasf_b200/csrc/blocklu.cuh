@@ -67,10 +67,21 @@ __device__ __forceinline__ int lu_block_of(const int* pre, int n_blocks, int ite
 
 __device__ __forceinline__ int lu_tiles(int dim) { return (dim + kLuT - 1) / kLuT; }
 
+// Matrix storage of a factorisation: complex128 (double2) or complex64 (float2). The diagonal,
+// panel and inverse steps compute in float64 in shared memory whatever the storage.
+__device__ __forceinline__ double2 lu_load(const double2& v) { return v; }
+__device__ __forceinline__ double2 lu_load(const float2& v) { return make_double2(v.x, v.y); }
+template <typename T> __device__ __forceinline__ T lu_cast(double2 v);
+template <> __device__ __forceinline__ double2 lu_cast<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ float2 lu_cast<float2>(double2 v) {
+  return make_float2((float)v.x, (float)v.y);
+}
+
 // ---- step k, part 1: the diagonal tile, partial pivoting inside it -----------------------------
 // piv[row0 + k*64 + r] = local source row (0..63) of row r after the interchanges.
-__global__ void __launch_bounds__(256) lu_diag_kernel(LuGeom g, const int* pre, int k, double2* mat,
-                                                      int* piv, int* err) {
+template <typename T>
+__global__ void __launch_bounds__(256) lu_diag_kernel(LuGeom g, const int* pre, int k, T* mat, int* piv,
+                                                      int* err) {
   extern __shared__ double2 lu_smem[];
   double2* t = lu_smem;  // [64][kLuS]
   __shared__ int perm[kLuT];
@@ -80,11 +91,11 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(LuGeom g, const int* pre, 
   const int dim = g.dim[b];
   const int k0 = k * kLuT;
   const int v = min(kLuT, dim - k0);
-  double2* A = mat + g.mat_off[b];
+  T* A = mat + g.mat_off[b];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
     const int r = e >> 6, c = e & 63;
-    t[r * kLuS + c] = (r < v && c < v) ? A[(size_t)(k0 + r) * dim + k0 + c]
+    t[r * kLuS + c] = (r < v && c < v) ? lu_load(A[(size_t)(k0 + r) * dim + k0 + c])
                                        : make_double2(r == c ? 1.0 : 0.0, 0.0);
   }
   if (tid < kLuT) perm[tid] = tid;
@@ -140,7 +151,7 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(LuGeom g, const int* pre, 
   __syncthreads();
   for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
     const int r = e >> 6, c = e & 63;
-    if (r < v && c < v) A[(size_t)(k0 + r) * dim + k0 + c] = t[r * kLuS + c];
+    if (r < v && c < v) A[(size_t)(k0 + r) * dim + k0 + c] = lu_cast<T>(t[r * kLuS + c]);
   }
   if (tid < v) piv[g.row0[b] + k0 + tid] = perm[tid];
   if (tid == 0 && singular) atomicExch(err, 1);
@@ -148,8 +159,8 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(LuGeom g, const int* pre, 
 
 // ---- step k, part 2: tile row k (interchanges; U_kj = L_kk^{-1} P A_kj) and tile column k
 // (L_ik = A_ik U_kk^{-1}) --------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre, int k, double2* mat,
-                                                       const int* piv) {
+template <typename T>
+__global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre, int k, T* mat, const int* piv) {
   extern __shared__ double2 lu_smem[];
   double2* X = lu_smem;               // [64][kLuS] the tile being solved
   double2* D = lu_smem + kLuT * kLuS;  // [64][kLuS] the factored diagonal tile
@@ -159,7 +170,7 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre,
   const int nt = lu_tiles(dim);
   const int k0 = k * kLuT;
   const int vk = min(kLuT, dim - k0);
-  double2* A = mat + g.mat_off[b];
+  T* A = mat + g.mat_off[b];
   const int tid = threadIdx.x;
   const int nrow = nt - 1;
   if (item < nrow) {
@@ -169,12 +180,12 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre,
     const int* p = piv + g.row0[b] + k0;
     for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
       const int r = e >> 6, c = e & 63;
-      X[r * kLuS + c] = (r < vk && c < vj) ? A[(size_t)(k0 + p[r]) * dim + j0 + c] : make_double2(0.0, 0.0);
+      X[r * kLuS + c] = (r < vk && c < vj) ? lu_load(A[(size_t)(k0 + p[r]) * dim + j0 + c]) : make_double2(0.0, 0.0);
     }
     if (j > k) {
       for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
         const int r = e >> 6, c = e & 63;
-        D[r * kLuS + c] = (r < vk && c < vk) ? A[(size_t)(k0 + r) * dim + k0 + c] : make_double2(0.0, 0.0);
+        D[r * kLuS + c] = (r < vk && c < vk) ? lu_load(A[(size_t)(k0 + r) * dim + k0 + c]) : make_double2(0.0, 0.0);
       }
       for (int c = 0; c < vk; ++c) {
         __syncthreads();
@@ -188,7 +199,7 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre,
     __syncthreads();
     for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
       const int r = e >> 6, c = e & 63;
-      if (r < vk && c < vj) A[(size_t)(k0 + r) * dim + j0 + c] = X[r * kLuS + c];
+      if (r < vk && c < vj) A[(size_t)(k0 + r) * dim + j0 + c] = lu_cast<T>(X[r * kLuS + c]);
     }
   } else {
     // tile (i, k), i > k: X U_kk = A_ik
@@ -196,8 +207,8 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre,
     const int i0 = i * kLuT, vi = min(kLuT, dim - i0);
     for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
       const int r = e >> 6, c = e & 63;
-      X[r * kLuS + c] = (r < vi && c < vk) ? A[(size_t)(i0 + r) * dim + k0 + c] : make_double2(0.0, 0.0);
-      D[r * kLuS + c] = (r < vk && c < vk) ? A[(size_t)(k0 + r) * dim + k0 + c] : make_double2(0.0, 0.0);
+      X[r * kLuS + c] = (r < vi && c < vk) ? lu_load(A[(size_t)(i0 + r) * dim + k0 + c]) : make_double2(0.0, 0.0);
+      D[r * kLuS + c] = (r < vk && c < vk) ? lu_load(A[(size_t)(k0 + r) * dim + k0 + c]) : make_double2(0.0, 0.0);
     }
     for (int c = 0; c < vk; ++c) {
       __syncthreads();
@@ -214,7 +225,7 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre,
     __syncthreads();
     for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
       const int r = e >> 6, c = e & 63;
-      if (r < vi && c < vk) A[(size_t)(i0 + r) * dim + k0 + c] = X[r * kLuS + c];
+      if (r < vi && c < vk) A[(size_t)(i0 + r) * dim + k0 + c] = lu_cast<T>(X[r * kLuS + c]);
     }
   }
 }
@@ -286,11 +297,79 @@ __global__ void __launch_bounds__(256, 2) lu_update_kernel(LuGeom g, const int* 
   }
 }
 
+// Complex64 storage: the same update in FP32, as packed FMAs (FFMA2). The staged operands are laid
+// out as the packed instructions consume them: Ls[kk][row] = (l_re, l_re, -l_im, l_im) and
+// Us[kk][col] = (u_re, u_im, u_im, u_re), so each complex multiply-add is two FFMA2 fed by two
+// 16-byte shared loads shared across the thread's 4 x 4 outputs:
+//   (acc_re, acc_im) += (l_re, l_re) * (u_re, u_im) + (-l_im, l_im) * (u_im, u_re).
+constexpr size_t kLuUpdateSmem32 = 2 * (size_t)kLuKc * kLuS * sizeof(float4);
+__global__ void __launch_bounds__(256, 2) lu_update32_kernel(LuGeom g, const int* pre, int k, float2* mat) {
+  extern __shared__ float4 lu_smem32[];
+  float4(*Ls)[kLuS] = reinterpret_cast<float4(*)[kLuS]>(lu_smem32);
+  float4(*Us)[kLuS] = reinterpret_cast<float4(*)[kLuS]>(lu_smem32 + kLuKc * kLuS);
+  const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
+  const int item = blockIdx.x - pre[b];
+  const int dim = g.dim[b];
+  const int nt = lu_tiles(dim);
+  const int nc = nt - k - 1;
+  const int i = k + 1 + item / nc, j = k + 1 + item % nc;
+  const int k0 = k * kLuT, i0 = i * kLuT, j0 = j * kLuT;
+  const int vk = min(kLuT, dim - k0), vi = min(kLuT, dim - i0), vj = min(kLuT, dim - j0);
+  float2* A = mat + g.mat_off[b];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  float2 acc[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[p][q] = make_float2(0.f, 0.f);
+  for (int kc = 0; kc < vk; kc += kLuKc) {
+    __syncthreads();
+    for (int e = tid; e < kLuT * kLuKc; e += blockDim.x) {
+      const int r = e / kLuKc, kk = e % kLuKc;
+      const float2 l = (r < vi && kc + kk < vk) ? A[(size_t)(i0 + r) * dim + k0 + kc + kk] : make_float2(0.f, 0.f);
+      Ls[kk][r] = make_float4(l.x, l.x, -l.y, l.y);
+      const int kk2 = e / kLuT, c = e % kLuT;
+      const float2 u = (kc + kk2 < vk && c < vj) ? A[(size_t)(k0 + kc + kk2) * dim + j0 + c] : make_float2(0.f, 0.f);
+      Us[kk2][c] = make_float4(u.x, u.y, u.y, u.x);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < kLuKc; ++kk) {
+      float4 l[4], u[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) l[p] = Ls[kk][ty + 16 * p];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) u[q] = Us[kk][tx + 16 * q];
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[p][q] = __ffma2_rn(make_float2(l[p].x, l[p].y), make_float2(u[q].x, u[q].y), acc[p][q]);
+          acc[p][q] = __ffma2_rn(make_float2(l[p].z, l[p].w), make_float2(u[q].z, u[q].w), acc[p][q]);
+        }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int r = ty + 16 * p;
+    if (r >= vi) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = tx + 16 * q;
+      if (c >= vj) continue;
+      float2* a = A + (size_t)(i0 + r) * dim + j0 + c;
+      const float2 o = *a;
+      *a = make_float2(o.x - acc[p][q].x, o.y - acc[p][q].y);
+    }
+  }
+}
+
 // ---- finalize: complex64 factors and the inverses of the diagonal tiles ------------------------
 // dinv[(tile0[b] + t) * 2 + 0] = L_tt^{-1} (unit lower), [.. + 1] = U_tt^{-1}, each 64 x 64
 // row-major complex64 (identity in the padded part); dinv64 (may be null) the same in complex128.
-__global__ void __launch_bounds__(256) lu_diag_inverse_kernel(LuGeom g, const int* pre, const double2* mat,
-                                                              float2* dinv, double2* dinv64, int* err) {
+template <typename T>
+__global__ void __launch_bounds__(256) lu_diag_inverse_kernel(LuGeom g, const int* pre, const T* mat, float2* dinv,
+                                                              double2* dinv64, int* err) {
   extern __shared__ double2 lu_smem[];
   double2* D = lu_smem;                // [64][kLuS] factored diagonal tile
   double2* X = lu_smem + kLuT * kLuS;  // [64][kLuS] inverse under construction
@@ -298,13 +377,14 @@ __global__ void __launch_bounds__(256) lu_diag_inverse_kernel(LuGeom g, const in
   const int t = blockIdx.x - pre[b];
   const int dim = g.dim[b];
   const int t0 = t * kLuT, v = min(kLuT, dim - t0);
-  const double2* A = mat + g.mat_off[b];
+  const T* A = mat + g.mat_off[b];
   const int tid = threadIdx.x;
   __shared__ int singular;
   if (tid == 0) singular = 0;
   for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
     const int r = e >> 6, c = e & 63;
-    D[r * kLuS + c] = (r < v && c < v) ? A[(size_t)(t0 + r) * dim + t0 + c] : make_double2(r == c ? 1.0 : 0.0, 0.0);
+    D[r * kLuS + c] =
+        (r < v && c < v) ? lu_load(A[(size_t)(t0 + r) * dim + t0 + c]) : make_double2(r == c ? 1.0 : 0.0, 0.0);
     X[r * kLuS + c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
   }
   // L X = I (unit lower): row c of X is final before rows below use it

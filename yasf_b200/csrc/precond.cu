@@ -37,7 +37,8 @@ struct yasf_precond {
   // complex64 factors' diagonal-tile inverses (and complex128 ones when the float64 factors are
   // kept), the sweep buffer of the apply
   bool factored = false;   // blocks hold LU factors (else: the caller's inverses)
-  bool keep_f64 = false;   // finalize keeps the complex128 factors (yasf_precond_keep_float64)
+  bool keep_f64 = false;   // factor in complex128 and keep those factors (yasf_precond_keep_float64)
+  bool factored_c64 = false;  // the factorisation ran in complex64 (d_mat32, complex128 released)
   int lu_steps = 0;        // tiles of the largest block
   int n_tiles = 0;         // diagonal tiles of all blocks
   std::vector<int> pre_diag, pre_panel, pre_update, pre_sweep;  // [step][n_blocks + 1]
@@ -414,12 +415,20 @@ int lu_smem_attributes() {
   static int done = 0;
   if (done) return YASF_OK;
   const int one = (int)(yasf::kLuT * yasf::kLuS * sizeof(double2));
-  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
-  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * one));
-  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      2 * one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     2 * one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_inverse_kernel<double2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_inverse_kernel<float2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * one));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)yasf::kLuUpdateSmem));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_update32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)yasf::kLuUpdateSmem32));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_solve_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)yasf::lu_solve_smem<float2>()));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_solve_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -437,18 +446,38 @@ extern "C" int yasf_precond_factor(yasf_precond* pc, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const LuGeom g = lu_geom(pc);
   const int one = (int)(kLuT * kLuS * sizeof(double2));
+  const bool c64 = !pc->keep_f64;
+  if (c64) {  // the reference's precision: convert the blocks, release the complex128 copy
+    if (!pc->d_mat32) {
+      cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&pc->d_mat32), pc->mat_elems * sizeof(float2));
+      if (e != cudaSuccess) {
+        set_cuda_error(e);
+        pc->d_mat32 = nullptr;
+        return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
+      }
+    }
+    YASF_COUNTED(to_c64_kernel<<<2048, 256, 0, s>>>(pc->mat_elems, pc->d_mat, pc->d_mat32));
+    YASF_CUDA_TRY(cudaGetLastError());
+    YASF_CUDA_TRY(cudaStreamSynchronize(s));
+    YASF_CUDA_TRY(cudaFree(pc->d_mat));
+    pc->d_mat = nullptr;
+  }
   YASF_CUDA_TRY(cudaMemsetAsync(pc->d_err, 0, sizeof(int), s));
   for (int k = 0; k < pc->lu_steps; ++k) {
     int n = 0;
     const int* pre = lu_pre(pc, 0, k, &n);
-    if (n) YASF_COUNTED(lu_diag_kernel<<<n, 256, one, s>>>(g, pre, k, pc->d_mat, pc->d_piv, pc->d_err));
+    if (n && c64) YASF_COUNTED(lu_diag_kernel<float2><<<n, 256, one, s>>>(g, pre, k, pc->d_mat32, pc->d_piv, pc->d_err));
+    else if (n) YASF_COUNTED(lu_diag_kernel<double2><<<n, 256, one, s>>>(g, pre, k, pc->d_mat, pc->d_piv, pc->d_err));
     pre = lu_pre(pc, 1, k, &n);
-    if (n) YASF_COUNTED(lu_panel_kernel<<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat, pc->d_piv));
+    if (n && c64) YASF_COUNTED(lu_panel_kernel<float2><<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat32, pc->d_piv));
+    else if (n) YASF_COUNTED(lu_panel_kernel<double2><<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat, pc->d_piv));
     pre = lu_pre(pc, 2, k, &n);
-    if (n) YASF_COUNTED(lu_update_kernel<<<n, 256, kLuUpdateSmem, s>>>(g, pre, k, pc->d_mat));
+    if (n && c64) YASF_COUNTED(lu_update32_kernel<<<n, 256, kLuUpdateSmem32, s>>>(g, pre, k, pc->d_mat32));
+    else if (n) YASF_COUNTED(lu_update_kernel<<<n, 256, kLuUpdateSmem, s>>>(g, pre, k, pc->d_mat));
     YASF_CUDA_TRY(cudaGetLastError());
   }
   pc->factored = true;
+  pc->factored_c64 = c64;
   pc->prepared = false;
   return YASF_OK;
 }
@@ -500,13 +529,14 @@ extern "C" int yasf_precond_assemble(yasf_precond* pc, const double* positions, 
   pc->assembled = true;
   pc->prepared = false;
   pc->factored = false;
+  pc->factored_c64 = false;
   return YASF_OK;
 }
 
 extern "C" int yasf_precond_block(const yasf_precond* pc, int block, double** matrix, int* dim) {
   if (!pc || !matrix || !dim || block < 0 || block >= pc->n_blocks) return YASF_ERR_INVALID_ARGUMENT;
   if (!pc->d_mat) {
-    set_error_text("the complex128 blocks were released by finalize");
+    set_error_text("the complex128 blocks were released (complex64 factorisation or finalize)");
     return YASF_ERR_NOT_PREPARED;
   }
   *matrix = reinterpret_cast<double*>(pc->d_mat + pc->mat_off[block]);
@@ -516,7 +546,11 @@ extern "C" int yasf_precond_block(const yasf_precond* pc, int block, double** ma
 
 extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
   if (!pc) return YASF_ERR_INVALID_ARGUMENT;
-  if (!pc->assembled || !pc->d_mat) return YASF_ERR_NOT_PREPARED;
+  if (!pc->assembled || (!pc->d_mat && !pc->factored_c64)) return YASF_ERR_NOT_PREPARED;
+  if (pc->factored_c64 && pc->keep_f64) {
+    set_error_text("keep_float64 must be set before factor: the blocks were factored in complex64");
+    return YASF_ERR_INVALID_ARGUMENT;
+  }
   if (int st = check_current_device(pc->plan->device)) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   auto alloc = [&](void** p, size_t bytes) -> int {
@@ -529,9 +563,11 @@ extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
     }
     return YASF_OK;
   };
-  if (int st = alloc(reinterpret_cast<void**>(&pc->d_mat32), pc->mat_elems * sizeof(float2))) return st;
-  YASF_COUNTED(to_c64_kernel<<<2048, 256, 0, s>>>(pc->mat_elems, pc->d_mat, pc->d_mat32));
-  YASF_CUDA_TRY(cudaGetLastError());
+  if (!pc->factored_c64) {  // the complex64 copy of the complex128 factors (or inverses)
+    if (int st = alloc(reinterpret_cast<void**>(&pc->d_mat32), pc->mat_elems * sizeof(float2))) return st;
+    YASF_COUNTED(to_c64_kernel<<<2048, 256, 0, s>>>(pc->mat_elems, pc->d_mat, pc->d_mat32));
+    YASF_CUDA_TRY(cudaGetLastError());
+  }
   if (pc->factored) {
     if (int st = lu_smem_attributes()) return st;
     const size_t tile_elems = (size_t)pc->n_tiles * 2 * kLuT * kLuT;
@@ -542,9 +578,12 @@ extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
     // every diagonal tile of every block: the sweep prefix of step 0 counts nt per block
     const int* pre = lu_pre(pc, 3, 0, &n);
     const int one = (int)(kLuT * kLuS * sizeof(double2));
-    YASF_COUNTED(lu_diag_inverse_kernel<<<n, 256, 2 * one, s>>>(lu_geom(pc), pre, pc->d_mat, pc->d_dinv,
-                                                                 pc->keep_f64 ? pc->d_dinv64 : nullptr,
-                                                                 pc->d_err));
+    if (pc->factored_c64)
+      YASF_COUNTED(lu_diag_inverse_kernel<float2><<<n, 256, 2 * one, s>>>(lu_geom(pc), pre, pc->d_mat32, pc->d_dinv,
+                                                                          nullptr, pc->d_err));
+    else
+      YASF_COUNTED(lu_diag_inverse_kernel<double2><<<n, 256, 2 * one, s>>>(
+          lu_geom(pc), pre, pc->d_mat, pc->d_dinv, pc->keep_f64 ? pc->d_dinv64 : nullptr, pc->d_err));
     YASF_CUDA_TRY(cudaGetLastError());
     int err = 0;
     YASF_CUDA_TRY(cudaMemcpyAsync(&err, pc->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -553,7 +592,7 @@ extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
       set_error_text("a block has a zero pivot (singular diagonal tile)");
       return YASF_ERR_NOT_FINITE;
     }
-    if (!pc->keep_f64) {  // the solves stream the complex64 factors only
+    if (!pc->keep_f64 && pc->d_mat) {  // the solves stream the complex64 factors only
       YASF_CUDA_TRY(cudaFree(pc->d_mat));
       pc->d_mat = nullptr;
     }

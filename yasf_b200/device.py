@@ -335,8 +335,9 @@ class DevicePreconditioner:
 
     def prepare(self, tmat: torch.Tensor, keep_float64: bool = False) -> dict:
         """Assemble, factor (the library's batched block LU) and finalize every block; returns the
-        seconds of each phase. keep_float64 keeps the complex128 factors beside the complex64 copy
-        the solves stream."""
+        seconds of each phase. The factorisation runs in complex64, as the reference's; with
+        keep_float64 it runs in complex128 and those factors stay beside the complex64 copy the
+        solves stream."""
         import time
 
         s = _stream_ptr()
@@ -344,10 +345,10 @@ class DevicePreconditioner:
         call("yasf_precond_assemble", self.handle, _ptr(self.dev.pos), self.dev.k, _ptr(tmat), s)
         torch.cuda.synchronize(self.dev.device)
         t1 = time.perf_counter()
+        call("yasf_precond_keep_float64", self.handle, 1 if keep_float64 else 0)
         call("yasf_precond_factor", self.handle, s)
         torch.cuda.synchronize(self.dev.device)
         t2 = time.perf_counter()
-        call("yasf_precond_keep_float64", self.handle, 1 if keep_float64 else 0)
         call("yasf_precond_finalize", self.handle, s)
         t3 = time.perf_counter()
         return {"assemble_s": t1 - t0, "factor_s": t2 - t1, "finalize_s": t3 - t2}
