@@ -52,6 +52,10 @@ __host__ __device__ constexpr int valid_rows(int L, int m1, int p) {
 // different counts (each its own stream layout): at lmax 6 on B200 the float64 contraction runs
 // fastest with 3 bundles of 32 rows (22.3 ms per C2 matvec against 25.7 ms with 4), the complex64
 // one with 4 of 24 rows (15.3 ms against 18.9 ms with 3, whose accumulators cost occupancy).
+// Unroll factor of the contraction's (+d, -d) loop: 2 (unrolled) or 1 (rolled, half the code).
+#ifndef YASF_SGN_UNROLL
+#define YASF_SGN_UNROLL 2
+#endif
 #ifndef YASF_BUNDLES_L6_F64
 #define YASF_BUNDLES_L6_F64 3
 #endif
