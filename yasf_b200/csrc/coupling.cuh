@@ -360,7 +360,7 @@ __device__ __forceinline__ bool contract_body(const ContractArgs& a, int tile, i
         const Real gpi = g0r * ph_i + g0i * ph_r;
         const Real gmr = g0r * ph_r + g0i * ph_i;
         const Real gmi = g0i * ph_r - g0r * ph_i;
-#pragma unroll YASF_SGN_UNROLL
+#pragma unroll kSgnUnroll
         for (int sgn = 0; sgn < 2; ++sgn) {
           if (sgn == 1 && d == 0) break;
           const Real gr = sgn == 0 ? gpr : gmr;

@@ -169,7 +169,7 @@ __device__ __forceinline__ bool contract_body_c64(const ContractArgs& a, int til
           gmr2[q] = make_float2(gmr, gmr);
           gmi2[q] = make_float2(gmi, gmi);
         }
-#pragma unroll YASF_SGN_UNROLL
+#pragma unroll kSgnUnroll
         for (int sgn = 0; sgn < 2; ++sgn) {
           if (sgn == 1 && d == 0) break;
 #pragma unroll

@@ -56,6 +56,7 @@ __host__ __device__ constexpr int valid_rows(int L, int m1, int p) {
 #ifndef YASF_SGN_UNROLL
 #define YASF_SGN_UNROLL 2
 #endif
+constexpr int kSgnUnroll = YASF_SGN_UNROLL;  // (pragma arguments are not macro-expanded)
 #ifndef YASF_BUNDLES_L6_F64
 #define YASF_BUNDLES_L6_F64 3
 #endif
