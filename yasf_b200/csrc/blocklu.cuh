@@ -299,11 +299,15 @@ __global__ void __launch_bounds__(256, 2) lu_update_kernel(LuGeom g, const int* 
 
 // Complex64 storage: the same update in FP32, as packed FMAs (FFMA2). The staged operands are laid
 // out as the packed instructions consume them: Ls[kk][row] = (l_re, l_re, -l_im, l_im) and
-// Us[kk][col] = (u_re, u_im, u_im, u_re), so each complex multiply-add is two FFMA2 fed by two
-// 16-byte shared loads shared across the thread's 4 x 4 outputs:
+// Us[kk][col] = (u_re, u_im, u_im, u_re), so each complex multiply-add is two FFMA2:
 //   (acc_re, acc_im) += (l_re, l_re) * (u_re, u_im) + (-l_im, l_im) * (u_im, u_re).
+// 128 threads, 8 x 4 outputs each (rows ty + 8p, columns tx + 16q): per inner index a warp issues
+// 12 shared loads (16 wavefronts) for 64 FFMA2, so the FP32 pipe, not shared memory, is the bound
+// (with 4 x 4 outputs it was 12 wavefronts per 32 FFMA2). Three CTAs per SM.
+constexpr int kLuUpd32Threads = 128;
 constexpr size_t kLuUpdateSmem32 = 2 * (size_t)kLuKc * kLuS * sizeof(float4);
-__global__ void __launch_bounds__(256, 2) lu_update32_kernel(LuGeom g, const int* pre, int k, float2* mat) {
+__global__ void __launch_bounds__(kLuUpd32Threads, 3) lu_update32_kernel(LuGeom g, const int* pre, int k,
+                                                                        float2* mat) {
   extern __shared__ float4 lu_smem32[];
   float4(*Ls)[kLuS] = reinterpret_cast<float4(*)[kLuS]>(lu_smem32);
   float4(*Us)[kLuS] = reinterpret_cast<float4(*)[kLuS]>(lu_smem32 + kLuKc * kLuS);
@@ -317,14 +321,14 @@ __global__ void __launch_bounds__(256, 2) lu_update32_kernel(LuGeom g, const int
   const int vk = min(kLuT, dim - k0), vi = min(kLuT, dim - i0), vj = min(kLuT, dim - j0);
   float2* A = mat + g.mat_off[b];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  float2 acc[4][4];
+  float2 acc[8][4];
 #pragma unroll
-  for (int p = 0; p < 4; ++p)
+  for (int p = 0; p < 8; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[p][q] = make_float2(0.f, 0.f);
   for (int kc = 0; kc < vk; kc += kLuKc) {
     __syncthreads();
-    for (int e = tid; e < kLuT * kLuKc; e += blockDim.x) {
+    for (int e = tid; e < kLuT * kLuKc; e += kLuUpd32Threads) {
       const int r = e / kLuKc, kk = e % kLuKc;
       const float2 l = (r < vi && kc + kk < vk) ? A[(size_t)(i0 + r) * dim + k0 + kc + kk] : make_float2(0.f, 0.f);
       Ls[kk][r] = make_float4(l.x, l.x, -l.y, l.y);
@@ -333,15 +337,15 @@ __global__ void __launch_bounds__(256, 2) lu_update32_kernel(LuGeom g, const int
       Us[kk2][c] = make_float4(u.x, u.y, u.y, u.x);
     }
     __syncthreads();
-#pragma unroll 4
+#pragma unroll 2
     for (int kk = 0; kk < kLuKc; ++kk) {
-      float4 l[4], u[4];
+      float4 l[8], u[4];
 #pragma unroll
-      for (int p = 0; p < 4; ++p) l[p] = Ls[kk][ty + 16 * p];
+      for (int p = 0; p < 8; ++p) l[p] = Ls[kk][ty + 8 * p];
 #pragma unroll
       for (int q = 0; q < 4; ++q) u[q] = Us[kk][tx + 16 * q];
 #pragma unroll
-      for (int p = 0; p < 4; ++p)
+      for (int p = 0; p < 8; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           acc[p][q] = __ffma2_rn(make_float2(l[p].x, l[p].y), make_float2(u[q].x, u[q].y), acc[p][q]);
@@ -350,8 +354,8 @@ __global__ void __launch_bounds__(256, 2) lu_update32_kernel(LuGeom g, const int
     }
   }
 #pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    const int r = ty + 16 * p;
+  for (int p = 0; p < 8; ++p) {
+    const int r = ty + 8 * p;
     if (r >= vi) continue;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -627,7 +631,7 @@ __device__ int lu_wait_rows(const int* done, int need, int* abort_word, unsigned
       atomicExch(abort_word, 1);
       return -1;
     }
-    __nanosleep(64);
+    if (spin >= 32) __nanosleep(64);  // the first polls spin: a row usually arrives within a few us
   }
 }
 
@@ -695,6 +699,19 @@ __global__ void __launch_bounds__(256, 2) lu_solve_kernel(LuSolveArgs a, const F
   double ax = 0.0, ay = 0.0;
   int c = 0;  // finished rows consumed
   while (ok && c < ndep) {
+    // The factor entries of the next dependency do not depend on z: they are loaded before the
+    // wait for its row, so a row that arrives late costs the chain no DRAM latency.
+    float4 pre[8];
+    if constexpr (sizeof(FT) == 8) {
+      const float4* M4 = reinterpret_cast<const float4*>(M);
+      const int j0 = (upper ? nt - 1 - c : c) * kLuT;
+      const int vj = min(kLuT, dim - j0);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int q = 2 * (part + 4 * k);
+        pre[k] = q < vj ? M4[(j0 + q) >> 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
     if (tid == 0) s_avail = lu_wait_rows(done, c, abort_word, a.wait_ns);
     __syncthreads();
     if (s_avail < 0) {
@@ -715,6 +732,10 @@ __global__ void __launch_bounds__(256, 2) lu_solve_kernel(LuSolveArgs a, const F
         // tiles' loads in flight. Block orders are even, so a pair never straddles the edge.
         const float4* M4 = reinterpret_cast<const float4*>(M);
         int u = 0;
+        if (c0 == c) {  // the prefetched tile
+          lu_pair_products(pre, zs, part, ax, ay);
+          u = 1;
+        }
 #pragma unroll 1
         for (; u + 1 < nb; u += 2) {
           const int ja = (upper ? nt - 1 - (c0 + u) : c0 + u) * kLuT;

@@ -472,7 +472,8 @@ extern "C" int yasf_precond_factor(yasf_precond* pc, void* stream) {
     if (n && c64) YASF_COUNTED(lu_panel_kernel<float2><<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat32, pc->d_piv));
     else if (n) YASF_COUNTED(lu_panel_kernel<double2><<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat, pc->d_piv));
     pre = lu_pre(pc, 2, k, &n);
-    if (n && c64) YASF_COUNTED(lu_update32_kernel<<<n, 256, kLuUpdateSmem32, s>>>(g, pre, k, pc->d_mat32));
+    if (n && c64)
+      YASF_COUNTED(lu_update32_kernel<<<n, kLuUpd32Threads, kLuUpdateSmem32, s>>>(g, pre, k, pc->d_mat32));
     else if (n) YASF_COUNTED(lu_update_kernel<<<n, 256, kLuUpdateSmem, s>>>(g, pre, k, pc->d_mat));
     YASF_CUDA_TRY(cudaGetLastError());
   }
