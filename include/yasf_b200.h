@@ -294,11 +294,14 @@ int yasf_precond_keep_float64(yasf_precond* pc, int keep);
 int yasf_precond_finalize(yasf_precond* pc, void* stream);
 /* Replaces BlockDiagonalPreconditioner.apply (yasfpy/preconditioner.py:177-219, the unit-lower and
  * upper triangular solves of :470-519): gather with the pivots, a forward sweep with L and a
- * backward sweep with U over tile rows (one launch per tile row, float64 arithmetic on the complex64
- * factors, or the complex128 ones when kept and precision is YASF_C128), scatter. The sweeps are
- * captured once per column count as a CUDA graph (on a private stream) and replayed on `stream`. The
- * first apply with more columns than any before allocates the preconditioner's sweep buffer; applies
- * of ONE preconditioner on different streams at the same time race on that buffer. */
+ * backward sweep with U over tile rows (float64 arithmetic on the complex64 factors, or the
+ * complex128 ones when kept and precision is YASF_C128), scatter. One column: both sweeps in one
+ * launch whose blocks take tile rows in dependency order and wait (bounded, 1 s; NaN output when a
+ * wait runs out) on per-block finished-row counters. Several columns: one launch per tile row,
+ * captured once per column count as a CUDA graph (on a private stream) and replayed on `stream`.
+ * The first apply with more columns than any before allocates the preconditioner's sweep buffer;
+ * applies of ONE preconditioner on different streams at the same time race on that buffer and on
+ * the one-column counters. */
 int yasf_precond_apply(const yasf_precond* pc, const double* x, double* y, int nrhs, long long ld,
                        int precision, void* stream);
 /* Device bytes held by the factors. */
