@@ -12,7 +12,8 @@
 //   within each tile row). Pivoting inside the diagonal tile rather than over the whole column
 //   keeps every step parallel over tiles; on the blocks of I - T W the growth factor stays near 1.
 //
-// Each step is three launches over all blocks that still have a tile k; host-built prefix sums
+// Each step is four launches over all blocks that still have a tile k (diagonal tile, its inverses,
+// tile row and column as products with those inverses, trailing update); host-built prefix sums
 // (one row per step) map a CTA index to (block, tile). Ragged edges (block order not a multiple of
 // 64) are padded with the identity in the diagonal tile and zeros elsewhere; padded entries are
 // never stored.
@@ -34,6 +35,7 @@ namespace yasf {
 
 constexpr int kLuT = 64;        // tile order
 constexpr int kLuS = kLuT + 1;  // shared-memory row stride (complex128), breaks bank conflicts
+constexpr int kLuKc = 32;       // inner-dimension chunk of the tile products
 
 struct LuGeom {
   const long long* mat_off;  // element offset of block b's matrix (row-major, order dim[b])
@@ -157,13 +159,18 @@ __global__ void __launch_bounds__(256) lu_diag_kernel(LuGeom g, const int* pre, 
   if (tid == 0 && singular) atomicExch(err, 1);
 }
 
-// ---- step k, part 2: tile row k (interchanges; U_kj = L_kk^{-1} P A_kj) and tile column k
-// (L_ik = A_ik U_kk^{-1}) --------------------------------------------------------------------------
+// ---- step k, part 2: tile row k and tile column k, as products with the inverses of the diagonal
+// tile (lu_diag_inverse_kernel, run right after the tile was factored; the apply uses the same
+// inverses): U_kj = L_kk^{-1} (P A_kj) for j > k, P A_kj for j < k (the interchanges applied to
+// the left part), and L_ik = A_ik U_kk^{-1} for i > k. Each tile is a 64 x 64 x 64 complex product
+// in float64 (256 threads, 4 x 4 outputs each, the inner dimension staged in two chunks of 32)
+// instead of 64 dependent elimination steps with a barrier each.
 template <typename T>
-__global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre, int k, T* mat, const int* piv) {
+__global__ void __launch_bounds__(256, 2) lu_panel_inv_kernel(LuGeom g, const int* pre, int k, T* mat,
+                                                             const int* piv, const double2* dinv64) {
   extern __shared__ double2 lu_smem[];
-  double2* X = lu_smem;               // [64][kLuS] the tile being solved
-  double2* D = lu_smem + kLuT * kLuS;  // [64][kLuS] the factored diagonal tile
+  double2(*Ls)[kLuS] = reinterpret_cast<double2(*)[kLuS]>(lu_smem);                 // Ls[kk][row] = Left[row][kc + kk]
+  double2(*Us)[kLuS] = reinterpret_cast<double2(*)[kLuS]>(lu_smem + kLuKc * kLuS);  // Us[kk][col] = Right[kc + kk][col]
   const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
   const int item = blockIdx.x - pre[b];
   const int dim = g.dim[b];
@@ -171,61 +178,80 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre,
   const int k0 = k * kLuT;
   const int vk = min(kLuT, dim - k0);
   T* A = mat + g.mat_off[b];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int nrow = nt - 1;
-  if (item < nrow) {
-    // tile (k, j), j != k: rows interchanged; for j > k then solved with the unit lower L_kk
-    const int j = item < k ? item : item + 1;
-    const int j0 = j * kLuT, vj = min(kLuT, dim - j0);
-    const int* p = piv + g.row0[b] + k0;
+  const bool row_tile = item < nrow;
+  const int j = row_tile ? (item < k ? item : item + 1) : k;  // output tile column
+  const int i = row_tile ? k : k + 1 + (item - nrow);         // output tile row
+  const int i0 = i * kLuT, j0 = j * kLuT;
+  const int vi = min(kLuT, dim - i0), vj = min(kLuT, dim - j0);
+  const int* p = piv + g.row0[b] + k0;
+  if (row_tile && j < k) {  // left of the diagonal: the interchanges only (rows of one tile row)
+    double2* X = lu_smem;   // [64][kLuS]
     for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
       const int r = e >> 6, c = e & 63;
       X[r * kLuS + c] = (r < vk && c < vj) ? lu_load(A[(size_t)(k0 + p[r]) * dim + j0 + c]) : make_double2(0.0, 0.0);
-    }
-    if (j > k) {
-      for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
-        const int r = e >> 6, c = e & 63;
-        D[r * kLuS + c] = (r < vk && c < vk) ? lu_load(A[(size_t)(k0 + r) * dim + k0 + c]) : make_double2(0.0, 0.0);
-      }
-      for (int c = 0; c < vk; ++c) {
-        __syncthreads();
-        const int rem = vk - 1 - c;
-        for (int e = tid; e < rem * vj; e += blockDim.x) {
-          const int r = c + 1 + e / vj, col = e % vj;
-          X[r * kLuS + col] = c_sub_mul(X[r * kLuS + col], D[r * kLuS + c], X[c * kLuS + col]);
-        }
-      }
     }
     __syncthreads();
     for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
       const int r = e >> 6, c = e & 63;
       if (r < vk && c < vj) A[(size_t)(k0 + r) * dim + j0 + c] = lu_cast<T>(X[r * kLuS + c]);
     }
-  } else {
-    // tile (i, k), i > k: X U_kk = A_ik
-    const int i = k + 1 + (item - nrow);
-    const int i0 = i * kLuT, vi = min(kLuT, dim - i0);
-    for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
-      const int r = e >> 6, c = e & 63;
-      X[r * kLuS + c] = (r < vi && c < vk) ? lu_load(A[(size_t)(i0 + r) * dim + k0 + c]) : make_double2(0.0, 0.0);
-      D[r * kLuS + c] = (r < vk && c < vk) ? lu_load(A[(size_t)(k0 + r) * dim + k0 + c]) : make_double2(0.0, 0.0);
-    }
-    for (int c = 0; c < vk; ++c) {
-      __syncthreads();
-      bool zero = false;
-      const double2 inv = c_inv(D[c * kLuS + c], &zero);  // zero pivots were flagged by the diag step
-      if (tid < vi) X[tid * kLuS + c] = c_mul(X[tid * kLuS + c], inv);
-      __syncthreads();
-      const int rem = vk - 1 - c;
-      for (int e = tid; e < vi * rem; e += blockDim.x) {
-        const int r = e / rem, jj = c + 1 + e % rem;
-        X[r * kLuS + jj] = c_sub_mul(X[r * kLuS + jj], X[r * kLuS + c], D[c * kLuS + jj]);
-      }
+    return;
+  }
+  // Left (rows) x Right (columns): row tile L_kk^{-1} x (P A_kj); column tile A_ik x U_kk^{-1}
+  const double2* inv = dinv64 + ((size_t)(g.tile0[b] + k) * 2 + (row_tile ? 0 : 1)) * kLuT * kLuT;
+  double2 acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[a][q] = make_double2(0.0, 0.0);
+  for (int kc = 0; kc < kLuT; kc += kLuKc) {
+    __syncthreads();
+    for (int e = tid; e < kLuT * kLuKc; e += blockDim.x) {
+      const int r = e / kLuKc, kk = e % kLuKc;  // Left[r][kc + kk]
+      double2 lv;
+      if (row_tile) lv = inv[r * kLuT + kc + kk];  // padded part: identity
+      else lv = (r < vi && kc + kk < vk) ? lu_load(A[(size_t)(i0 + r) * dim + k0 + kc + kk]) : make_double2(0.0, 0.0);
+      Ls[kk][r] = lv;
+      const int kk2 = e / kLuT, c = e % kLuT;  // Right[kc + kk2][c]
+      double2 rv;
+      if (row_tile)
+        rv = (kc + kk2 < vk && c < vj) ? lu_load(A[(size_t)(k0 + p[kc + kk2]) * dim + j0 + c]) : make_double2(0.0, 0.0);
+      else
+        rv = inv[(kc + kk2) * kLuT + c];
+      Us[kk2][c] = rv;
     }
     __syncthreads();
-    for (int e = tid; e < kLuT * kLuT; e += blockDim.x) {
-      const int r = e >> 6, c = e & 63;
-      if (r < vi && c < vk) A[(size_t)(i0 + r) * dim + k0 + c] = lu_cast<T>(X[r * kLuS + c]);
+#pragma unroll 4
+    for (int kk = 0; kk < kLuKc; ++kk) {
+      double2 l[4], u[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) l[a] = Ls[kk][ty + 16 * a];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) u[q] = Us[kk][tx + 16 * q];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[a][q].x = fma(l[a].x, u[q].x, acc[a][q].x);
+          acc[a][q].x = fma(-l[a].y, u[q].y, acc[a][q].x);
+          acc[a][q].y = fma(l[a].x, u[q].y, acc[a][q].y);
+          acc[a][q].y = fma(l[a].y, u[q].x, acc[a][q].y);
+        }
+    }
+  }
+  __syncthreads();  // every read of the tile (row tile: in place) precedes the stores
+  const int vr = row_tile ? vk : vi, vc = row_tile ? vj : vk;
+  const int c0 = row_tile ? j0 : k0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int r = ty + 16 * a;
+    if (r >= vr) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = tx + 16 * q;
+      if (c < vc) A[(size_t)(i0 + r) * dim + c0 + c] = lu_cast<T>(acc[a][q]);
     }
   }
 }
@@ -233,7 +259,6 @@ __global__ void __launch_bounds__(256) lu_panel_kernel(LuGeom g, const int* pre,
 // ---- step k, part 3: trailing update A_ij -= L_ik U_kj for i, j > k ----------------------------
 // 256 threads, 4 x 4 outputs each (rows ty + 16p, columns tx + 16q); the inner dimension is
 // staged in two chunks of 32 (L transposed, U as is).
-constexpr int kLuKc = 32;
 constexpr size_t kLuUpdateSmem = 2 * (size_t)kLuKc * kLuS * sizeof(double2);
 __global__ void __launch_bounds__(256, 2) lu_update_kernel(LuGeom g, const int* pre, int k, double2* mat) {
   extern __shared__ double2 lu_smem[];
@@ -368,17 +393,18 @@ __global__ void __launch_bounds__(kLuUpd32Threads, 3) lu_update32_kernel(LuGeom 
   }
 }
 
-// ---- finalize: complex64 factors and the inverses of the diagonal tiles ------------------------
+// ---- step k, part 1b: the inverses of the factored diagonal tile k of every block ----------------
 // dinv[(tile0[b] + t) * 2 + 0] = L_tt^{-1} (unit lower), [.. + 1] = U_tt^{-1}, each 64 x 64
-// row-major complex64 (identity in the padded part); dinv64 (may be null) the same in complex128.
+// row-major complex64 (identity in the padded part); dinv64 the same in complex128 (the panel
+// products read it; finalize keeps it only with the complex128 factors).
 template <typename T>
 __global__ void __launch_bounds__(256) lu_diag_inverse_kernel(LuGeom g, const int* pre, const T* mat, float2* dinv,
-                                                              double2* dinv64, int* err) {
+                                                              double2* dinv64, int* err, int step) {
   extern __shared__ double2 lu_smem[];
   double2* D = lu_smem;                // [64][kLuS] factored diagonal tile
   double2* X = lu_smem + kLuT * kLuS;  // [64][kLuS] inverse under construction
   const int b = lu_block_of(pre, g.n_blocks, blockIdx.x);
-  const int t = blockIdx.x - pre[b];
+  const int t = step;  // diagonal tile `step` of every block that has one
   const int dim = g.dim[b];
   const int t0 = t * kLuT, v = min(kLuT, dim - t0);
   const T* A = mat + g.mat_off[b];

@@ -417,10 +417,10 @@ int lu_smem_attributes() {
   const int one = (int)(yasf::kLuT * yasf::kLuS * sizeof(double2));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
-  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     2 * one));
-  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     2 * one));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_inv_kernel<double2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yasf::kLuUpdateSmem));
+  YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_panel_inv_kernel<float2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)yasf::kLuUpdateSmem));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_inverse_kernel<double2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * one));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_inverse_kernel<float2>,
@@ -462,15 +462,39 @@ extern "C" int yasf_precond_factor(yasf_precond* pc, void* stream) {
     YASF_CUDA_TRY(cudaFree(pc->d_mat));
     pc->d_mat = nullptr;
   }
+  {  // the diagonal-tile inverses: complex64 for the apply, complex128 for the panel products
+    const size_t tile_elems = (size_t)pc->n_tiles * 2 * kLuT * kLuT;
+    for (int w = 0; w < 2; ++w) {
+      void** p = w ? reinterpret_cast<void**>(&pc->d_dinv64) : reinterpret_cast<void**>(&pc->d_dinv);
+      if (*p) continue;
+      cudaError_t e = cudaMalloc(p, tile_elems * (w ? sizeof(double2) : sizeof(float2)));
+      if (e != cudaSuccess) {
+        set_cuda_error(e);
+        *p = nullptr;
+        return e == cudaErrorMemoryAllocation ? YASF_ERR_OUT_OF_MEMORY : YASF_ERR_CUDA;
+      }
+    }
+  }
   YASF_CUDA_TRY(cudaMemsetAsync(pc->d_err, 0, sizeof(int), s));
   for (int k = 0; k < pc->lu_steps; ++k) {
     int n = 0;
     const int* pre = lu_pre(pc, 0, k, &n);
-    if (n && c64) YASF_COUNTED(lu_diag_kernel<float2><<<n, 256, one, s>>>(g, pre, k, pc->d_mat32, pc->d_piv, pc->d_err));
-    else if (n) YASF_COUNTED(lu_diag_kernel<double2><<<n, 256, one, s>>>(g, pre, k, pc->d_mat, pc->d_piv, pc->d_err));
+    if (n && c64) {
+      YASF_COUNTED(lu_diag_kernel<float2><<<n, 256, one, s>>>(g, pre, k, pc->d_mat32, pc->d_piv, pc->d_err));
+      YASF_COUNTED(lu_diag_inverse_kernel<float2><<<n, 256, 2 * one, s>>>(g, pre, pc->d_mat32, pc->d_dinv,
+                                                                          pc->d_dinv64, pc->d_err, k));
+    } else if (n) {
+      YASF_COUNTED(lu_diag_kernel<double2><<<n, 256, one, s>>>(g, pre, k, pc->d_mat, pc->d_piv, pc->d_err));
+      YASF_COUNTED(lu_diag_inverse_kernel<double2><<<n, 256, 2 * one, s>>>(g, pre, pc->d_mat, pc->d_dinv,
+                                                                           pc->d_dinv64, pc->d_err, k));
+    }
     pre = lu_pre(pc, 1, k, &n);
-    if (n && c64) YASF_COUNTED(lu_panel_kernel<float2><<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat32, pc->d_piv));
-    else if (n) YASF_COUNTED(lu_panel_kernel<double2><<<n, 256, 2 * one, s>>>(g, pre, k, pc->d_mat, pc->d_piv));
+    if (n && c64)
+      YASF_COUNTED(lu_panel_inv_kernel<float2><<<n, 256, kLuUpdateSmem, s>>>(g, pre, k, pc->d_mat32, pc->d_piv,
+                                                                             pc->d_dinv64));
+    else if (n)
+      YASF_COUNTED(lu_panel_inv_kernel<double2><<<n, 256, kLuUpdateSmem, s>>>(g, pre, k, pc->d_mat, pc->d_piv,
+                                                                              pc->d_dinv64));
     pre = lu_pre(pc, 2, k, &n);
     if (n && c64)
       YASF_COUNTED(lu_update32_kernel<<<n, kLuUpd32Threads, kLuUpdateSmem32, s>>>(g, pre, k, pc->d_mat32));
@@ -569,23 +593,7 @@ extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
     YASF_COUNTED(to_c64_kernel<<<2048, 256, 0, s>>>(pc->mat_elems, pc->d_mat, pc->d_mat32));
     YASF_CUDA_TRY(cudaGetLastError());
   }
-  if (pc->factored) {
-    if (int st = lu_smem_attributes()) return st;
-    const size_t tile_elems = (size_t)pc->n_tiles * 2 * kLuT * kLuT;
-    if (int st = alloc(reinterpret_cast<void**>(&pc->d_dinv), tile_elems * sizeof(float2))) return st;
-    if (pc->keep_f64)
-      if (int st = alloc(reinterpret_cast<void**>(&pc->d_dinv64), tile_elems * sizeof(double2))) return st;
-    int n = 0;
-    // every diagonal tile of every block: the sweep prefix of step 0 counts nt per block
-    const int* pre = lu_pre(pc, 3, 0, &n);
-    const int one = (int)(kLuT * kLuS * sizeof(double2));
-    if (pc->factored_c64)
-      YASF_COUNTED(lu_diag_inverse_kernel<float2><<<n, 256, 2 * one, s>>>(lu_geom(pc), pre, pc->d_mat32, pc->d_dinv,
-                                                                          nullptr, pc->d_err));
-    else
-      YASF_COUNTED(lu_diag_inverse_kernel<double2><<<n, 256, 2 * one, s>>>(
-          lu_geom(pc), pre, pc->d_mat, pc->d_dinv, pc->keep_f64 ? pc->d_dinv64 : nullptr, pc->d_err));
-    YASF_CUDA_TRY(cudaGetLastError());
+  if (pc->factored) {  // the inverses of the diagonal tiles were made during the factorisation
     int err = 0;
     YASF_CUDA_TRY(cudaMemcpyAsync(&err, pc->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     YASF_CUDA_TRY(cudaStreamSynchronize(s));
@@ -593,9 +601,11 @@ extern "C" int yasf_precond_finalize(yasf_precond* pc, void* stream) {
       set_error_text("a block has a zero pivot (singular diagonal tile)");
       return YASF_ERR_NOT_FINITE;
     }
-    if (!pc->keep_f64 && pc->d_mat) {  // the solves stream the complex64 factors only
-      YASF_CUDA_TRY(cudaFree(pc->d_mat));
+    if (!pc->keep_f64) {  // the solves stream the complex64 factors and inverses only
+      if (pc->d_mat) YASF_CUDA_TRY(cudaFree(pc->d_mat));
       pc->d_mat = nullptr;
+      if (pc->d_dinv64) YASF_CUDA_TRY(cudaFree(pc->d_dinv64));
+      pc->d_dinv64 = nullptr;
     }
   }
   for (auto& gr : pc->graphs) cudaGraphExecDestroy(gr.exec);  // captured the previous factors
