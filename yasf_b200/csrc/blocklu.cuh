@@ -323,9 +323,9 @@ __global__ void __launch_bounds__(256, 2) lu_update_kernel(LuGeom g, const int* 
 }
 
 // Complex64 storage: the same update in FP32, as packed FMAs (FFMA2). The staged operands are laid
-// out as the packed instructions consume them: Ls[kk][row] = (l_re, l_re, -l_im, l_im) and
-// Us[kk][col] = (u_re, u_im, u_im, u_re), so each complex multiply-add is two FFMA2:
-//   (acc_re, acc_im) += (l_re, l_re) * (u_re, u_im) + (-l_im, l_im) * (u_im, u_re).
+// out as the packed instructions consume them, L negated: Ls[kk][row] = (-l_re, -l_re, l_im, -l_im)
+// and Us[kk][col] = (u_re, u_im, u_im, u_re), so each complex multiply-subtract is two FFMA2:
+//   (acc_re, acc_im) += (-l_re, -l_re) * (u_re, u_im) + (l_im, -l_im) * (u_im, u_re).
 // 128 threads, 8 x 4 outputs each (rows ty + 8p, columns tx + 16q): per inner index a warp issues
 // 12 shared loads (16 wavefronts) for 64 FFMA2, so the FP32 pipe, not shared memory, is the bound
 // (with 4 x 4 outputs it was 12 wavefronts per 32 FFMA2). Three CTAs per SM.
@@ -346,17 +346,22 @@ __global__ void __launch_bounds__(kLuUpd32Threads, 3) lu_update32_kernel(LuGeom 
   const int vk = min(kLuT, dim - k0), vi = min(kLuT, dim - i0), vj = min(kLuT, dim - j0);
   float2* A = mat + g.mat_off[b];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // the accumulators start from the C tile (its loads overlap the first staging): C - L U is
+  // accumulated directly and the epilogue is a plain store
   float2 acc[8][4];
 #pragma unroll
   for (int p = 0; p < 8; ++p)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[p][q] = make_float2(0.f, 0.f);
+    for (int q = 0; q < 4; ++q) {
+      const int r = ty + 8 * p, c = tx + 16 * q;
+      acc[p][q] = (r < vi && c < vj) ? A[(size_t)(i0 + r) * dim + j0 + c] : make_float2(0.f, 0.f);
+    }
   for (int kc = 0; kc < vk; kc += kLuKc) {
     __syncthreads();
     for (int e = tid; e < kLuT * kLuKc; e += kLuUpd32Threads) {
       const int r = e / kLuKc, kk = e % kLuKc;
       const float2 l = (r < vi && kc + kk < vk) ? A[(size_t)(i0 + r) * dim + k0 + kc + kk] : make_float2(0.f, 0.f);
-      Ls[kk][r] = make_float4(l.x, l.x, -l.y, l.y);
+      Ls[kk][r] = make_float4(-l.x, -l.x, l.y, -l.y);  // negated: acc = C - L U
       const int kk2 = e / kLuT, c = e % kLuT;
       const float2 u = (kc + kk2 < vk && c < vj) ? A[(size_t)(k0 + kc + kk2) * dim + j0 + c] : make_float2(0.f, 0.f);
       Us[kk2][c] = make_float4(u.x, u.y, u.y, u.x);
@@ -386,9 +391,7 @@ __global__ void __launch_bounds__(kLuUpd32Threads, 3) lu_update32_kernel(LuGeom 
     for (int q = 0; q < 4; ++q) {
       const int c = tx + 16 * q;
       if (c >= vj) continue;
-      float2* a = A + (size_t)(i0 + r) * dim + j0 + c;
-      const float2 o = *a;
-      *a = make_float2(o.x - acc[p][q].x, o.y - acc[p][q].y);
+      A[(size_t)(i0 + r) * dim + j0 + c] = acc[p][q];
     }
   }
 }
