@@ -210,6 +210,21 @@ int yasf_plane_wave_rhs(int lmax, int n_particles, const double* positions, int 
                         const double* kvec, const double* coef, const double* focal_point,
                         const double* tmat, double* a, double* b, long long ld, void* stream);
 
+/* ---- far field of the scattered wave (consumers of the coefficients) ---------------------------
+ * Replaces Optics.compute_scattered_e_field_angle_components (yasfpy/optics.py:178-267; kernels
+ * yasfpy/functions/cpu_numba.py:536-601 and cuda_numba.py:824-894) and the Stokes part of
+ * compute_polarization_components (cpu_numba.py:604-660) for one wavelength: for every sampling
+ * direction a, E_theta(a) and E_phi(a) = sum over particles s and modes n of
+ * i^{tau-l-2} coef[s,n] / sqrt(2l(l+1)) e^{i(m phi_a - k r_s.e_r(a))} times the angular functions,
+ * and (stokes, may be NULL) I, Q, U, V per direction (4 doubles each). coef: device (N*nmax)
+ * complex128, particle-major (the solution vector); positions: device (N, 3); polar, azimuthal:
+ * device (n_dirs) radians; pilm, taulm: device (lmax+1, lmax+1, n_dirs) float64, the reference's
+ * spherical_functions_trigon arrays (yasfpy/functions/spherical_functions_trigon.py:11-96);
+ * e_theta, e_phi: device (n_dirs) complex128. Asynchronous. */
+int yasf_far_field(int lmax, int n_particles, const double* positions, double k_medium, const double* coef,
+                   int n_dirs, const double* polar, const double* azimuthal, const double* pilm,
+                   const double* taulm, double* e_theta, double* e_phi, double* stokes, void* stream);
+
 /* ---- grouped solve: right-hand sides of several aggregates at once -------------------------------
  * No single reference counterpart: the reference solves one aggregate and one incidence per
  * Simulation (yasfpy/scattered_field_coefficients.py:95-144, yasfpy/solver.py:108-121). Here the

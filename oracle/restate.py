@@ -15,6 +15,10 @@ Functions and the reference code they restate:
                             pin (yasfpy/preconditioner.py:92-175 cannot build multi-sphere blocks)
   reference_translation_table  the reference's own Numerics.translation_ab5 (yasfpy/numerics.py:187-281)
                             for lmax 1-8, as generated by tests/golden/make_golden.py
+  angular_functions         yasfpy/functions/spherical_functions_trigon.py:11-96 (pi_lm, tau_lm)
+  far_field                 yasfpy/functions/cpu_numba.py:536-601 evaluated serially (the reference's
+                            parallel loop adds into shared elements), one wavelength
+  polarization_components   yasfpy/functions/cpu_numba.py:604-660
 """
 
 from __future__ import annotations
@@ -143,3 +147,81 @@ def block_matrix(lmax, positions, k, table, tmat_flat, block: np.ndarray) -> np.
         e[gi] = 1.0
         M[:, c] = master_matvec(lmax, positions, k, table, tmat_flat, e)[idx]
     return M
+
+
+def angular_functions(lmax: int, theta: np.ndarray):
+    """pi_lm(theta), tau_lm(theta), each (lmax+1, lmax+1, n): the normalised angular functions of
+    yasfpy/functions/spherical_functions_trigon.py:11-96, by the same recurrences."""
+    from math import factorial
+
+    ct = np.cos(np.asarray(theta, dtype=float).ravel())
+    st = np.sin(np.asarray(theta, dtype=float).ravel())
+    K = ct.size
+    plm = np.zeros((lmax + 1, lmax + 1, K))
+    pilm = np.zeros_like(plm)
+    taulm = np.zeros_like(plm)
+    dp0 = np.zeros((lmax + 1, K))  # d/dct of P_l0
+    plm[0, 0] = np.sqrt(0.5)
+    plm[1, 0] = np.sqrt(1.5) * ct
+    dp0[1] = np.sqrt(3.0) * plm[0, 0]
+    taulm[1, 0] = -st * dp0[1]
+    for l in range(1, lmax):
+        plm[l + 1, 0] = (np.sqrt((2 * l + 1) * (2 * l + 3)) * ct * plm[l, 0]
+                         - l * np.sqrt((2 * l + 3) / (2 * l - 1)) * plm[l - 1, 0]) / (l + 1)
+        dp0[l + 1] = np.sqrt((2 * l + 3) / (2 * l + 1)) * ((l + 1) * plm[l, 0] + ct * dp0[l])
+        taulm[l + 1, 0] = -st * dp0[l + 1]
+    for m in range(1, lmax + 1):
+        c = np.sqrt((2 * m + 1) / 2 / factorial(2 * m)) * np.prod(np.arange(1, 2 * m, 2, dtype=float))
+        plm[m, m] = c * st**m
+        pilm[m, m] = c * st ** (m - 1)
+        taulm[m, m] = m * ct * pilm[m, m]
+        for l in range(m, lmax):
+            a1 = np.sqrt((2 * l + 1) * (2 * l + 3) / (l + 1 - m) / (l + 1 + m)) * ct
+            a2 = np.sqrt((2 * l + 3) * (l - m) * (l + m) / (2 * l - 1) / (l + 1 - m) / (l + 1 + m))
+            prev_p = plm[l - 1, m] if l - 1 >= m else 0.0
+            prev_pi = pilm[l - 1, m] if l - 1 >= m else 0.0
+            plm[l + 1, m] = a1 * plm[l, m] - a2 * prev_p
+            pilm[l + 1, m] = a1 * pilm[l, m] - a2 * prev_pi
+            taulm[l + 1, m] = ((l + 1) * ct * pilm[l + 1, m]
+                               - (l + 1 + m) * np.sqrt((2 * l + 3) * (l + 1 - m) / (2 * l + 1) / (l + 1 + m))
+                               * pilm[l, m])
+    return pilm, taulm
+
+
+def far_field(lmax: int, positions: np.ndarray, k: float, coef: np.ndarray, polar: np.ndarray,
+              azimuthal: np.ndarray):
+    """(E_theta, E_phi) on the sampling directions, each (n,) complex: the sum over every particle s
+    and mode n = (tau, l, m) of yasfpy/functions/cpu_numba.py:536-601 for one wavelength, with
+    coef (N, nmax) the scattered-field coefficients."""
+    polar = np.asarray(polar, dtype=float).ravel()
+    azimuthal = np.asarray(azimuthal, dtype=float).ravel()
+    pilm, taulm = angular_functions(lmax, polar)
+    e_r = np.stack((np.sin(polar) * np.cos(azimuthal), np.sin(polar) * np.sin(azimuthal), np.cos(polar)), axis=1)
+    phase = np.exp(-1j * k * (np.asarray(positions) @ e_r.T))  # (N, A)
+    nmax = 2 * lmax * (lmax + 2)
+    e_theta = np.zeros(polar.size, dtype=complex)
+    e_phi = np.zeros_like(e_theta)
+    for n in range(nmax):
+        tau = 1 if n < nmax // 2 else 2
+        rem = n - (tau - 1) * (nmax // 2)
+        l = int(np.floor(np.sqrt(rem + 1)))
+        m = rem + 1 - l * l - l
+        t = (1j ** (tau - l - 2)) / np.sqrt(2 * l * (l + 1)) * np.exp(1j * m * azimuthal) \
+            * (coef[:, n] @ phase)
+        pi_, ta_ = pilm[l, abs(m)], taulm[l, abs(m)]
+        if tau == 1:
+            e_theta += t * pi_ * 1j * m
+            e_phi -= t * ta_
+        else:
+            e_theta += t * ta_
+            e_phi += t * pi_ * 1j * m
+    return e_theta, e_phi
+
+
+def polarization_components(e_theta: np.ndarray, e_phi: np.ndarray):
+    """I and the degrees of polarisation (dop, dolp, dolp_q, dolp_u, docp) of the far field
+    (yasfpy/functions/cpu_numba.py:604-660)."""
+    at, ap = np.abs(e_theta) ** 2, np.abs(e_phi) ** 2
+    x = e_theta * np.conj(e_phi)
+    I, Q, U, V = at + ap, at - ap, -2 * x.real, 2 * x.imag
+    return I, np.sqrt(Q**2 + U**2 + V**2) / I, np.sqrt(Q**2 + U**2) / I, -Q / I, U / I, V / I

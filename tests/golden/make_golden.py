@@ -7,7 +7,9 @@ location must be given in ``$YASF_REFERENCE`` (there is no default):
 
 Parts: ``tables`` (CELES goldens and translation tables lmax 1-6), ``c1``, ``l78`` (translation
 tables lmax 7 and 8 and reference matvec fixtures at those orders), ``nearfar`` (the near-field
-backend), ``celes500``; no part = all.
+backend), ``celes500``, ``farfield`` (the scattered far field, Stokes parameters and phase function
+of a solved aggregate on a 2-D sampling grid; run alone, with the reference's Numba loops on one
+thread: its far-field loop adds into shared array elements from a parallel loop); no part = all.
 
 The reference imports with the stand-ins from ``oracle/stubs`` (pywigxjpf via sympy's exact 3j,
 refidxdb and pyperf as inert stand-ins). Two kinds of fixtures are written:
@@ -44,6 +46,8 @@ sys.path.insert(0, str(REPO / "oracle" / "stubs"))
 sys.path.insert(0, str(REF))
 # the reference caches its translation tables under $HOME: keep that cache in a temporary directory
 os.environ["HOME"] = tempfile.mkdtemp(prefix="yasf_golden_home_")
+if sys.argv[1:] == ["farfield"]:  # serial Numba loops (set before numba is imported)
+    os.environ["NUMBA_NUM_THREADS"] = "1"
 
 from scipy.io import loadmat  # noqa: E402
 
@@ -63,7 +67,7 @@ def ref_modules():
 
 
 def ref_simulation(positions, radii, m, wavelength, lmax, tol=1e-8, restart=100, max_iter=1000,
-                   polar=0.0, azimuthal=0.0, pol="TE", wavelengths=None):
+                   polar=0.0, azimuthal=0.0, pol="TE", wavelengths=None, sampling=(10,)):
     InitialField, Numerics, Optics, Parameters, Particles, Simulation, Solver = ref_modules()
     n = positions.shape[0]
     particles = Particles(position=positions, r=radii, refractive_index=np.full(n, m, dtype=complex))
@@ -73,7 +77,7 @@ def ref_simulation(positions, radii, m, wavelength, lmax, tol=1e-8, restart=100,
     params = Parameters(wavelength=wl, medium_refractive_index=np.ones(wl.size, dtype=complex),
                         particles=particles, initial_field=field)
     solver = Solver(solver_type="gmres", tolerance=tol, max_iter=max_iter, restart=restart)
-    numerics = Numerics(lmax=lmax, sampling_points_number=np.array([10]), gpu=False, solver=solver,
+    numerics = Numerics(lmax=lmax, sampling_points_number=np.array(sampling), gpu=False, solver=solver,
                         coupling_backend="dense")
     numerics.compute_translation_table()
     sim = Simulation(params, numerics)
@@ -288,9 +292,44 @@ def precond_fixture():
          tmat=sim.mie_coefficients[sidx, :, 0].ravel(), **mats)
 
 
+def farfield_fixture():
+    """The reference's Optics far field on a solved aggregate: E_theta, E_phi
+    (compute_scattered_e_field_angle_components, yasfpy/optics.py:178-267) and the phase function
+    with its degrees of polarisation (compute_phase_function, :752-1038) on a 2-D sampling grid."""
+    rng = np.random.default_rng(31)
+    radii = rng.uniform(0.05, 0.1, size=24)
+    pos = rsa_cube(radii, 0.15, rng, max_attempts=200_000)
+    lmax, wl, m = 3, 0.55, 1.5 + 0.01j
+    grid = np.array([12, 9])  # azimuthal x polar sampling points
+    sim, Optics = ref_simulation(pos, radii, m, wl, lmax, tol=1e-12, sampling=grid)
+    sim.numerics.compute_spherical_unity_vectors()  # as yasfpy/yasf.py:172 does before optics
+    sim.compute_mie_coefficients()
+    sim.compute_initial_field_coefficients()
+    sim.compute_right_hand_side()
+    sim.compute_scattered_field_coefficients()
+    opt = Optics(sim)
+    opt.compute_cross_sections()
+    e_theta, e_phi = opt.compute_scattered_e_field_angle_components()
+    opt.compute_phase_function(legendre_coefficients_number=8)
+    save("ref_farfield.npz", lmax=lmax, wavelength=wl, refractive_index=m, positions=pos, radii=radii,
+         grid=grid, polar=sim.numerics.polar_angles, azimuthal=sim.numerics.azimuthal_angles,
+         scattered=sim.scattered_field_coefficients[:, :, 0], c_sca=opt.c_sca, c_ext=opt.c_ext,
+         e_theta=e_theta[:, 0], e_phi=e_phi[:, 0], phase_function_3d=opt.phase_function_3d[:, 0],
+         phase_function=opt.phase_function[:, 0],
+         legendre=opt.phase_function_legendre_coefficients[:, 0],
+         dop_3d=opt.degree_of_polarization_3d[:, 0], dolp_3d=opt.degree_of_linear_polarization_3d[:, 0],
+         dolq_3d=opt.degree_of_linear_polarization_q_3d[:, 0],
+         dolu_3d=opt.degree_of_linear_polarization_u_3d[:, 0],
+         docp_3d=opt.degree_of_circular_polarization_3d[:, 0],
+         dop=opt.degree_of_polarization[:, 0], scattering_angles=opt.scattering_angles)
+
+
 def main():
     t0 = time.time()
     only = set(sys.argv[1:])
+    if only == {"farfield"}:
+        farfield_fixture()
+        return
     if not only or "tables" in only:
         celes_fixtures()
         celes_fits_fixture()

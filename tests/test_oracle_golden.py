@@ -116,3 +116,19 @@ def test_oracle_near_field_matches_reference_nearfar_backend(golden):
     dense = R.coupling_matvec_rows(lmax, g["positions"], k, table, g["x"])
     assert rel_err(dense, g["wx_dense"]) < 1e-12
     assert rel_err(near, dense) > 1e-3  # the cutoff drops pairs that matter
+
+
+def test_far_field_oracle_matches_reference(golden):
+    """The oracle's far field (E_theta, E_phi) and degrees of polarisation equal the reference's own
+    Optics output (serial Numba loops) on a solved 24-sphere aggregate, 12 x 9 sampling grid."""
+    g = golden("ref_farfield.npz")
+    k = 2 * np.pi / float(g["wavelength"])
+    et, ep = R.far_field(int(g["lmax"]), g["positions"], k, g["scattered"], g["polar"], g["azimuthal"])
+    assert np.abs(et - g["e_theta"]).max() <= 1e-12 * np.abs(g["e_theta"]).max()
+    assert np.abs(ep - g["e_phi"]).max() <= 1e-12 * np.abs(g["e_phi"]).max()
+    I, dop, dolp, dolq, dolu, docp = R.polarization_components(et, ep)
+    pf = I * 4 * np.pi / k**2 / g["c_sca"][0]
+    assert np.abs(pf - g["phase_function_3d"]).max() <= 1e-12 * np.abs(pf).max()
+    for ours, key in ((dop, "dop_3d"), (dolp, "dolp_3d"), (dolq, "dolq_3d"), (dolu, "dolu_3d"),
+                      (docp, "docp_3d")):
+        assert np.allclose(ours, g[key], rtol=0, atol=1e-12), key

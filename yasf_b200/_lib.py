@@ -63,6 +63,7 @@ SIGNATURES = {
     "yasf_grouped_workspace_size": [_vp, _i, _vp, _i, _c.POINTER(_sz)],
     "yasf_grouped_solve": [_vp, _i, _vp, _d, _i, _i, _d, _i, _vp, _sz, _dp, _dp, _vp],
     "yasf_plane_wave_rhs": [_i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _ll, _vp],
+    "yasf_far_field": [_i, _i, _vp, _d, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "yasf_plan_create": [_i, _vp, _c.POINTER(_vp)],
     "yasf_plan_destroy": [_vp],
     "yasf_plan_info": [_vp, _c.POINTER(_i), _c.POINTER(_ll), _c.POINTER(_ll)],

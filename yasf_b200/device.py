@@ -207,6 +207,28 @@ class CouplingDevice:
              f.ctypes.data_as(ctypes.c_void_p), _ptr(tmat), _ptr(A), _ptr(B), self.n, _stream_ptr())
         return A, B
 
+    def far_field(self, coef: torch.Tensor, polar, azimuthal, stokes: bool = True):
+        """Scattered far field on sampling directions (yasf_far_field): (E_theta, E_phi) as
+        complex128 device tensors (n_dirs,) and, with stokes, (n_dirs, 4) float64 I, Q, U, V.
+        coef: the (N*nmax,) complex128 scattered-field coefficients, particle-major."""
+        from yasf_b200.incident import spherical_functions_trigon
+
+        polar = np.ascontiguousarray(np.asarray(polar, dtype=np.float64).ravel())
+        azimuthal = np.ascontiguousarray(np.asarray(azimuthal, dtype=np.float64).ravel())
+        A = polar.size
+        pilm, taulm = spherical_functions_trigon(self.lmax, np.cos(polar), np.sin(polar))
+        dv = self.device
+        pt, at = torch.from_numpy(polar).to(dv), torch.from_numpy(azimuthal).to(dv)
+        pl = torch.from_numpy(np.ascontiguousarray(pilm)).to(dv)
+        tl = torch.from_numpy(np.ascontiguousarray(taulm)).to(dv)
+        c = coef.reshape(-1).contiguous()
+        et = torch.empty(A, dtype=torch.complex128, device=dv)
+        ep = torch.empty(A, dtype=torch.complex128, device=dv)
+        st = torch.empty((A, 4), dtype=torch.float64, device=dv) if stokes else None
+        call("yasf_far_field", self.lmax, self.n_particles, _ptr(self.pos), float(self.k), _ptr(c), A, _ptr(pt),
+             _ptr(at), _ptr(pl), _ptr(tl), _ptr(et), _ptr(ep), _ptr(st), _stream_ptr())
+        return et, ep, st
+
     INNER_KINDS = {"tf32": 0, "c64": 1, "c128": 2}
 
     def batched_solve(self, tmat: torch.Tensor, B: torch.Tensor, rtol: float, restart: int = 50,
