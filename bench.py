@@ -936,6 +936,36 @@ def precond_probe(args) -> None:
                       "finite": bool(torch.isfinite(y).all() and torch.isfinite(Y).all())}))
 
 
+def farfield_probe(args) -> None:
+    """Far field (E_theta, E_phi, Stokes) of the first N spheres of the C2 aggregate on 10,000
+    Fibonacci sampling directions, random coefficients: one warm-up and five timed launches."""
+    import torch
+
+    from yasf_b200.device import CouplingDevice
+    from yasf_b200.numerics import Numerics, cached_translation_table
+
+    agg, _, _ = workload("c2")
+    n = min(args.farfield_probe, agg.n)
+    dev = CouplingDevice(agg.lmax, cached_translation_table(agg.lmax), agg.positions[:n], agg.k,
+                         torch.device("cuda", 0))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    coef = torch.randn(dev.n, dtype=torch.complex128, device=dev.device, generator=g)
+    _, polar, azim = Numerics.compute_fibonacci_sphere_points(10_000)
+    dirs = dev.far_field_directions(polar, azim)  # setup, outside the timed launches
+    dev.far_field(coef, dirs)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        dev.far_field(coef, dirs)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    cmacs = 10_000 * n * dev.nmax
+    print(json.dumps({"probe": "farfield", "n": n, "directions": 10_000, "ms": ms,
+                      "complex_macs": cmacs, "tflops_fp64": cmacs * 8 / ms / 1e9}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -956,6 +986,8 @@ def main() -> None:
     ap.add_argument("--panel-probe", type=int, default=0, metavar="N",
                     help="profiling aid: run 4 TF32 panel matvecs on the first N spheres and exit")
     ap.add_argument("--nrhs", type=int, default=128, help="columns of --panel-probe")
+    ap.add_argument("--farfield-probe", type=int, default=0, metavar="N",
+                    help="profiling aid: time the far field of the first N spheres on 10,000 directions and exit")
     ap.add_argument("--precond-probe", type=int, default=0, metavar="N",
                     help="profiling aid: prepare the block-Jacobi preconditioner on the first N spheres, "
                          "time its applies and exit")
@@ -984,6 +1016,9 @@ def main() -> None:
         return
     if args.precond_probe:
         precond_probe(args)
+        return
+    if args.farfield_probe:
+        farfield_probe(args)
         return
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)

@@ -207,20 +207,27 @@ class CouplingDevice:
              f.ctypes.data_as(ctypes.c_void_p), _ptr(tmat), _ptr(A), _ptr(B), self.n, _stream_ptr())
         return A, B
 
-    def far_field(self, coef: torch.Tensor, polar, azimuthal, stokes: bool = True):
-        """Scattered far field on sampling directions (yasf_far_field): (E_theta, E_phi) as
-        complex128 device tensors (n_dirs,) and, with stokes, (n_dirs, 4) float64 I, Q, U, V.
-        coef: the (N*nmax,) complex128 scattered-field coefficients, particle-major."""
+    def far_field_directions(self, polar, azimuthal) -> tuple:
+        """Device arrays of a set of sampling directions for far_field: the angles and the angular
+        functions pi_lm, tau_lm of yasfpy/functions/spherical_functions_trigon.py:11-96."""
         from yasf_b200.incident import spherical_functions_trigon
 
         polar = np.ascontiguousarray(np.asarray(polar, dtype=np.float64).ravel())
         azimuthal = np.ascontiguousarray(np.asarray(azimuthal, dtype=np.float64).ravel())
-        A = polar.size
         pilm, taulm = spherical_functions_trigon(self.lmax, np.cos(polar), np.sin(polar))
         dv = self.device
-        pt, at = torch.from_numpy(polar).to(dv), torch.from_numpy(azimuthal).to(dv)
-        pl = torch.from_numpy(np.ascontiguousarray(pilm)).to(dv)
-        tl = torch.from_numpy(np.ascontiguousarray(taulm)).to(dv)
+        return (torch.from_numpy(polar).to(dv), torch.from_numpy(azimuthal).to(dv),
+                torch.from_numpy(np.ascontiguousarray(pilm)).to(dv),
+                torch.from_numpy(np.ascontiguousarray(taulm)).to(dv))
+
+    def far_field(self, coef: torch.Tensor, polar, azimuthal=None, stokes: bool = True):
+        """Scattered far field on sampling directions (yasf_far_field): (E_theta, E_phi) as
+        complex128 device tensors (n_dirs,) and, with stokes, (n_dirs, 4) float64 I, Q, U, V.
+        coef: the (N*nmax,) complex128 scattered-field coefficients, particle-major; the directions
+        as (polar, azimuthal) angles or as the tuple far_field_directions returns."""
+        pt, at, pl, tl = polar if isinstance(polar, tuple) else self.far_field_directions(polar, azimuthal)
+        A = pt.numel()
+        dv = self.device
         c = coef.reshape(-1).contiguous()
         et = torch.empty(A, dtype=torch.complex128, device=dv)
         ep = torch.empty(A, dtype=torch.complex128, device=dv)
