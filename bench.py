@@ -225,6 +225,62 @@ def run_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def reference_gpu_probe(args) -> None:
+    """The reference's own GPU coupling matvec (Numba-CUDA CudaDenseCouplingOps,
+    yasfpy/coupling/cuda_dense.py:160-448) from the unmodified copy in baseline/_ref, on the chosen
+    workload's aggregate: Simulation set-up, one warm-up matvec, then the mean of three. Its stand-ins
+    for pywigxjpf / refidxdb / pyperf come from oracle/stubs; its table cache goes to a temporary
+    HOME. Prints one JSON line (or the reason it cannot run)."""
+    import tempfile
+
+    root = Path(__file__).resolve().parent
+    out = {"probe": "reference_gpu_matvec", "workload": args.workload}
+    if not (root / "baseline" / "_ref" / "yasfpy").is_dir():
+        out["unavailable"] = "baseline/_ref holds no copy of the reference"
+        print(json.dumps(out))
+        return
+    sys.path.insert(0, str(root / "baseline" / "_ref"))
+    sys.path.insert(0, str(root / "oracle" / "stubs"))
+    os.environ["HOME"] = tempfile.mkdtemp(prefix="yasf_ref_home_")
+    try:
+        from numba import cuda
+
+        from yasfpy.initial_field import InitialField
+        from yasfpy.numerics import Numerics
+        from yasfpy.parameters import Parameters
+        from yasfpy.particles import Particles
+        from yasfpy.simulation import Simulation
+        from yasfpy.solver import Solver
+
+        out["device"] = str(cuda.get_current_device().name)
+        agg, _, _ = workload(args.workload)
+        particles = Particles(position=agg.positions, r=agg.radii,
+                              refractive_index=np.full(agg.n, agg.refractive_index))
+        field = InitialField(beam_width=0, focal_point=np.zeros(3), polar_angle=0.0, azimuthal_angle=0.0,
+                             polarization="TE")
+        params = Parameters(wavelength=np.array([agg.wavelength]), medium_refractive_index=np.ones(1, dtype=complex),
+                            particles=particles, initial_field=field)
+        numerics = Numerics(lmax=agg.lmax, sampling_points_number=np.array([10]), gpu=True,
+                            solver=Solver(solver_type="gmres", tolerance=1e-8, max_iter=100, restart=100),
+                            coupling_backend="dense")
+        numerics.compute_translation_table()
+        t0 = time.perf_counter()
+        sim = Simulation(params, numerics)
+        out["setup_s"] = time.perf_counter() - t0
+        rng = np.random.default_rng(0)
+        x = rng.normal(size=agg.n * numerics.nmax) + 1j * rng.normal(size=agg.n * numerics.nmax)
+        t0 = time.perf_counter()
+        sim.coupling_matrix_multiply(x, idx=0)
+        out["first_matvec_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(3):
+            sim.coupling_matrix_multiply(x, idx=0)
+        out["matvec_s"] = (time.perf_counter() - t0) / 3
+    except Exception as e:  # record why the reference's GPU path cannot run here
+        out["unavailable"] = f"{type(e).__name__}: {e}"
+    print(json.dumps(out))
+
+
 # ---------------------------------------------------------------------------------------------
 def run_b200(args, rank: int, world: int) -> None:
     import torch
@@ -986,6 +1042,9 @@ def main() -> None:
     ap.add_argument("--panel-probe", type=int, default=0, metavar="N",
                     help="profiling aid: run 4 TF32 panel matvecs on the first N spheres and exit")
     ap.add_argument("--nrhs", type=int, default=128, help="columns of --panel-probe")
+    ap.add_argument("--reference-gpu-probe", action="store_true",
+                    help="with --impl reference: time the reference's own Numba-CUDA matvec on the workload "
+                         "(baseline/_ref) and exit")
     ap.add_argument("--farfield-probe", type=int, default=0, metavar="N",
                     help="profiling aid: time the far field of the first N spheres on 10,000 directions and exit")
     ap.add_argument("--precond-probe", type=int, default=0, metavar="N",
@@ -1019,6 +1078,9 @@ def main() -> None:
         return
     if args.farfield_probe:
         farfield_probe(args)
+        return
+    if args.reference_gpu_probe:
+        reference_gpu_probe(args)
         return
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
