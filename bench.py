@@ -1043,8 +1043,8 @@ def main() -> None:
                     help="profiling aid: run 4 TF32 panel matvecs on the first N spheres and exit")
     ap.add_argument("--nrhs", type=int, default=128, help="columns of --panel-probe")
     ap.add_argument("--reference-gpu-probe", action="store_true",
-                    help="with --impl reference: time the reference's own Numba-CUDA matvec on the workload "
-                         "(baseline/_ref) and exit")
+                    help="profiling aid: time the reference's own Numba-CUDA matvec (the unmodified copy in "
+                         "baseline/_ref) on the workload's aggregate and exit")
     ap.add_argument("--farfield-probe", type=int, default=0, metavar="N",
                     help="profiling aid: time the far field of the first N spheres on 10,000 directions and exit")
     ap.add_argument("--precond-probe", type=int, default=0, metavar="N",
