@@ -8,6 +8,7 @@
 // the same pair generator as the matvec (receiver Mie factor, pair vector pos[s1] - pos[s2]),
 // inverted once (the caller factorises it in place between assemble and finalize), and applied
 // as a gather / dense GEMV / scatter that streams the inverse once per application.
+#include <atomic>
 #include <cmath>
 #include <new>
 
@@ -411,9 +412,14 @@ const int* lu_pre(const yasf_precond* pc, int which, int k, int* ctas) {
   *ctas = (*v[which])[(size_t)k * W + pc->n_blocks];
   return pc->d_pre + (size_t)which * pc->lu_steps * W + (size_t)k * W;
 }
+// The kernels' dynamic shared-memory limits are function attributes of the current device: set
+// once per device (a process may drive several GPUs, from several host threads).
 int lu_smem_attributes() {
-  static int done = 0;
-  if (done) return YASF_OK;
+  static std::atomic<unsigned long long> done{0};
+  int dev = 0;
+  YASF_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return YASF_OK;
   const int one = (int)(yasf::kLuT * yasf::kLuS * sizeof(double2));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_diag_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, one));
@@ -433,7 +439,7 @@ int lu_smem_attributes() {
                                      (int)yasf::lu_solve_smem<float2>()));
   YASF_CUDA_TRY(cudaFuncSetAttribute(yasf::lu_solve_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)yasf::lu_solve_smem<double2>()));
-  done = 1;
+  done.fetch_or(bit, std::memory_order_release);
   return YASF_OK;
 }
 }  // namespace
