@@ -17,6 +17,9 @@
 // particle for the warp's directions, which are then broadcast by shuffles, and the coefficient
 // rows b[s, :] are read coalesced (one particle's modes across the lanes). The angular factors
 // are applied in the epilogue, the warp reduces, lane 0 writes E_theta, E_phi and (I, Q, U, V).
+// The rows of 32 particles at a time are staged in shared memory by asynchronous copies (two
+// buffers: the next chunk arrives while the current one is summed), so the block's 8 warps read
+// each row from shared memory instead of each waiting on its own L2 load.
 // Float64 throughout; every output is written by one warp in a fixed order (deterministic).
 #include <cmath>
 
@@ -27,15 +30,25 @@ namespace yasf {
 constexpr int kFfDirs = 4;   // directions per warp
 constexpr int kFfModes = 5;  // modes per lane: nmax <= 160 = 5 x 32 (lmax 8)
 
+__device__ __forceinline__ void ff_copy16(void* smem_dst, const void* gsrc) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void ff_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void ff_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Dynamic shared memory: two buffers of kFfChunk coefficient rows (kFfChunk x nmax complex128).
+constexpr int kFfChunk = 32;
 __global__ void __launch_bounds__(256) far_field_kernel(int L, int nmax, int n_particles, int n_dirs,
                                                         const double* pos, double k, const double2* coef,
                                                         const double* polar, const double* azimuthal,
                                                         const double* pilm, const double* taulm,
                                                         double2* e_theta, double2* e_phi, double* stokes) {
+  extern __shared__ __align__(16) double2 ff_rows[];  // [2][kFfChunk * nmax]
   const int lane = threadIdx.x & 31;
   const int warp = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-  const int a0 = warp * kFfDirs;
-  if (a0 >= n_dirs) return;  // whole warps only
+  const int a0 = warp * kFfDirs;  // warps past the last direction still stage rows, write nothing
   double ex[kFfDirs], ey[kFfDirs], ez[kFfDirs];
 #pragma unroll
   for (int d = 0; d < kFfDirs; ++d) {
@@ -53,8 +66,29 @@ __global__ void __launch_bounds__(256) far_field_kernel(int L, int nmax, int n_p
   for (int d = 0; d < kFfDirs; ++d)
 #pragma unroll
     for (int j = 0; j < kFfModes; ++j) F[d][j] = make_double2(0.0, 0.0);
+  // the block's warps share every coefficient row: a chunk of rows is copied into shared memory
+  // once per block (asynchronously, the next chunk while the current one is summed)
+  const int chunks = (n_particles + kFfChunk - 1) / kFfChunk;
+  const int chunk_elems = kFfChunk * nmax;
+  auto stage = [&](int c) {
+    double2* dst = ff_rows + (size_t)(c & 1) * chunk_elems;
+    const int rows = min(kFfChunk, n_particles - c * kFfChunk);
+    const double2* src = coef + (size_t)c * chunk_elems;
+    for (int e = threadIdx.x; e < rows * nmax; e += blockDim.x) ff_copy16(dst + e, src + e);
+    ff_commit();
+  };
+  stage(0);
 #pragma unroll 1
-  for (int s0 = 0; s0 < n_particles; s0 += 32) {
+  for (int c = 0; c < chunks; ++c) {
+    if (c + 1 < chunks) {
+      stage(c + 1);
+      ff_wait<1>();
+    } else {
+      ff_wait<0>();
+    }
+    __syncthreads();  // chunk c is in shared memory for every thread
+    const int s0 = c * kFfChunk;
+    const double2* rows = ff_rows + (size_t)(c & 1) * chunk_elems;
     // phases e^{-i k r_s . e_r} of particle s0 + lane for the warp's directions
     double pr[kFfDirs], pi[kFfDirs];
     const int sl = s0 + lane;
@@ -68,10 +102,10 @@ __global__ void __launch_bounds__(256) far_field_kernel(int L, int nmax, int n_p
       pr[d] = cs;
       pi[d] = sn;
     }
-    const int cnt = min(32, n_particles - s0);
+    const int cnt = min(kFfChunk, n_particles - s0);
 #pragma unroll 1
     for (int p = 0; p < cnt; ++p) {
-      const double2* row = coef + (size_t)(s0 + p) * nmax;
+      const double2* row = rows + (size_t)p * nmax;
       double qr[kFfDirs], qi[kFfDirs];
 #pragma unroll
       for (int d = 0; d < kFfDirs; ++d) {
@@ -91,7 +125,9 @@ __global__ void __launch_bounds__(256) far_field_kernel(int L, int nmax, int n_p
         }
       }
     }
+    __syncthreads();  // every warp is done with buffer c & 1 before chunk c + 2 is copied into it
   }
+  if (a0 >= n_dirs) return;  // whole warps only (after the block's last barrier)
   // angular factors of the lane's modes and the reduction over modes
   const int half = nmax / 2;
 #pragma unroll
@@ -176,7 +212,9 @@ extern "C" int yasf_far_field(int lmax, int n_particles, const double* positions
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const long long warps = ((long long)n_dirs + kFfDirs - 1) / kFfDirs;
   const int blocks = (int)((warps * 32 + 255) / 256);
-  YASF_COUNTED(far_field_kernel<<<blocks, 256, 0, s>>>(
+  const size_t smem = 2 * (size_t)kFfChunk * nmax * sizeof(double2);
+  YASF_CUDA_TRY(cudaFuncSetAttribute(far_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  YASF_COUNTED(far_field_kernel<<<blocks, 256, smem, s>>>(
       lmax, nmax, n_particles, n_dirs, positions, k_medium, reinterpret_cast<const double2*>(coef), polar,
       azimuthal, pilm, taulm, reinterpret_cast<double2*>(e_theta), reinterpret_cast<double2*>(e_phi), stokes));
   YASF_CUDA_TRY(cudaGetLastError());
